@@ -1,0 +1,271 @@
+/*
+ * C ABI of the B200 (sm_100a) KZG proving kernels for BN254.
+ *
+ * Part 1 is a drop-in for the reference's static library
+ * `zkwasm_prover_kernel` (build.rs:5-10): the same 27 symbols with the
+ * signatures the Rust FFI declares in src/cuda/bn254_c.rs:4-309.  Conventions,
+ * as in the reference:
+ *   - every pointer is a device pointer; Fr / Fq elements are 32 bytes
+ *     (4 x u64 little-endian, Montgomery form, R = 2^256); G1 affine points
+ *     are 64 bytes (x, y; identity (0, 0)); G1 Jacobian points 96 bytes
+ *     (X, Y, Z; identity Z = 0);
+ *   - `T**` arguments are device arrays of device pointers;
+ *   - the return value is cudaGetLastError() after enqueueing (asynchronous);
+ *   - entry points without a stream argument run on the legacy default stream.
+ * Rotations are taken modulo n for either sign.  None of these functions
+ * allocates device memory or blocks the host (the reference's msm does both:
+ * cuda/msm.cu:384-418).
+ *
+ * Part 2 adds batched, allocation-free entry points (prefix zkp_) that the
+ * Rust host can call for whole phases; their scratch memory is supplied by the
+ * caller and sized by the matching *_scratch_bytes query.
+ */
+#ifndef ZKWASM_PROVER_KERNEL_H
+#define ZKWASM_PROVER_KERNEL_H
+
+#include <stddef.h>
+#include <stdint.h>
+#include <cuda_runtime_api.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ======================================================================
+ * Part 1: reference-compatible symbols
+ * ==================================================================== */
+
+/* src/cuda/bn254_c.rs:6-16, cuda/bn254.cu:1357-1428.  Natural-order NTT of
+ * 2^array_log elements by the twiddle table `omega` built by
+ * expand_omega_buffer; scaled by *n_inv when n_inv is non-null (inverse
+ * transform).  The result is in `buf` if *(bool*)swap is false on return,
+ * else in `tmp`; *swap is written synchronously.  `pq` and `max_deg` are
+ * accepted and unused. */
+cudaError_t ntt(void *buf, void *tmp, void *pq, void *omega, void *n_inv, int array_log, int max_deg, void *swap,
+                cudaStream_t stream);
+
+/* src/cuda/bn254_c.rs:18-29, cuda/bn254.cu:1269-1286.  res[i] = L op R with
+ * L = l[(i+l_rot) mod size] (* l_c[0]) or l_c[0], R likewise;
+ * op 0 add, 1 mul, 2 copy L, 3 sub. */
+cudaError_t field_op(void *res, void *l, int l_rot, void *l_c, void *r, int r_rot, void *r_c, int size, int op,
+                     cudaStream_t stream);
+
+/* src/cuda/bn254_c.rs:31-39, cuda/bn254.cu:1232-1253.  to_coset == 0: zero
+ * s[size..extended_size) and multiply s[i] (i < size) by
+ * coset_powers[i mod coset_powers_n - 1] when i mod coset_powers_n != 0;
+ * to_coset != 0: the same multiply over i < extended_size. */
+cudaError_t extended_prepare(void *s, void *coset_powers, int coset_powers_n, int size, int extended_size,
+                             int to_coset, cudaStream_t stream);
+
+/* src/cuda/bn254_c.rs:41-49, cuda/bn254.cu:1288-1303 (default stream) */
+cudaError_t permutation_eval_h_p1(void *res, void *first_set, void *last_set, void *l0, void *l_last, void *y,
+                                  int n);
+
+/* src/cuda/bn254_c.rs:51-60, cuda/bn254.cu:1305-1319 (default stream) */
+cudaError_t permutation_eval_h_p2(void *res, void *set, void *l0, void *l_last, void *y, int n_set, int rot, int n);
+
+/* src/cuda/bn254_c.rs:62-69, cuda/bn254.cu:1321-1331 */
+cudaError_t permutation_eval_h_l(void *res, void *beta, void *gamma, void *p, int n, cudaStream_t stream);
+
+/* src/cuda/bn254_c.rs:71-79, cuda/bn254.cu:1217-1230 (default stream) */
+cudaError_t field_sum(void *res, void *v, void *v_c, void *v_rot, void *omegas, int v_n, int n);
+
+/* src/cuda/bn254_c.rs:81-88, cuda/bn254.cu:1255-1267.
+ * v = [coeff0, a00, a01, NULL, coeff1, a10, NULL, ...] (v_n entries),
+ * rot = one rotation per column entry; res[i] += sum_t coeff_t prod_j a_tj[i+rot]. */
+cudaError_t field_op_batch_mul_sum(void *res, void *v, void *rot, int v_n, int n, cudaStream_t stream);
+
+/* src/cuda/bn254_c.rs:90-106, cuda/bn254.cu:1430-1456 */
+cudaError_t lookup_eval_h(void *res, void *input, void *table, void *permuted_input, void *permuted_table, void *z,
+                          void *l0, void *l_last, void *l_active_row, void *y, void *beta, void *gamma, int rot,
+                          int n, cudaStream_t stream);
+
+/* src/cuda/bn254_c.rs:108-123, cuda/bn254.cu:1480-1504 */
+cudaError_t logup_eval_h(void *res, void *input_product, void *input_product_sum, void *table, void *multiplicity,
+                         void *z_first, void *z_last, void *l0, void *l_last, void *l_active_row, void *y, int rot,
+                         int n, cudaStream_t stream);
+
+/* src/cuda/bn254_c.rs:125-135, cuda/bn254.cu:1506-1522 */
+cudaError_t logup_eval_h_extra_inputs(void *res, void *input_product, void *input_product_sum, void *z,
+                                      void *l_active_row, void *y, int rot, int n, cudaStream_t stream);
+
+/* src/cuda/bn254_c.rs:137-147, cuda/bn254.cu:1524-1541 */
+cudaError_t logup_eval_h_z_set(void *res, void *set, void *l0, void *l_last, void *y, int n_set, int rot, int n,
+                               cudaStream_t stream);
+
+/* src/cuda/bn254_c.rs:149-157, cuda/bn254.cu:1914-1934.
+ * sum[i] = (init ? sum[i] : 0) + 1 / (input[i] + beta[0]).  `temp` is unused. */
+cudaError_t logup_sum_input_inv(void *sum, void *input, void *temp, void *beta, int init, int n,
+                                cudaStream_t stream);
+
+/* src/cuda/bn254_c.rs:159-166, cuda/bn254.cu:1995-2010 */
+cudaError_t logup_eval_h_inputs_product_sum(void *product, void *product_sum, void *sets, int n_set, int n,
+                                            cudaStream_t stream);
+
+/* src/cuda/bn254_c.rs:168-179, cuda/bn254.cu:1458-1478 (default stream) */
+cudaError_t shuffle_eval_h(void *res, void *input, void *table, void *z, void *l0, void *l_last, void *l_active_row,
+                           void *y, int rot, int n);
+
+/* src/cuda/bn254_c.rs:181-194, cuda/bn254.cu:1543-1566 (default stream) */
+cudaError_t shuffle_eval_h_v2(void *res, void *inputs, void *tables, void *betas, int group_len, void *z, void *l0,
+                              void *l_last, void *l_active_row, void *y, int rot, int n);
+
+/* src/cuda/bn254_c.rs:196, cuda/bn254.cu:1333-1355 (default stream).
+ * buf[0] = 1 and buf[1] = w are written by the caller; fills buf[i] = w^i for
+ * i < 2^n.  The table is natural order whatever may_bit_reversed says; ntt()
+ * is its only consumer besides the shplonk kernels, which need natural order. */
+cudaError_t expand_omega_buffer(void *buf, int n, int may_bit_reversed);
+
+/* src/cuda/bn254_c.rs:198, cuda/bn254.cu:1568-1578 (default stream) */
+cudaError_t field_mul_zip(void *buf, void *coeff, int coeff_n, int n);
+
+/* src/cuda/bn254_c.rs:200-206, cuda/bn254.cu:1608-1634.  x = table of
+ * x^(2^d), d < log2 n; res (n elements) is workspace and res[0] = p(x). */
+cudaError_t poly_eval(void *p, void *res, void *x, int n, cudaStream_t stream);
+
+/* src/cuda/bn254_c.rs:208-216, cuda/bn254.cu:1580-1592 (default stream) */
+cudaError_t shplonk_h_x_merge(void *res, void *v, void *values, void *omegas, void *diff_points, int diff_points_n,
+                              int n);
+
+/* src/cuda/bn254_c.rs:218-224, cuda/bn254.cu:1594-1606 (default stream);
+ * values[i] /= prod_j (omegas[i] - points[j]) by batch inversion. */
+cudaError_t shplonk_h_x_div_points(void *values, void *omegas, void *points, int points_n, int n);
+
+/* src/cuda/bn254_c.rs:226-236, cuda/bn254.cu:1968-1993.
+ * z = *last_z + exclusive prefix sum of input[i] - multiplicity[i]/(table[i]+beta);
+ * then *last_z = z[last_z_index].  `table` is used as scratch (as in the
+ * reference); `input` is not modified. */
+cudaError_t eval_logup_z_compose(void *z, void *input, void *table, void *multiplicity, void *beta, void *last_z,
+                                 int last_z_index, int n, cudaStream_t stream);
+
+/* src/cuda/bn254_c.rs:238-246, cuda/bn254.cu:1936-1966.  z = *last_z +
+ * exclusive prefix sum of z (in place); *last_z = z[last_z_index]; `table` is
+ * scratch (n/2048 + 2 elements), `input` is unused. */
+cudaError_t eval_logup_z_pure(void *z, void *input, void *table, void *last_z, int last_z_index, int n,
+                              cudaStream_t stream);
+
+/* src/cuda/bn254_c.rs:248-259, cuda/msm.cu:434-467.  The whole MSM already ran
+ * inside msm(); this leaves each result where the reference does (element 0
+ * of each per-MSM region) and only reports pending errors. */
+cudaError_t batch_msm_collect(void *remain_indices, void *remain_acc, void *next_remain_indices,
+                              void *next_remain_acc, void *buckets, uint32_t workers, uint32_t windows,
+                              uint32_t window_bits, uint32_t batch_size, cudaStream_t stream);
+
+/* src/cuda/bn254_c.rs:261-279, cuda/msm.cu:350-432.  Computes
+ * sum_i [s_i] p_i for array_len affine bases p and Montgomery-form scalars s
+ * and writes the Jacobian sum to res[0] (96 bytes).  res must span the
+ * reference's per-MSM region of (windows << window_bits) + 2 * workers
+ * Jacobian points and sort_buf 3 * array_len * windows u32 (the sizes
+ * src/cuda/msm.rs:297-317 allocates); both are used as scratch.  The other
+ * index buffers, threads, workers, the sort-storage size and skip_zero are
+ * accepted and unused.  Never blocks the host. */
+cudaError_t msm(void *res, void *p, void *s, void *indices_buf0, void *indices_buf1, void *indices_buf2,
+                void *indices_buf3, void *sort_buf, void *indices_buf, int array_len, int windows, int window_bits,
+                int threads, int workers, int prepared_sort_indices_temp_storage_bytes, int skip_zero,
+                cudaStream_t stream);
+
+/* src/cuda/bn254_c.rs:281-293, cuda/bn254.cu:1863-1912.  Builds a hash index
+ * of the table's usable rows in start_offset (2^(k+3) u32 available, as the
+ * reference allocates n Fr). Other buffers unused. */
+cudaError_t prepare_table_lookup(void *table, void *table_lowest_u32, void *sorted_table_lowest_u32, void *index,
+                                 void *sorted_index, void *start_offset, void *candidate_sort_temp_storage,
+                                 uint32_t candidate_sort_temp_storage_bytes, uint32_t k,
+                                 uint32_t unusable_rows_start, cudaStream_t stream);
+
+/* src/cuda/bn254_c.rs:295-308, cuda/bn254.cu:1796-1861.  m[row] += number of
+ * usable input rows equal to table[row], crediting the largest usable row
+ * among equal table values; matched_index holds the per-row counts. */
+cudaError_t calc_m(void *m, void *table, void *input, void *sorted_index, void *start_offset, void *matched_index,
+                   void *sorted_matched_index, void *candidate_sort_temp_storage,
+                   uint32_t candidate_sort_temp_storage_bytes, uint32_t k, uint32_t unusable_rows_start,
+                   cudaStream_t stream);
+
+/* ======================================================================
+ * Part 2: batched, allocation-free entry points
+ * ==================================================================== */
+
+/* Scratch bytes zkp_msm needs for n points with window_bits (0 = automatic). */
+size_t zkp_msm_scratch_bytes(uint32_t n, int window_bits);
+
+/* Window width zkp_msm picks for n points when window_bits is 0. */
+int zkp_msm_default_window(uint32_t n);
+
+/* One MSM: out (96-byte Jacobian) = sum_i [scalars_i] bases_i.  Replaces the
+ * msm + batch_msm_collect pair (src/cuda/msm.rs:239-455) without host
+ * synchronisation; capturable in a CUDA graph. */
+cudaError_t zkp_msm(void *out, const void *bases, const void *scalars, uint32_t n, int window_bits, void *scratch,
+                    size_t scratch_bytes, cudaStream_t stream);
+
+/* Batched NTT of ncols columns (column c at buf + c * col_stride elements)
+ * by the natural twiddle table `omegas` (2^log_n entries), optional output
+ * scale.  *result_in_tmp (host) tells whether the result is in tmp. */
+cudaError_t zkp_ntt_batch(void *buf, void *tmp, const void *omegas, const void *scale, int log_n, uint32_t ncols,
+                          size_t col_stride, int *result_in_tmp, cudaStream_t stream);
+
+/* out[i] = base * w^i for i < n (base and w device scalars). */
+cudaError_t zkp_powers(void *out, const void *base, const void *w, uint32_t n, cudaStream_t stream);
+
+/* Coset-extension twist tables: twist[j * n + k] = (shift * w_N^j)^k for
+ * j < 2^ext_bits, k < n = 2^log_n, where w_N is a primitive
+ * 2^(log_n + ext_bits)-th root of unity (device scalars shift and w_ext).
+ * Scratch: 2^ext_bits elements. */
+cudaError_t zkp_coset_twist_tables(void *twist, const void *shift, const void *w_ext, int log_n, int ext_bits,
+                                   void *scratch, cudaStream_t stream);
+
+/* Extended-domain phase for ncols columns of 2^log_n Lagrange values:
+ *   coeff = iNTT(lagrange)            (tw_inv = natural table of w_n^-1, n_inv)
+ *   ext[c][2^e * i + j] = NTT_n(coeff * twist_j)[i]
+ * i.e. ext is the evaluation on the coset shift * <w_N>, N = 2^(log_n + e), in
+ * natural order.  scratch: ncols * 2^e * n elements.  coeff_out may be NULL
+ * only when log_n <= 12 (one pass per transform).  Each stage is one launch
+ * over all columns.  stage_events (may be NULL) is an array of 5 cudaEvent_t
+ * recorded on `stream` before the first stage, between the stages and after
+ * the last, so a caller can time each stage. */
+cudaError_t zkp_extend_batch(void *ext_out, void *coeff_out, const void *lagrange_in, uint32_t ncols, int log_n,
+                             int ext_bits, const void *tw_inv, const void *n_inv, const void *tw, const void *twist,
+                             void *scratch, void *stage_events, cudaStream_t stream);
+
+/* out[i] = (accumulate ? out[i] : 0) + 1 / (in[i] + c[0]) (c may be NULL);
+ * zero maps to zero. out may alias in. */
+cudaError_t zkp_batch_inverse(void *out, const void *in, const void *c, uint32_t n, int accumulate,
+                              cudaStream_t stream);
+
+/* Scratch elements (32 bytes each) the prefix scans need for n elements. */
+size_t zkp_scan_scratch_elems(uint32_t n);
+
+/* Exclusive prefix product / sum with carried-in value (init may be NULL):
+ * out[i] = init (op) in[0] (op) ... (op) in[i-1]; out may alias in. */
+cudaError_t zkp_grand_product(void *out, const void *in, uint32_t n, const void *init, void *scratch,
+                              cudaStream_t stream);
+cudaError_t zkp_grand_sum(void *out, const void *in, uint32_t n, const void *init, void *scratch,
+                          cudaStream_t stream);
+
+/* Permutation argument, one chunk of ncols columns (src/permutation.rs:16-150):
+ * z[0] = *init, z[i+1] = z[i] * prod_c (v_c[i] + dbeta[c]*w^i + gamma) /
+ * (v_c[i] + beta*sigma_c[i] + gamma), with dbeta[c] = beta * delta^(offset+c).
+ * cols, sigmas: device arrays of ncols device pointers; omegas: w^i table. */
+cudaError_t zkp_permutation_z(void *z, const void *cols, const void *sigmas, int ncols, const void *beta,
+                              const void *gamma, const void *dbeta, const void *omegas, const void *init, uint32_t n,
+                              void *scratch, cudaStream_t stream);
+
+/* Shuffle argument (src/shuffle.rs:143-212): z[0] = 1,
+ * z[i+1] = z[i] * prod_g (input_g[i] + betas[g]) / prod_g (table_g[i] + betas[g]).
+ * scratch: n + zkp_scan_scratch_elems(n) elements. */
+cudaError_t zkp_shuffle_z(void *z, const void *inputs, const void *tables, const void *betas, int groups, uint32_t n,
+                          void *scratch, cudaStream_t stream);
+
+/* ======================================================================
+ * Part 3: calibration
+ * ==================================================================== */
+
+/* Runs blocks x 256 threads, each 4 independent chains of `iters` dependent
+ * Fr Montgomery products (4 * iters * blocks * 256 products in total); timed
+ * by the caller, this is the integer-pipe roofline denominator for the NTT
+ * and MSM kernels.  `out` (one element) is written only if the result is 0. */
+cudaError_t zkp_calib_mont_rate(void *out, uint32_t blocks, uint32_t iters, cudaStream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

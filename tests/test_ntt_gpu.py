@@ -1,0 +1,115 @@
+"""NTT parity on the GPU through the C ABI (ntt / expand_omega_buffer /
+extended_prepare as the reference's host calls them, src/cuda/ntt.rs), and the
+batched zkp_* transforms, against the oracle DFT bit for bit."""
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+
+def _omega_mont(O, log_n, inverse=False):
+    w = O.omega(log_n)
+    if inverse:
+        w = pow(w, -1, O.R_MOD)
+    return O.fr(w)
+
+
+@pytest.mark.parametrize("log_n", [1, 2, 3, 4, 5, 6, 7, 9, 10, 11, 12, 13, 15, 17, 20])
+def test_ntt_forward_and_inverse(O, gpu, log_n):
+    H = gpu.host
+    n = 1 << log_n
+    a = O.rand_fr(n, 1000 + log_n)
+    omegas, pq = H.generate_ntt_buffers(_omega_mont(O, log_n), log_n)
+    iomegas, ipq = H.generate_ntt_buffers(_omega_mont(O, log_n, True), log_n)
+    div = H.to_device(O.fr(pow(n, -1, O.R_MOD)))
+    s = H.to_device(a)
+    t = H.empty_fr(n)
+    s, t = H.ntt_raw(s, t, pq, omegas, log_n)
+    torch.cuda.synchronize()
+    assert (H.to_host(s) == O.ntt(a, log_n)).all()
+    s, t = H.ntt_raw(s, t, ipq, iomegas, log_n, intt_divisor=div)
+    torch.cuda.synchronize()
+    assert (H.to_host(s) == a).all()
+
+
+def test_ntt_reference_test_input(O, gpu):
+    # src/profile.rs:198-205: s_0 random, s_i = s_{i-1} + i, k = 22 in the reference
+    H = gpu.host
+    log_n = 16
+    s0 = O.fr_ints(O.rand_fr(1, 77))[0]
+    xs = [s0]
+    for i in range(1, 1 << log_n):
+        xs.append((xs[-1] + i) % O.R_MOD)
+    a = O.fr_vec(xs)
+    omegas, pq = H.generate_ntt_buffers(_omega_mont(O, log_n), log_n)
+    s, t = H.ntt_raw(H.to_device(a), H.empty_fr(1 << log_n), pq, omegas, log_n)
+    torch.cuda.synchronize()
+    assert (H.to_host(s) == O.ntt(a, log_n)).all()
+
+
+def test_expand_omega_buffer_natural(O, gpu):
+    H = gpu.host
+    for log_n in (1, 5, 11, 22):
+        buf = H.generate_omega_buffers(_omega_mont(O, log_n), log_n, True)
+        got = H.to_host(buf)
+        n = 1 << log_n
+        # spot check against w^i
+        idx = sorted({0, 1, 2, 3, n // 2, n - 1} | set(np.random.default_rng(1).integers(0, n, 50).tolist()))
+        w = O.omega(log_n)
+        for i in idx:
+            assert O.fr_ints(got[i])[0] == pow(w, i, O.R_MOD)
+
+
+def test_extended_prepare(O, gpu):
+    H = gpu.host
+    n, N = 1 << 10, 1 << 13
+    z = O.cube_roots_of_unity()[1]
+    cp = O.fr_vec([z, pow(z, 2, O.R_MOD)])
+    s = np.concatenate([O.rand_fr(n, 3), O.rand_fr(N - n, 4)])
+    d = H.to_device(s)
+    H.extended_prepare(d, H.to_device(cp), 3, n, N, False)
+    torch.cuda.synchronize()
+    assert (H.to_host(d) == O.extended_prepare(s, cp, 3, n, N, False)).all()
+    H.extended_prepare(d, H.to_device(cp), 3, n, N, True)
+    torch.cuda.synchronize()
+    exp = O.extended_prepare(O.extended_prepare(s, cp, 3, n, N, False), cp, 3, n, N, True)
+    assert (H.to_host(d) == exp).all()
+
+
+@pytest.mark.parametrize("log_n,ncols", [(6, 5), (12, 3), (14, 4), (18, 2)])
+def test_ntt_batch_columns(O, gpu, log_n, ncols):
+    H = gpu.host
+    n = 1 << log_n
+    a = O.rand_fr(n * ncols, 500 + log_n)
+    omegas = H.generate_omega_buffers(_omega_mont(O, log_n), log_n)
+    buf = H.to_device(a)
+    tmp = H.empty_fr(n * ncols)
+    out = H.ntt_batch(buf, tmp, omegas, log_n, ncols)
+    torch.cuda.synchronize()
+    got = H.to_host(out)
+    for c in range(ncols):
+        assert (got[c * n:(c + 1) * n] == O.ntt(a[c * n:(c + 1) * n], log_n)).all()
+
+
+@pytest.mark.parametrize("log_n,ext_bits,ncols", [(4, 3, 2), (10, 3, 3), (13, 3, 2), (16, 2, 2)])
+def test_extend_batch_matches_coset_ntt(O, gpu, log_n, ext_bits, ncols):
+    H = gpu.host
+    n = 1 << log_n
+    shift = 7  # the field's multiplicative generator
+    lag = O.rand_fr(n * ncols, 900 + log_n)
+    tw_inv = H.generate_omega_buffers(_omega_mont(O, log_n, True), log_n)
+    tw = H.generate_omega_buffers(_omega_mont(O, log_n), log_n)
+    n_inv = H.to_device(O.fr(pow(n, -1, O.R_MOD)))
+    twist = H.twist_tables(O.fr(shift), O.fr(O.omega(log_n + ext_bits)), log_n, ext_bits)
+    E = 1 << ext_bits
+    ext = H.empty_fr(ncols * E * n)
+    coeff = H.empty_fr(ncols * n)
+    scratch = H.empty_fr(ncols * E * n)
+    H.extend_batch(ext, coeff, H.to_device(lag), ncols, log_n, ext_bits, tw_inv, n_inv, tw, twist, scratch)
+    torch.cuda.synchronize()
+    ge, gc = H.to_host(ext), H.to_host(coeff)
+    for c in range(ncols):
+        co = O.intt(lag[c * n:(c + 1) * n], log_n)
+        assert (gc[c * n:(c + 1) * n] == co).all()
+        assert (ge[c * E * n:(c + 1) * E * n] == O.coset_ntt(co, log_n, log_n + ext_bits, shift)).all()

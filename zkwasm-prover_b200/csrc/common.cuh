@@ -1,0 +1,43 @@
+// Shared device helpers: 32-byte element loads/stores and launch checks.
+#pragma once
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include "field.cuh"
+
+namespace zk {
+
+template <class C>
+__device__ __forceinline__ Fe<C> ld_elem(const Fe<C>* p) {
+    const uint4* q = reinterpret_cast<const uint4*>(p);
+    uint4 a = q[0], b = q[1];
+    Fe<C> r;
+    r.v[0] = a.x; r.v[1] = a.y; r.v[2] = a.z; r.v[3] = a.w;
+    r.v[4] = b.x; r.v[5] = b.y; r.v[6] = b.z; r.v[7] = b.w;
+    return r;
+}
+
+// read-only path (input buffers that the kernel does not write)
+template <class C>
+__device__ __forceinline__ Fe<C> ldg_elem(const Fe<C>* p) {
+    const uint4* q = reinterpret_cast<const uint4*>(p);
+    uint4 a = __ldg(q), b = __ldg(q + 1);
+    Fe<C> r;
+    r.v[0] = a.x; r.v[1] = a.y; r.v[2] = a.z; r.v[3] = a.w;
+    r.v[4] = b.x; r.v[5] = b.y; r.v[6] = b.z; r.v[7] = b.w;
+    return r;
+}
+
+template <class C>
+__device__ __forceinline__ void st_elem(Fe<C>* p, const Fe<C>& v) {
+    uint4* q = reinterpret_cast<uint4*>(p);
+    q[0] = make_uint4(v.v[0], v.v[1], v.v[2], v.v[3]);
+    q[1] = make_uint4(v.v[4], v.v[5], v.v[6], v.v[7]);
+}
+
+}  // namespace zk
+
+#define ZK_CHECK(x)                           \
+    do {                                      \
+        cudaError_t err__ = (x);              \
+        if (err__ != cudaSuccess) return err__; \
+    } while (0)

@@ -1,0 +1,431 @@
+// Elementwise kernels of the quotient (eval_h) evaluation on the extended
+// domain, one thread per row, grid-stride, rotations taken modulo n.
+//
+// Reference kernels restated (cuda/bn254.cu): _field_op 585-639,
+// _field_op_batch_mul_sum 542-572, _extended_prepare 641-662,
+// _permutation_eval_h_p1/p2/l 664-765, _lookup_eval_h 798-865,
+// _logup_eval_h 867-921, _logup_eval_h_extra_inputs 924-948,
+// _shuffle_eval_h 975-1015, _shuffle_eval_h_v2 1017-1071, _field_mul_zip
+// 1121-1131, _field_sum 496-540, _shplonk_h_x_merge 1133-1149,
+// _logup_eval_h_inputs_product_sum 1172-1213.  The formulas are the same
+// polynomial identities; the launch shapes are not (the reference uses
+// 64-thread blocks and requires n to be a multiple of 64).
+#include "common.cuh"
+#include "kernels.h"
+
+namespace zk {
+
+static __device__ __forceinline__ uint32_t rot_idx(uint32_t i, int rot, uint32_t n) {
+    // (i + rot) mod n for any sign of rot; n need not be a power of two
+    long long r = ((long long)i + rot) % (long long)n;
+    if (r < 0) r += n;
+    return (uint32_t)r;
+}
+
+static __device__ __forceinline__ uint32_t rot_pow2(uint32_t i, int rot, uint32_t n) {
+    return (uint32_t)((int)i + rot) & (n - 1);
+}
+
+#define ZK_GRID_LOOP(i, n) \
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < (n); i += gridDim.x * blockDim.x)
+
+static inline unsigned grid_for(uint32_t n, unsigned tb = 256) {
+    uint64_t b = ((uint64_t)n + tb - 1) / tb;
+    if (b > 148u * 32u) b = 148u * 32u;
+    if (b == 0) b = 1;
+    return (unsigned)b;
+}
+
+// ------------------------------------------------------------------ field_op
+
+__global__ void field_op_kernel(Fr* res, const Fr* l, int l_rot, const Fr* l_c, const Fr* r, int r_rot,
+                                const Fr* r_c, uint32_t n, int op) {
+    ZK_GRID_LOOP(i, n) {
+        Fr fl, fr_;
+        if (l) {
+            fl = ld_elem<FrCfg>(l + rot_idx(i, l_rot, n));
+            if (l_c) fl = fe_mul<FrCfg>(fl, ld_elem<FrCfg>(l_c));
+        } else {
+            fl = ld_elem<FrCfg>(l_c);
+        }
+        if (r) {
+            fr_ = ld_elem<FrCfg>(r + rot_idx(i, r_rot, n));
+            if (r_c) fr_ = fe_mul<FrCfg>(fr_, ld_elem<FrCfg>(r_c));
+        } else if (r_c) {
+            fr_ = ld_elem<FrCfg>(r_c);
+        } else {
+            fr_ = fe_zero<FrCfg>();
+        }
+        Fr out;
+        if (op == 0)
+            out = fe_add<FrCfg>(fl, fr_);
+        else if (op == 1)
+            out = fe_mul<FrCfg>(fl, fr_);
+        else if (op == 2)
+            out = fl;
+        else
+            out = fe_sub<FrCfg>(fl, fr_);
+        st_elem<FrCfg>(res + i, out);
+    }
+}
+
+cudaError_t field_op(Fr* res, const Fr* l, int l_rot, const Fr* l_c, const Fr* r, int r_rot, const Fr* r_c,
+                     uint32_t n, int op, cudaStream_t s) {
+    if (op < 0 || op > 3) return cudaErrorInvalidValue;
+    if (n == 0) return cudaSuccess;
+    if (!l && !l_c) return cudaErrorInvalidValue;
+    // the rows are read rotated, so an in-place rotated operand needs a
+    // snapshot; the reference has the same hazard and callers avoid it
+    field_op_kernel<<<grid_for(n), 256, 0, s>>>(res, l, l_rot, l_c, r, r_rot, r_c, n, op);
+    return cudaGetLastError();
+}
+
+// --------------------------------------------------- field_op_batch_mul_sum
+// v = [coeff0, a00, a01, .., null, coeff1, a10, .., null, ...] (device array of
+// device pointers), rot = rotation per non-coefficient entry.
+
+__global__ void batch_mul_sum_kernel(Fr* res, Fr* const* v, const int* rot, int n_v, uint32_t n) {
+    ZK_GRID_LOOP(i, n) {
+        Fr acc = fe_zero<FrCfg>();
+        int vi = 0, ri = 0;
+        while (vi < n_v) {
+            Fr t = ld_elem<FrCfg>(v[vi++]);
+            while (vi < n_v && v[vi]) {
+                t = fe_mul<FrCfg>(t, ld_elem<FrCfg>(v[vi] + rot_pow2(i, rot[ri], n)));
+                vi++;
+                ri++;
+            }
+            acc = fe_add<FrCfg>(acc, t);
+            vi++;
+        }
+        st_elem<FrCfg>(res + i, fe_add<FrCfg>(ld_elem<FrCfg>(res + i), acc));
+    }
+}
+
+cudaError_t field_op_batch_mul_sum(Fr* res, Fr* const* v, const int* rot, int n_v, uint32_t n, cudaStream_t s) {
+    if (n == 0 || n_v <= 0) return cudaSuccess;
+    batch_mul_sum_kernel<<<grid_for(n), 256, 0, s>>>(res, v, rot, n_v, n);
+    return cudaGetLastError();
+}
+
+// ----------------------------------------------------------- extended_prepare
+
+__global__ void extended_prepare_kernel(Fr* s, const Fr* cp, uint32_t cpn, uint32_t n) {
+    ZK_GRID_LOOP(i, n) {
+        uint32_t k = i % cpn;
+        if (k != 0) st_elem<FrCfg>(s + i, fe_mul<FrCfg>(ld_elem<FrCfg>(s + i), ld_elem<FrCfg>(cp + k - 1)));
+    }
+}
+
+cudaError_t extended_prepare(Fr* s, const Fr* coset_powers, uint32_t cpn, uint32_t size, uint32_t ext_size,
+                             int to_coset, cudaStream_t st) {
+    if (cpn == 0) return cudaErrorInvalidValue;
+    uint32_t lim = size;
+    if (to_coset) {
+        lim = ext_size;
+    } else if (ext_size > size) {
+        ZK_CHECK(cudaMemsetAsync(s + size, 0, (size_t)(ext_size - size) * sizeof(Fr), st));
+    }
+    if (lim == 0 || cpn == 1) return cudaGetLastError();
+    extended_prepare_kernel<<<grid_for(lim), 256, 0, st>>>(s, coset_powers, cpn, lim);
+    return cudaGetLastError();
+}
+
+// --------------------------------------------------------------- permutation
+
+__global__ void perm_p1_kernel(Fr* res, const Fr* first, const Fr* last, const Fr* l0, const Fr* l_last,
+                               const Fr* y, uint32_t n) {
+    const Fr yy = ld_elem<FrCfg>(y);
+    const Fr one = fe_one<FrCfg>();
+    ZK_GRID_LOOP(i, n) {
+        Fr t1 = fe_mul<FrCfg>(ld_elem<FrCfg>(res + i), yy);
+        Fr t2 = fe_mul<FrCfg>(fe_sub<FrCfg>(one, ld_elem<FrCfg>(first + i)), ld_elem<FrCfg>(l0 + i));
+        t1 = fe_mul<FrCfg>(fe_add<FrCfg>(t1, t2), yy);
+        Fr z = ld_elem<FrCfg>(last + i);
+        t2 = fe_mul<FrCfg>(fe_sub<FrCfg>(fe_sqr<FrCfg>(z), z), ld_elem<FrCfg>(l_last + i));
+        st_elem<FrCfg>(res + i, fe_add<FrCfg>(t1, t2));
+    }
+}
+
+cudaError_t permutation_eval_h_p1(Fr* res, const Fr* first_set, const Fr* last_set, const Fr* l0,
+                                  const Fr* l_last, const Fr* y, uint32_t n, cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    perm_p1_kernel<<<grid_for(n), 256, 0, s>>>(res, first_set, last_set, l0, l_last, y, n);
+    return cudaGetLastError();
+}
+
+__global__ void perm_p2_kernel(Fr* res, const Fr* const* set, const Fr* l0, const Fr* y, int n_set, int rot,
+                               uint32_t n) {
+    const Fr yy = ld_elem<FrCfg>(y);
+    ZK_GRID_LOOP(i, n) {
+        const uint32_t rp = rot_pow2(i, rot, n);
+        Fr t1 = ld_elem<FrCfg>(res + i);
+        const Fr l = ld_elem<FrCfg>(l0 + i);
+        for (int j = 1; j < n_set; j++) {
+            t1 = fe_mul<FrCfg>(t1, yy);
+            Fr t2 = fe_sub<FrCfg>(ld_elem<FrCfg>(set[j] + i), ld_elem<FrCfg>(set[j - 1] + rp));
+            t1 = fe_add<FrCfg>(t1, fe_mul<FrCfg>(t2, l));
+        }
+        st_elem<FrCfg>(res + i, t1);
+    }
+}
+
+cudaError_t permutation_eval_h_p2(Fr* res, const Fr* const* set, const Fr* l0, const Fr* y, int n_set, int rot,
+                                  uint32_t n, cudaStream_t s) {
+    if (n == 0 || n_set < 2) return cudaSuccess;
+    perm_p2_kernel<<<grid_for(n), 256, 0, s>>>(res, set, l0, y, n_set, rot, n);
+    return cudaGetLastError();
+}
+
+__global__ void perm_l_kernel(Fr* res, const Fr* beta, const Fr* gamma, const Fr* p, uint32_t n) {
+    const Fr b = ld_elem<FrCfg>(beta);
+    ZK_GRID_LOOP(i, n) {
+        Fr t = fe_mul<FrCfg>(ld_elem<FrCfg>(p + i), b);
+        if (i == 0) t = fe_add<FrCfg>(t, ld_elem<FrCfg>(gamma));
+        st_elem<FrCfg>(res + i, fe_add<FrCfg>(ld_elem<FrCfg>(res + i), t));
+    }
+}
+
+cudaError_t permutation_eval_h_l(Fr* res, const Fr* beta, const Fr* gamma, const Fr* p, uint32_t n,
+                                 cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    perm_l_kernel<<<grid_for(n), 256, 0, s>>>(res, beta, gamma, p, n);
+    return cudaGetLastError();
+}
+
+// --------------------------------------------------------------------- lookup
+
+__global__ void lookup_kernel(Fr* res, const Fr* input, const Fr* table, const Fr* pin, const Fr* ptab,
+                              const Fr* z, const Fr* l0, const Fr* l_last, const Fr* l_act, const Fr* y,
+                              const Fr* beta, const Fr* gamma, int rot, uint32_t n) {
+    const Fr yy = ld_elem<FrCfg>(y), bb = ld_elem<FrCfg>(beta), gg = ld_elem<FrCfg>(gamma);
+    const Fr one = fe_one<FrCfg>();
+    ZK_GRID_LOOP(i, n) {
+        const uint32_t rn = rot_pow2(i, rot, n), rp = rot_pow2(i, -rot, n);
+        const Fr zi = ld_elem<FrCfg>(z + i);
+        Fr t = fe_mul<FrCfg>(ld_elem<FrCfg>(res + i), yy);
+        t = fe_add<FrCfg>(t, fe_mul<FrCfg>(ld_elem<FrCfg>(l0 + i), fe_sub<FrCfg>(one, zi)));
+        t = fe_mul<FrCfg>(t, yy);
+        t = fe_add<FrCfg>(t, fe_mul<FrCfg>(ld_elem<FrCfg>(l_last + i), fe_sub<FrCfg>(fe_sqr<FrCfg>(zi), zi)));
+        t = fe_mul<FrCfg>(t, yy);
+        const Fr a = ld_elem<FrCfg>(pin + i), sv = ld_elem<FrCfg>(ptab + i);
+        Fr u = fe_mul<FrCfg>(fe_add<FrCfg>(a, bb), fe_add<FrCfg>(sv, gg));
+        u = fe_mul<FrCfg>(u, ld_elem<FrCfg>(z + rn));
+        Fr x = fe_mul<FrCfg>(ld_elem<FrCfg>(input + i), ld_elem<FrCfg>(table + i));
+        u = fe_sub<FrCfg>(u, fe_mul<FrCfg>(zi, x));
+        t = fe_add<FrCfg>(t, fe_mul<FrCfg>(u, ld_elem<FrCfg>(l_act + i)));
+        t = fe_mul<FrCfg>(t, yy);
+        const Fr p = fe_sub<FrCfg>(a, sv);
+        t = fe_add<FrCfg>(t, fe_mul<FrCfg>(ld_elem<FrCfg>(l0 + i), p));
+        t = fe_mul<FrCfg>(t, yy);
+        u = fe_mul<FrCfg>(fe_sub<FrCfg>(a, ld_elem<FrCfg>(pin + rp)), p);
+        t = fe_add<FrCfg>(t, fe_mul<FrCfg>(u, ld_elem<FrCfg>(l_act + i)));
+        st_elem<FrCfg>(res + i, t);
+    }
+}
+
+cudaError_t lookup_eval_h(Fr* res, const Fr* input, const Fr* table, const Fr* permuted_input,
+                          const Fr* permuted_table, const Fr* z, const Fr* l0, const Fr* l_last,
+                          const Fr* l_active_row, const Fr* y, const Fr* beta, const Fr* gamma, int rot, uint32_t n,
+                          cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    lookup_kernel<<<grid_for(n), 256, 0, s>>>(res, input, table, permuted_input, permuted_table, z, l0, l_last,
+                                              l_active_row, y, beta, gamma, rot, n);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------- logup
+
+__global__ void logup_kernel(Fr* res, const Fr* ip, const Fr* ips, const Fr* table, const Fr* m, const Fr* zf,
+                             const Fr* zl, const Fr* l0, const Fr* l_last, const Fr* l_act, const Fr* y, int rot,
+                             uint32_t n) {
+    const Fr yy = ld_elem<FrCfg>(y);
+    ZK_GRID_LOOP(i, n) {
+        const uint32_t rn = rot_pow2(i, rot, n);
+        const Fr z = ld_elem<FrCfg>(zf + i);
+        Fr t = fe_mul<FrCfg>(ld_elem<FrCfg>(res + i), yy);
+        t = fe_add<FrCfg>(t, fe_mul<FrCfg>(ld_elem<FrCfg>(l0 + i), z));
+        t = fe_mul<FrCfg>(t, yy);
+        t = fe_add<FrCfg>(t, fe_mul<FrCfg>(ld_elem<FrCfg>(l_last + i), ld_elem<FrCfg>(zl + i)));
+        t = fe_mul<FrCfg>(t, yy);
+        const Fr tab = ld_elem<FrCfg>(table + i);
+        Fr u = fe_mul<FrCfg>(fe_sub<FrCfg>(ld_elem<FrCfg>(zf + rn), z), tab);
+        u = fe_add<FrCfg>(u, ld_elem<FrCfg>(m + i));
+        u = fe_mul<FrCfg>(u, ld_elem<FrCfg>(ip + i));
+        u = fe_sub<FrCfg>(u, fe_mul<FrCfg>(tab, ld_elem<FrCfg>(ips + i)));
+        t = fe_add<FrCfg>(t, fe_mul<FrCfg>(u, ld_elem<FrCfg>(l_act + i)));
+        st_elem<FrCfg>(res + i, t);
+    }
+}
+
+cudaError_t logup_eval_h(Fr* res, const Fr* input_product, const Fr* input_product_sum, const Fr* table,
+                         const Fr* multiplicity, const Fr* z_first, const Fr* z_last, const Fr* l0,
+                         const Fr* l_last, const Fr* l_active_row, const Fr* y, int rot, uint32_t n, cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    logup_kernel<<<grid_for(n), 256, 0, s>>>(res, input_product, input_product_sum, table, multiplicity, z_first,
+                                             z_last, l0, l_last, l_active_row, y, rot, n);
+    return cudaGetLastError();
+}
+
+__global__ void logup_extra_kernel(Fr* res, const Fr* ip, const Fr* ips, const Fr* z, const Fr* l_act,
+                                   const Fr* y, int rot, uint32_t n) {
+    const Fr yy = ld_elem<FrCfg>(y);
+    ZK_GRID_LOOP(i, n) {
+        const uint32_t rn = rot_pow2(i, rot, n);
+        Fr t = fe_mul<FrCfg>(ld_elem<FrCfg>(res + i), yy);
+        Fr u = fe_sub<FrCfg>(ld_elem<FrCfg>(z + rn), ld_elem<FrCfg>(z + i));
+        u = fe_mul<FrCfg>(u, ld_elem<FrCfg>(ip + i));
+        u = fe_sub<FrCfg>(u, ld_elem<FrCfg>(ips + i));
+        t = fe_add<FrCfg>(t, fe_mul<FrCfg>(u, ld_elem<FrCfg>(l_act + i)));
+        st_elem<FrCfg>(res + i, t);
+    }
+}
+
+cudaError_t logup_eval_h_extra_inputs(Fr* res, const Fr* input_product, const Fr* input_product_sum, const Fr* z,
+                                      const Fr* l_active_row, const Fr* y, int rot, uint32_t n, cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    logup_extra_kernel<<<grid_for(n), 256, 0, s>>>(res, input_product, input_product_sum, z, l_active_row, y, rot,
+                                                   n);
+    return cudaGetLastError();
+}
+
+__global__ void inputs_product_sum_kernel(Fr* prod, Fr* psum, const Fr* const* set, int n_set, uint32_t n) {
+    ZK_GRID_LOOP(i, n) {
+        // prefix and suffix products give every leave-one-out product in 3k mults
+        Fr p = fe_one<FrCfg>();
+        Fr sum = fe_zero<FrCfg>();
+        // running: sum_{j<k} prod_{l<=k, l!=j} a_l  updated as sum = sum * a_k + p_{k-1}
+        for (int k = 0; k < n_set; k++) {
+            const Fr a = ld_elem<FrCfg>(set[k] + i);
+            sum = fe_add<FrCfg>(fe_mul<FrCfg>(sum, a), p);
+            p = fe_mul<FrCfg>(p, a);
+        }
+        st_elem<FrCfg>(prod + i, p);
+        st_elem<FrCfg>(psum + i, sum);
+    }
+}
+
+cudaError_t logup_eval_h_inputs_product_sum(Fr* product, Fr* product_sum, const Fr* const* set, int n_set,
+                                            uint32_t n, cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    inputs_product_sum_kernel<<<grid_for(n), 256, 0, s>>>(product, product_sum, set, n_set, n);
+    return cudaGetLastError();
+}
+
+// -------------------------------------------------------------------- shuffle
+
+__device__ __forceinline__ Fr shuffle_tail(Fr t, const Fr& yy, const Fr& zi, const Fr& zn, const Fr& l0,
+                                           const Fr& ll, const Fr& la, const Fr& lhs, const Fr& rhs) {
+    const Fr one = fe_one<FrCfg>();
+    t = fe_mul<FrCfg>(t, yy);
+    t = fe_add<FrCfg>(t, fe_mul<FrCfg>(l0, fe_sub<FrCfg>(one, zi)));
+    t = fe_mul<FrCfg>(t, yy);
+    t = fe_add<FrCfg>(t, fe_mul<FrCfg>(ll, fe_sub<FrCfg>(fe_sqr<FrCfg>(zi), zi)));
+    t = fe_mul<FrCfg>(t, yy);
+    Fr u = fe_sub<FrCfg>(fe_mul<FrCfg>(rhs, zn), fe_mul<FrCfg>(lhs, zi));
+    return fe_add<FrCfg>(t, fe_mul<FrCfg>(u, la));
+}
+
+__global__ void shuffle_kernel(Fr* res, const Fr* input, const Fr* table, const Fr* z, const Fr* l0,
+                               const Fr* l_last, const Fr* l_act, const Fr* y, int rot, uint32_t n) {
+    const Fr yy = ld_elem<FrCfg>(y);
+    ZK_GRID_LOOP(i, n) {
+        const uint32_t rn = rot_pow2(i, rot, n);
+        Fr t = shuffle_tail(ld_elem<FrCfg>(res + i), yy, ld_elem<FrCfg>(z + i), ld_elem<FrCfg>(z + rn),
+                            ld_elem<FrCfg>(l0 + i), ld_elem<FrCfg>(l_last + i), ld_elem<FrCfg>(l_act + i),
+                            ld_elem<FrCfg>(input + i), ld_elem<FrCfg>(table + i));
+        st_elem<FrCfg>(res + i, t);
+    }
+}
+
+cudaError_t shuffle_eval_h(Fr* res, const Fr* input, const Fr* table, const Fr* z, const Fr* l0, const Fr* l_last,
+                           const Fr* l_active_row, const Fr* y, int rot, uint32_t n, cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    shuffle_kernel<<<grid_for(n), 256, 0, s>>>(res, input, table, z, l0, l_last, l_active_row, y, rot, n);
+    return cudaGetLastError();
+}
+
+__global__ void shuffle_v2_kernel(Fr* res, const Fr* const* inputs, const Fr* const* tables, const Fr* betas,
+                                  int group_len, const Fr* z, const Fr* l0, const Fr* l_last, const Fr* l_act,
+                                  const Fr* y, int rot, uint32_t n) {
+    const Fr yy = ld_elem<FrCfg>(y);
+    ZK_GRID_LOOP(i, n) {
+        const uint32_t rn = rot_pow2(i, rot, n);
+        Fr b = ld_elem<FrCfg>(betas);
+        Fr l = fe_add<FrCfg>(ld_elem<FrCfg>(inputs[0] + i), b);
+        Fr r = fe_add<FrCfg>(ld_elem<FrCfg>(tables[0] + i), b);
+        for (int j = 1; j < group_len; j++) {
+            b = ld_elem<FrCfg>(betas + j);
+            l = fe_mul<FrCfg>(l, fe_add<FrCfg>(ld_elem<FrCfg>(inputs[j] + i), b));
+            r = fe_mul<FrCfg>(r, fe_add<FrCfg>(ld_elem<FrCfg>(tables[j] + i), b));
+        }
+        Fr t = shuffle_tail(ld_elem<FrCfg>(res + i), yy, ld_elem<FrCfg>(z + i), ld_elem<FrCfg>(z + rn),
+                            ld_elem<FrCfg>(l0 + i), ld_elem<FrCfg>(l_last + i), ld_elem<FrCfg>(l_act + i), l, r);
+        st_elem<FrCfg>(res + i, t);
+    }
+}
+
+cudaError_t shuffle_eval_h_v2(Fr* res, const Fr* const* inputs, const Fr* const* tables, const Fr* betas,
+                              int group_len, const Fr* z, const Fr* l0, const Fr* l_last, const Fr* l_active_row,
+                              const Fr* y, int rot, uint32_t n, cudaStream_t s) {
+    if (n == 0 || group_len <= 0) return cudaSuccess;
+    shuffle_v2_kernel<<<grid_for(n), 256, 0, s>>>(res, inputs, tables, betas, group_len, z, l0, l_last,
+                                                  l_active_row, y, rot, n);
+    return cudaGetLastError();
+}
+
+// --------------------------------------------------------------- small maps
+
+__global__ void mul_zip_kernel(Fr* buf, const Fr* coeff, uint32_t coeff_n, uint32_t n) {
+    ZK_GRID_LOOP(i, n) {
+        st_elem<FrCfg>(buf + i, fe_mul<FrCfg>(ld_elem<FrCfg>(buf + i), ld_elem<FrCfg>(coeff + i % coeff_n)));
+    }
+}
+
+cudaError_t field_mul_zip(Fr* buf, const Fr* coeff, uint32_t coeff_n, uint32_t n, cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    if (coeff_n == 0) return cudaErrorInvalidValue;
+    mul_zip_kernel<<<grid_for(n), 256, 0, s>>>(buf, coeff, coeff_n, n);
+    return cudaGetLastError();
+}
+
+__global__ void field_sum_kernel(Fr* res, Fr* const* v, Fr* const* v_c, const int* v_rot, const Fr* omegas,
+                                 int v_n, uint32_t n) {
+    ZK_GRID_LOOP(i, n) {
+        Fr acc = fe_zero<FrCfg>();
+        for (int j = 0; j < v_n; j++) {
+            const uint32_t e = (uint32_t)(((long long)((int)n + v_rot[j]) * (long long)i) & (long long)(n - 1));
+            Fr t = fe_mul<FrCfg>(ld_elem<FrCfg>(v[j] + i), ld_elem<FrCfg>(omegas + e));
+            if (v_c[j]) t = fe_mul<FrCfg>(t, ld_elem<FrCfg>(v_c[j]));
+            acc = (j == 0) ? t : fe_add<FrCfg>(acc, t);
+        }
+        st_elem<FrCfg>(res + i, acc);
+    }
+}
+
+cudaError_t field_sum(Fr* res, Fr* const* v, Fr* const* v_c, const int* v_rot, const Fr* omegas, int v_n,
+                      uint32_t n, cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    field_sum_kernel<<<grid_for(n), 256, 0, s>>>(res, v, v_c, v_rot, omegas, v_n, n);
+    return cudaGetLastError();
+}
+
+__global__ void shplonk_merge_kernel(Fr* res, const Fr* v, const Fr* values, const Fr* omegas, const Fr* diff,
+                                     int nd, uint32_t n) {
+    const Fr vv = ld_elem<FrCfg>(v);
+    ZK_GRID_LOOP(i, n) {
+        Fr t = ld_elem<FrCfg>(values + i);
+        const Fr w = ld_elem<FrCfg>(omegas + i);
+        for (int j = 0; j < nd; j++) t = fe_mul<FrCfg>(t, fe_sub<FrCfg>(w, ld_elem<FrCfg>(diff + j)));
+        st_elem<FrCfg>(res + i, fe_add<FrCfg>(fe_mul<FrCfg>(ld_elem<FrCfg>(res + i), vv), t));
+    }
+}
+
+cudaError_t shplonk_h_x_merge(Fr* res, const Fr* v, const Fr* values, const Fr* omegas, const Fr* diff_points,
+                              int diff_points_n, uint32_t n, cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    shplonk_merge_kernel<<<grid_for(n), 256, 0, s>>>(res, v, values, omegas, diff_points, diff_points_n, n);
+    return cudaGetLastError();
+}
+
+}  // namespace zk

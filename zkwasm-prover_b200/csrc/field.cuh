@@ -1,0 +1,378 @@
+// BN254 prime-field arithmetic for sm_100a: 8 x 32-bit limbs, Montgomery form
+// with R = 2^256.  In memory an element is 32 bytes, little-endian, which is
+// byte-identical to halo2's 4 x u64 layout (reference: cuda/zprize/ff_storage.cuh,
+// src/cuda/msm.rs:441-452), so device buffers are shared with the Rust host
+// unchanged.
+//
+// Multiplication is operand-scanning Montgomery multiplication (Montgomery,
+// "Modular multiplication without trial division", 1985) with the reduction
+// interleaved row by row.  Each row is two carry chains of mad.lo / mad.hi on
+// the integer multiply-add pipe; every chain is one inline-PTX block so the
+// carry flag never crosses an asm statement.  On the host the same chains are
+// emulated in plain C, which lets the CPU test-suite run the exact operation
+// sequence of the device code against the oracle.
+//
+// Bounds: with m < 2^254, inputs a, b < 2m give a 9-word accumulator that never
+// overflows (intermediates stay below 4m * 2^32 < 2^288) and a pre-subtraction
+// result below 2m; one conditional subtraction then returns a value below m.
+#pragma once
+#include <stdint.h>
+
+#if defined(__CUDACC__)
+#define ZK_HD __host__ __device__ __forceinline__
+#else
+#define ZK_HD inline
+#endif
+
+namespace zk {
+
+// pick j-th of eight constants; folds to an immediate when j is a compile-time constant
+ZK_HD constexpr uint32_t pick8(int j, uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, uint32_t a4, uint32_t a5,
+                               uint32_t a6, uint32_t a7) {
+    return j == 0 ? a0 : j == 1 ? a1 : j == 2 ? a2 : j == 3 ? a3 : j == 4 ? a4 : j == 5 ? a5 : j == 6 ? a6 : a7;
+}
+
+struct FrCfg {
+    // r = 0x30644e72e131a029b85045b68181585d2833e84879b9709143e1f593f0000001
+    static ZK_HD constexpr uint32_t M(int j) {
+        return pick8(j, 0xf0000001u, 0x43e1f593u, 0x79b97091u, 0x2833e848u, 0x8181585du, 0xb85045b6u, 0xe131a029u,
+                     0x30644e72u);
+    }
+    static constexpr uint32_t INV = 0xefffffffu;  // -r^-1 mod 2^32
+    static ZK_HD constexpr uint32_t ONE(int j) {  // 2^256 mod r
+        return pick8(j, 0x4ffffffbu, 0xac96341cu, 0x9f60cd29u, 0x36fc7695u, 0x7879462eu, 0x666ea36fu, 0x9a07df2fu,
+                     0x0e0a77c1u);
+    }
+    static ZK_HD constexpr uint32_t R2(int j) {  // 2^512 mod r
+        return pick8(j, 0xae216da7u, 0x1bb8e645u, 0xe35c59e3u, 0x53fe3ab1u, 0x53bb8085u, 0x8c49833du, 0x7f4e44a5u,
+                     0x0216d0b1u);
+    }
+};
+
+struct FqCfg {
+    // p = 0x30644e72e131a029b85045b68181585d97816a916871ca8d3c208c16d87cfd47
+    static ZK_HD constexpr uint32_t M(int j) {
+        return pick8(j, 0xd87cfd47u, 0x3c208c16u, 0x6871ca8du, 0x97816a91u, 0x8181585du, 0xb85045b6u, 0xe131a029u,
+                     0x30644e72u);
+    }
+    static constexpr uint32_t INV = 0xe4866389u;  // -p^-1 mod 2^32
+    static ZK_HD constexpr uint32_t ONE(int j) {
+        return pick8(j, 0xc58f0d9du, 0xd35d438du, 0xf5c70b3du, 0x0a78eb28u, 0x7879462cu, 0x666ea36fu, 0x9a07df2fu,
+                     0x0e0a77c1u);
+    }
+    static ZK_HD constexpr uint32_t R2(int j) {
+        return pick8(j, 0x538afa89u, 0xf32cfc5bu, 0xd44501fbu, 0xb5e71911u, 0x0a417ff6u, 0x47ab1effu, 0xcab8351fu,
+                     0x06d89f71u);
+    }
+};
+
+template <class C>
+struct alignas(16) Fe {
+    uint32_t v[8];
+};
+
+typedef Fe<FrCfg> Fr;
+typedef Fe<FqCfg> Fq;
+
+// ---------------------------------------------------------------------------
+// carry-chain building blocks (device: PTX; host: C emulation of the same ops)
+
+// t[0..8] += a[0..7] * b   (lo chain then hi chain; t[8] absorbs the carries)
+ZK_HD void row_mad(uint32_t t[9], const uint32_t a[8], uint32_t b) {
+#if defined(__CUDA_ARCH__)
+    asm("mad.lo.cc.u32  %0, %9,  %17, %0;\n\t"
+        "madc.lo.cc.u32 %1, %10, %17, %1;\n\t"
+        "madc.lo.cc.u32 %2, %11, %17, %2;\n\t"
+        "madc.lo.cc.u32 %3, %12, %17, %3;\n\t"
+        "madc.lo.cc.u32 %4, %13, %17, %4;\n\t"
+        "madc.lo.cc.u32 %5, %14, %17, %5;\n\t"
+        "madc.lo.cc.u32 %6, %15, %17, %6;\n\t"
+        "madc.lo.cc.u32 %7, %16, %17, %7;\n\t"
+        "addc.u32       %8, %8, 0;\n\t"
+        "mad.hi.cc.u32  %1, %9,  %17, %1;\n\t"
+        "madc.hi.cc.u32 %2, %10, %17, %2;\n\t"
+        "madc.hi.cc.u32 %3, %11, %17, %3;\n\t"
+        "madc.hi.cc.u32 %4, %12, %17, %4;\n\t"
+        "madc.hi.cc.u32 %5, %13, %17, %5;\n\t"
+        "madc.hi.cc.u32 %6, %14, %17, %6;\n\t"
+        "madc.hi.cc.u32 %7, %15, %17, %7;\n\t"
+        "madc.hi.u32    %8, %16, %17, %8;"
+        : "+r"(t[0]), "+r"(t[1]), "+r"(t[2]), "+r"(t[3]), "+r"(t[4]), "+r"(t[5]), "+r"(t[6]),
+          "+r"(t[7]), "+r"(t[8])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(a[4]), "r"(a[5]), "r"(a[6]), "r"(a[7]),
+          "r"(b));
+#else
+    uint64_t c = 0;
+    for (int j = 0; j < 8; j++) {
+        uint64_t s = (uint64_t)(uint32_t)((uint64_t)a[j] * b) + t[j] + c;
+        t[j] = (uint32_t)s;
+        c = s >> 32;
+    }
+    t[8] = (uint32_t)(t[8] + c);
+    c = 0;
+    for (int j = 0; j < 8; j++) {
+        uint64_t s = (uint64_t)(uint32_t)(((uint64_t)a[j] * b) >> 32) + t[j + 1] + c;
+        t[j + 1] = (uint32_t)s;
+        c = s >> 32;
+    }
+#endif
+}
+
+// r = t - m (8 words) and returns the borrow mask (0 or 0xffffffff)
+ZK_HD uint32_t sub8_borrow(uint32_t r[8], const uint32_t t[8], const uint32_t m[8]) {
+#if defined(__CUDA_ARCH__)
+    uint32_t br;
+    asm("sub.cc.u32  %0, %9,  %17;\n\t"
+        "subc.cc.u32 %1, %10, %18;\n\t"
+        "subc.cc.u32 %2, %11, %19;\n\t"
+        "subc.cc.u32 %3, %12, %20;\n\t"
+        "subc.cc.u32 %4, %13, %21;\n\t"
+        "subc.cc.u32 %5, %14, %22;\n\t"
+        "subc.cc.u32 %6, %15, %23;\n\t"
+        "subc.cc.u32 %7, %16, %24;\n\t"
+        "subc.u32    %8, 0, 0;"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7]), "=r"(br)
+        : "r"(t[0]), "r"(t[1]), "r"(t[2]), "r"(t[3]), "r"(t[4]), "r"(t[5]), "r"(t[6]), "r"(t[7]),
+          "r"(m[0]), "r"(m[1]), "r"(m[2]), "r"(m[3]), "r"(m[4]), "r"(m[5]), "r"(m[6]), "r"(m[7]));
+    return br;
+#else
+    uint64_t b = 0;
+    for (int j = 0; j < 8; j++) {
+        uint64_t d = (uint64_t)t[j] - m[j] - b;
+        r[j] = (uint32_t)d;
+        b = (d >> 63) & 1;
+    }
+    return b ? 0xffffffffu : 0u;
+#endif
+}
+
+// r = a + b (8 words), returns carry (0/1)
+ZK_HD uint32_t add8_carry(uint32_t r[8], const uint32_t a[8], const uint32_t b[8]) {
+#if defined(__CUDA_ARCH__)
+    uint32_t c;
+    asm("add.cc.u32  %0, %9,  %17;\n\t"
+        "addc.cc.u32 %1, %10, %18;\n\t"
+        "addc.cc.u32 %2, %11, %19;\n\t"
+        "addc.cc.u32 %3, %12, %20;\n\t"
+        "addc.cc.u32 %4, %13, %21;\n\t"
+        "addc.cc.u32 %5, %14, %22;\n\t"
+        "addc.cc.u32 %6, %15, %23;\n\t"
+        "addc.cc.u32 %7, %16, %24;\n\t"
+        "addc.u32    %8, 0, 0;"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7]), "=r"(c)
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(a[4]), "r"(a[5]), "r"(a[6]), "r"(a[7]),
+          "r"(b[0]), "r"(b[1]), "r"(b[2]), "r"(b[3]), "r"(b[4]), "r"(b[5]), "r"(b[6]), "r"(b[7]));
+    return c;
+#else
+    uint64_t c = 0;
+    for (int j = 0; j < 8; j++) {
+        uint64_t s = (uint64_t)a[j] + b[j] + c;
+        r[j] = (uint32_t)s;
+        c = s >> 32;
+    }
+    return (uint32_t)c;
+#endif
+}
+
+// r = mask ? a : b  (mask is 0 or all ones)
+ZK_HD void select8(uint32_t r[8], uint32_t mask, const uint32_t a[8], const uint32_t b[8]) {
+#pragma unroll
+    for (int j = 0; j < 8; j++) r[j] = b[j] ^ ((a[j] ^ b[j]) & mask);
+}
+
+// ---------------------------------------------------------------------------
+// field operations
+
+template <class C>
+ZK_HD Fe<C> fe_zero() {
+    Fe<C> r;
+#pragma unroll
+    for (int j = 0; j < 8; j++) r.v[j] = 0;
+    return r;
+}
+
+template <class C>
+ZK_HD Fe<C> fe_one() {
+    Fe<C> r;
+#pragma unroll
+    for (int j = 0; j < 8; j++) r.v[j] = C::ONE(j);
+    return r;
+}
+
+template <class C>
+ZK_HD Fe<C> fe_modulus() {
+    Fe<C> r;
+#pragma unroll
+    for (int j = 0; j < 8; j++) r.v[j] = C::M(j);
+    return r;
+}
+
+// Conditional subtraction of m: input < 2m, output < m.
+template <class C>
+ZK_HD void fe_reduce_once(uint32_t t[8]) {
+    uint32_t u[8], m[8];
+#pragma unroll
+    for (int j = 0; j < 8; j++) m[j] = C::M(j);
+    uint32_t br = sub8_borrow(u, t, m);
+    select8(t, br, t, u);
+}
+
+// Montgomery product a * b * 2^-256 mod m; a, b < 2m, result < m.
+template <class C>
+ZK_HD Fe<C> fe_mul(const Fe<C>& a, const Fe<C>& b) {
+    uint32_t t[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    uint32_t m[8];
+#pragma unroll
+    for (int j = 0; j < 8; j++) m[j] = C::M(j);
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        row_mad(t, a.v, b.v[i]);
+        uint32_t q = t[0] * C::INV;
+        row_mad(t, m, q);
+        // t[0] is now zero: shift one word down
+#pragma unroll
+        for (int j = 0; j < 8; j++) t[j] = t[j + 1];
+        t[8] = 0;
+    }
+    fe_reduce_once<C>(t);
+    Fe<C> r;
+#pragma unroll
+    for (int j = 0; j < 8; j++) r.v[j] = t[j];
+    return r;
+}
+
+template <class C>
+ZK_HD Fe<C> fe_sqr(const Fe<C>& a) {
+    return fe_mul<C>(a, a);
+}
+
+// Montgomery reduction only: a * 2^-256 mod m (leaves Montgomery form).
+template <class C>
+ZK_HD Fe<C> fe_from_mont(const Fe<C>& a) {
+    uint32_t t[9];
+    uint32_t m[8];
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+        m[j] = C::M(j);
+        t[j] = a.v[j];
+    }
+    t[8] = 0;
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        uint32_t q = t[0] * C::INV;
+        row_mad(t, m, q);
+#pragma unroll
+        for (int j = 0; j < 8; j++) t[j] = t[j + 1];
+        t[8] = 0;
+    }
+    fe_reduce_once<C>(t);
+    Fe<C> r;
+#pragma unroll
+    for (int j = 0; j < 8; j++) r.v[j] = t[j];
+    return r;
+}
+
+template <class C>
+ZK_HD Fe<C> fe_to_mont(const Fe<C>& a) {
+    Fe<C> r2;
+#pragma unroll
+    for (int j = 0; j < 8; j++) r2.v[j] = C::R2(j);
+    return fe_mul<C>(a, r2);
+}
+
+// a + b mod m for a, b < m
+template <class C>
+ZK_HD Fe<C> fe_add(const Fe<C>& a, const Fe<C>& b) {
+    Fe<C> r;
+    add8_carry(r.v, a.v, b.v);
+    fe_reduce_once<C>(r.v);
+    return r;
+}
+
+// a - b mod m for a, b < m
+template <class C>
+ZK_HD Fe<C> fe_sub(const Fe<C>& a, const Fe<C>& b) {
+    uint32_t t[8], u[8], m[8];
+#pragma unroll
+    for (int j = 0; j < 8; j++) m[j] = C::M(j);
+    uint32_t br = sub8_borrow(t, a.v, b.v);
+    add8_carry(u, t, m);
+    Fe<C> r;
+    select8(r.v, br, u, t);
+    return r;
+}
+
+template <class C>
+ZK_HD Fe<C> fe_dbl(const Fe<C>& a) {
+    return fe_add<C>(a, a);
+}
+
+template <class C>
+ZK_HD bool fe_is_zero(const Fe<C>& a) {
+    uint32_t x = 0;
+#pragma unroll
+    for (int j = 0; j < 8; j++) x |= a.v[j];
+    return x == 0;
+}
+
+template <class C>
+ZK_HD bool fe_eq(const Fe<C>& a, const Fe<C>& b) {
+    uint32_t x = 0;
+#pragma unroll
+    for (int j = 0; j < 8; j++) x |= a.v[j] ^ b.v[j];
+    return x == 0;
+}
+
+template <class C>
+ZK_HD Fe<C> fe_neg(const Fe<C>& a) {
+    return fe_sub<C>(fe_zero<C>(), a);
+}
+
+// a^e for a 32-bit exponent
+template <class C>
+ZK_HD Fe<C> fe_pow_u32(Fe<C> a, uint32_t e) {
+    Fe<C> r = fe_one<C>();
+    while (e) {
+        if (e & 1) r = fe_mul<C>(r, a);
+        e >>= 1;
+        if (e) a = fe_sqr<C>(a);
+    }
+    return r;
+}
+
+// a^(m-2): multiplicative inverse by Fermat's little theorem (0 maps to 0).
+template <class C>
+ZK_HD Fe<C> fe_inv(const Fe<C>& a) {
+    // exponent e = m - 2, scanned from the most significant bit
+    uint32_t e[8];
+    uint32_t two[8] = {2, 0, 0, 0, 0, 0, 0, 0};
+    uint32_t m[8];
+#pragma unroll
+    for (int j = 0; j < 8; j++) m[j] = C::M(j);
+    sub8_borrow(e, m, two);
+    Fe<C> r = fe_one<C>();
+    bool started = false;
+    for (int w = 7; w >= 0; w--) {
+        for (int b = 31; b >= 0; b--) {
+            if (started) r = fe_sqr<C>(r);
+            if ((e[w] >> b) & 1) {
+                r = started ? fe_mul<C>(r, a) : a;
+                started = true;
+            }
+        }
+    }
+    return r;
+}
+
+// n-bit field of a canonical (non-Montgomery) 256-bit value starting at bit `start`
+ZK_HD uint32_t bits_at(const uint32_t v[8], uint32_t start, uint32_t nbits) {
+    uint32_t w = start >> 5, off = start & 31;
+    uint64_t lo = v[w];
+    uint64_t hi = (w + 1 < 8) ? v[w + 1] : 0;
+    uint64_t x = (lo | (hi << 32)) >> off;
+    return (uint32_t)(x & ((nbits >= 32) ? 0xffffffffull : ((1ull << nbits) - 1)));
+}
+
+}  // namespace zk

@@ -1,0 +1,134 @@
+// Internal C++ interface between the kernels and the C-ABI layer.
+#pragma once
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+#include "field.cuh"
+#include "curve.cuh"
+
+namespace zk {
+
+// ------------------------------------------------------------------ NTT
+struct NttPassArgs {
+    const Fr* src;
+    Fr* dst;
+    const Fr* tw;        // natural table w^i, i < 2^log_n
+    int log_n;
+    int log_p;           // log2 of the product of the radices of earlier passes
+    const Fr* in_mul;    // optional multiplier per natural input position (first pass only)
+    const Fr* scale;     // optional multiplier of every output (last pass only)
+    int out_shift;       // output index = (pos << out_shift) + blockIdx.z * out_off_z
+    size_t out_off_z;
+    size_t src_ys, dst_ys;  // per-column strides (blockIdx.y), elements
+    size_t src_zs, dst_zs;  // per-sub-transform strides (blockIdx.z), elements
+    size_t in_mul_zs;
+};
+
+cudaError_t ntt_pass(const NttPassArgs& a, int log_r, unsigned ny, unsigned nz, cudaStream_t s);
+int ntt_plan(int log_n, int radices[4]);
+// Full transform of ncols columns (stride col_stride elements) by the twiddle
+// table tw; result in buf or tmp (*result_in_tmp), multiplied by *scale if given.
+cudaError_t ntt_run(Fr* buf, Fr* tmp, const Fr* tw, const Fr* scale, int log_n, unsigned ncols,
+                    size_t col_stride, bool* result_in_tmp, cudaStream_t s);
+cudaError_t expand_powers(Fr* buf, uint32_t n, cudaStream_t s);
+cudaError_t geometric(Fr* out, const Fr* base, const Fr* w, uint32_t n, cudaStream_t s);
+
+// ------------------------------------------------------------------ MSM
+struct MsmPlan {
+    int c;          // window bits (signed digits in [-(2^(c-1)-1), 2^(c-1)])
+    int W;          // windows
+    uint32_t B;     // buckets per window, 2^(c-1)
+    uint32_t NB;    // W * B
+    uint32_t L;     // sorted entries per accumulation thread
+    uint32_t nacc;  // accumulation threads
+    uint32_t seg;   // buckets per reduction segment
+    uint32_t G;     // reduction segments per window
+    uint32_t n;
+};
+
+struct MsmScratch {
+    uint32_t* count;     // NB
+    uint32_t* offset;    // NB + 1
+    uint32_t* scan_tmp;  // scan_tmp_words(NB)
+    uint32_t* entries;   // n * W
+    uint32_t* part_key;  // 2 * nacc
+    Xyzz* part_pt;       // 2 * nacc
+    Xyzz* buckets;       // NB
+    Xyzz* segsum;        // W * G
+    Xyzz* winsum;        // W
+};
+
+MsmPlan msm_make_plan(uint32_t n, int c);
+size_t msm_u32_words(const MsmPlan& p);     // count + offset + scan tmp + entries + part keys
+size_t msm_point_count(const MsmPlan& p);   // partial points + buckets + segment and window sums
+size_t msm_scratch_bytes(const MsmPlan& p); // one contiguous scratch area (both of the above)
+void msm_layout(const MsmPlan& p, void* base, MsmScratch* s);
+void msm_layout_split(const MsmPlan& p, uint32_t* words, Xyzz* points, MsmScratch* s);
+// sum_i [scalars_i] bases_i written as a Jacobian point at out; scalars in
+// Montgomery form; no allocation, no host synchronisation.
+cudaError_t msm_run(Jac* out, const Aff* bases, const Fr* scalars, const MsmPlan& p, const MsmScratch& s,
+                    cudaStream_t st);
+
+// ------------------------------------------------------------------ scans
+size_t scan_tmp_words(uint32_t n);
+// exclusive prefix sum of n u32 values; out[n] = total
+cudaError_t scan_u32(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* tmp, cudaStream_t s);
+
+
+// ------------------------------------------------------------------ elementwise (eval_h)
+cudaError_t field_op(Fr* res, const Fr* l, int l_rot, const Fr* l_c, const Fr* r, int r_rot, const Fr* r_c,
+                     uint32_t n, int op, cudaStream_t s);
+cudaError_t field_op_batch_mul_sum(Fr* res, Fr* const* v, const int* rot, int n_v, uint32_t n, cudaStream_t s);
+cudaError_t extended_prepare(Fr* s, const Fr* coset_powers, uint32_t cpn, uint32_t size, uint32_t ext_size,
+                             int to_coset, cudaStream_t st);
+cudaError_t permutation_eval_h_p1(Fr* res, const Fr* first_set, const Fr* last_set, const Fr* l0,
+                                  const Fr* l_last, const Fr* y, uint32_t n, cudaStream_t s);
+cudaError_t permutation_eval_h_p2(Fr* res, const Fr* const* set, const Fr* l0, const Fr* y, int n_set, int rot,
+                                  uint32_t n, cudaStream_t s);
+cudaError_t permutation_eval_h_l(Fr* res, const Fr* beta, const Fr* gamma, const Fr* p, uint32_t n,
+                                 cudaStream_t s);
+cudaError_t lookup_eval_h(Fr* res, const Fr* input, const Fr* table, const Fr* permuted_input,
+                          const Fr* permuted_table, const Fr* z, const Fr* l0, const Fr* l_last,
+                          const Fr* l_active_row, const Fr* y, const Fr* beta, const Fr* gamma, int rot, uint32_t n,
+                          cudaStream_t s);
+cudaError_t logup_eval_h(Fr* res, const Fr* input_product, const Fr* input_product_sum, const Fr* table,
+                         const Fr* multiplicity, const Fr* z_first, const Fr* z_last, const Fr* l0,
+                         const Fr* l_last, const Fr* l_active_row, const Fr* y, int rot, uint32_t n, cudaStream_t s);
+cudaError_t logup_eval_h_extra_inputs(Fr* res, const Fr* input_product, const Fr* input_product_sum, const Fr* z,
+                                      const Fr* l_active_row, const Fr* y, int rot, uint32_t n, cudaStream_t s);
+cudaError_t logup_eval_h_inputs_product_sum(Fr* product, Fr* product_sum, const Fr* const* set, int n_set,
+                                            uint32_t n, cudaStream_t s);
+cudaError_t shuffle_eval_h(Fr* res, const Fr* input, const Fr* table, const Fr* z, const Fr* l0, const Fr* l_last,
+                           const Fr* l_active_row, const Fr* y, int rot, uint32_t n, cudaStream_t s);
+cudaError_t shuffle_eval_h_v2(Fr* res, const Fr* const* inputs, const Fr* const* tables, const Fr* betas,
+                              int group_len, const Fr* z, const Fr* l0, const Fr* l_last, const Fr* l_active_row,
+                              const Fr* y, int rot, uint32_t n, cudaStream_t s);
+cudaError_t field_mul_zip(Fr* buf, const Fr* coeff, uint32_t coeff_n, uint32_t n, cudaStream_t s);
+cudaError_t field_sum(Fr* res, Fr* const* v, Fr* const* v_c, const int* v_rot, const Fr* omegas, int v_n,
+                      uint32_t n, cudaStream_t s);
+cudaError_t shplonk_h_x_merge(Fr* res, const Fr* v, const Fr* values, const Fr* omegas, const Fr* diff_points,
+                              int diff_points_n, uint32_t n, cudaStream_t s);
+
+
+// ------------------------------------------------------------------ Fr scans
+cudaError_t batch_inverse(Fr* out, const Fr* in, const Fr* c, uint32_t n, int accumulate, cudaStream_t s);
+cudaError_t div_by_point_diffs(Fr* values, const Fr* omegas, const Fr* points, int np, uint32_t n, cudaStream_t s);
+size_t fr_scan_tmp_elems(uint32_t n);
+cudaError_t fr_scan_excl(Fr* out, const Fr* in, uint32_t n, const Fr* init, int op, Fr* tmp, cudaStream_t s);
+cudaError_t logup_z_scan(Fr* z, Fr* last_z, int last_index, uint32_t n, Fr* tmp, cudaStream_t s);
+cudaError_t logup_z_compose(Fr* z, const Fr* sum, const Fr* table, const Fr* m, const Fr* beta, Fr* last_z,
+                            int last_index, uint32_t n, Fr* tmp, cudaStream_t s);
+cudaError_t permutation_chunk_z(Fr* z, const Fr* const* cols, const Fr* const* sig, int ncols, const Fr* beta,
+                                const Fr* gamma, const Fr* dbeta, const Fr* omegas, const Fr* init, uint32_t n,
+                                Fr* tmp, cudaStream_t s);
+cudaError_t shuffle_z(Fr* z, const Fr* const* inputs, const Fr* const* tables, const Fr* betas, int groups,
+                      uint32_t n, Fr* num_tmp, Fr* tmp, cudaStream_t s);
+
+// ------------------------------------------------------------------ lookup / poly
+cudaError_t lookup_table_build(const Fr* table, uint32_t usable, uint32_t* slots, uint32_t log_slots,
+                               cudaStream_t s);
+cudaError_t lookup_count(Fr* m, const Fr* table, const Fr* input, uint32_t n, uint32_t usable, const uint32_t* slots,
+                         uint32_t log_slots, uint32_t* cnt, cudaStream_t s);
+cudaError_t poly_eval(const Fr* p, Fr* res, const Fr* x_table, uint32_t n, cudaStream_t s);
+
+}  // namespace zk

@@ -1,0 +1,322 @@
+// Pippenger multi-scalar multiplication over BN254 G1 for sm_100a.
+//
+// Pipeline (all on one stream, no host synchronisation, no allocation):
+//   1. count    one thread per scalar: Montgomery -> canonical, signed c-bit
+//               digits, atomic histogram of bucket keys (window * B + |d| - 1)
+//   2. scan     exclusive prefix sum of the histogram -> bucket offsets
+//   3. scatter  digits again; each non-zero digit claims a slot in its bucket
+//               and stores (point index | sign << 31): a device counting sort
+//   4. accumulate  every thread owns a fixed-length slice of the sorted entries
+//               and sums runs of equal key with XYZZ + affine additions; runs
+//               that cross a slice boundary are left as head / tail partials
+//   5. merge    each tail partial absorbs the following heads of the same key
+//   6. reduce   per window, segments of buckets by running sums:
+//               sum_b (b+1) B_b = S_seg + lo * T_seg
+//   7. window   tree sum of the segment results per window
+//   8. final    Horner over windows (c doublings each) -> Jacobian output
+//
+// Reference behaviour replaced: cuda/msm.cu:9-467 (unsigned digits, CUB radix
+// sort, Jacobian accumulation, one-thread window combine) behind the C entry
+// points msm / batch_msm_collect.
+#include "common.cuh"
+#include "kernels.h"
+
+namespace zk {
+
+static constexpr uint32_t KEY_NONE = 0xffffffffu;
+
+__device__ __forceinline__ Aff ld_aff(const Aff* p) {
+    Aff a;
+    a.x = ldg_elem<FqCfg>(&p->x);
+    a.y = ldg_elem<FqCfg>(&p->y);
+    return a;
+}
+
+__device__ __forceinline__ Xyzz ld_xyzz(const Xyzz* p) {
+    Xyzz r;
+    r.x = ld_elem<FqCfg>(&p->x);
+    r.y = ld_elem<FqCfg>(&p->y);
+    r.zz = ld_elem<FqCfg>(&p->zz);
+    r.zzz = ld_elem<FqCfg>(&p->zzz);
+    return r;
+}
+
+__device__ __forceinline__ void st_xyzz(Xyzz* p, const Xyzz& v) {
+    st_elem<FqCfg>(&p->x, v.x);
+    st_elem<FqCfg>(&p->y, v.y);
+    st_elem<FqCfg>(&p->zz, v.zz);
+    st_elem<FqCfg>(&p->zzz, v.zzz);
+}
+
+__global__ void msm_count_kernel(const Fr* __restrict__ scalars, uint32_t n, int c, int W,
+                                 uint32_t* __restrict__ count) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    Fr k = fe_from_mont<FrCfg>(ldg_elem<FrCfg>(scalars + i));
+    const uint32_t B = 1u << (c - 1);
+    uint32_t carry = 0;
+    for (int w = 0; w < W; w++) {
+        int d = msm_signed_digit(k.v, w, c, carry);
+        if (d != 0) {
+            uint32_t mag = d > 0 ? (uint32_t)d : (uint32_t)(-d);
+            atomicAdd(&count[(uint32_t)w * B + mag - 1], 1u);
+        }
+    }
+}
+
+__global__ void msm_scatter_kernel(const Fr* __restrict__ scalars, uint32_t n, int c, int W,
+                                   const uint32_t* __restrict__ offset, uint32_t* __restrict__ count,
+                                   uint32_t* __restrict__ entries) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    Fr k = fe_from_mont<FrCfg>(ldg_elem<FrCfg>(scalars + i));
+    const uint32_t B = 1u << (c - 1);
+    uint32_t carry = 0;
+    for (int w = 0; w < W; w++) {
+        int d = msm_signed_digit(k.v, w, c, carry);
+        if (d != 0) {
+            uint32_t mag = d > 0 ? (uint32_t)d : (uint32_t)(-d);
+            uint32_t key = (uint32_t)w * B + mag - 1;
+            uint32_t slot = atomicSub(&count[key], 1u) - 1u;
+            entries[offset[key] + slot] = i | (d < 0 ? 0x80000000u : 0u);
+        }
+    }
+}
+
+// largest k in [lo, hi) with off[k] <= pos
+__device__ __forceinline__ uint32_t find_bucket(const uint32_t* off, uint32_t lo, uint32_t hi, uint32_t pos) {
+    while (hi - lo > 1) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (off[mid] <= pos)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+__global__ void __launch_bounds__(128) msm_accumulate_kernel(const uint32_t* __restrict__ entries,
+                                                             const uint32_t* __restrict__ offset, uint32_t NB,
+                                                             const Aff* __restrict__ bases, uint32_t L,
+                                                             uint32_t nacc, Xyzz* __restrict__ buckets,
+                                                             uint32_t* __restrict__ part_key,
+                                                             Xyzz* __restrict__ part_pt) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nacc) return;
+    const uint32_t total = offset[NB];
+    const uint32_t s = t * L;
+    uint32_t head_key = KEY_NONE, tail_key = KEY_NONE;
+    if (s < total) {
+        const uint32_t e = min(s + L, total);
+        uint32_t key = find_bucket(offset, 0, NB, s);
+        uint32_t pos = s;
+        while (pos < e) {
+            const uint32_t kbeg = offset[key], kend = offset[key + 1];
+            const uint32_t rend = min(kend, e);
+            Xyzz acc = xyzz_identity();
+            for (uint32_t p = pos; p < rend; p++) {
+                const uint32_t ent = entries[p];
+                Aff a = ld_aff(bases + (ent & 0x7fffffffu));
+                if (aff_is_id(a)) continue;
+                if (ent >> 31) a.y = fe_neg<FqCfg>(a.y);
+                acc = xyzz_add_aff(acc, a.x, a.y);
+            }
+            const bool before = kbeg < s;
+            const bool after = kend > e;
+            if (!before && !after) {
+                st_xyzz(buckets + key, acc);
+            } else if (before) {
+                head_key = key;
+                st_xyzz(part_pt + 2 * t, acc);
+            } else {
+                tail_key = key;
+                st_xyzz(part_pt + 2 * t + 1, acc);
+            }
+            pos = rend;
+            if (pos < e) key = find_bucket(offset, key + 1, NB, pos);
+        }
+    }
+    part_key[2 * t] = head_key;
+    part_key[2 * t + 1] = tail_key;
+}
+
+__global__ void __launch_bounds__(128) msm_merge_kernel(const uint32_t* __restrict__ part_key,
+                                                        const Xyzz* __restrict__ part_pt, uint32_t nacc,
+                                                        Xyzz* __restrict__ buckets) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nacc) return;
+    const uint32_t key = part_key[2 * t + 1];
+    if (key == KEY_NONE) return;
+    Xyzz acc = ld_xyzz(part_pt + 2 * t + 1);
+    for (uint32_t u = t + 1; u < nacc; u++) {
+        if (part_key[2 * u] != key) break;
+        acc = xyzz_add(acc, ld_xyzz(part_pt + 2 * u));
+    }
+    st_xyzz(buckets + key, acc);
+}
+
+__global__ void __launch_bounds__(128) msm_reduce_kernel(const Xyzz* __restrict__ buckets,
+                                                         const uint32_t* __restrict__ offset, int W, uint32_t B,
+                                                         uint32_t seg, uint32_t G, Xyzz* __restrict__ segsum) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (uint32_t)W * G) return;
+    const uint32_t w = t / G, g = t % G;
+    const uint32_t lo = g * seg;
+    Xyzz T = xyzz_identity(), S = xyzz_identity();
+    for (uint32_t j = 0; j < seg; j++) {
+        const uint32_t b = lo + seg - 1 - j;
+        const uint32_t key = w * B + b;
+        if (offset[key + 1] != offset[key]) T = xyzz_add(T, ld_xyzz(buckets + key));
+        S = xyzz_add(S, T);
+    }
+    if (lo) S = xyzz_add(S, xyzz_mul_u32(T, lo));
+    st_xyzz(segsum + t, S);
+}
+
+__global__ void msm_window_kernel(const Xyzz* __restrict__ segsum, uint32_t G, Xyzz* __restrict__ winsum) {
+    extern __shared__ uint4 smem_u4[];
+    Xyzz* sm = reinterpret_cast<Xyzz*>(smem_u4);
+    const uint32_t w = blockIdx.x, i = threadIdx.x;
+    sm[i] = ld_xyzz(segsum + (size_t)w * G + i);
+    __syncthreads();
+    for (uint32_t h = G >> 1; h > 0; h >>= 1) {
+        if (i < h) sm[i] = xyzz_add(sm[i], sm[i + h]);
+        __syncthreads();
+    }
+    if (i == 0) st_xyzz(winsum + w, sm[0]);
+}
+
+__global__ void msm_final_kernel(const Xyzz* __restrict__ winsum, int W, int c, Jac* __restrict__ out) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    Xyzz acc = W > 0 ? ld_xyzz(winsum + W - 1) : xyzz_identity();
+    for (int w = W - 2; w >= 0; w--) {
+        for (int i = 0; i < c; i++) acc = xyzz_dbl(acc);
+        acc = xyzz_add(acc, ld_xyzz(winsum + w));
+    }
+    Jac j = xyzz_to_jac(acc);
+    st_elem<FqCfg>(&out->x, j.x);
+    st_elem<FqCfg>(&out->y, j.y);
+    st_elem<FqCfg>(&out->z, j.z);
+}
+
+// ------------------------------------------------------------------ planning
+
+static int windows_for(int c) { return (254 + c - 1) / c; }
+
+static int pick_c(uint32_t n) {
+    int best = 4;
+    double best_cost = 1e300;
+    for (int c = 4; c <= 20; c++) {
+        const double W = windows_for(c);
+        const double cost = 10.0 * n * W + 28.0 * W * (double)(1u << (c - 1)) + 9.0 * 300.0 * (W - 1) * c;
+        if (cost < best_cost) {
+            best_cost = cost;
+            best = c;
+        }
+    }
+    return best;
+}
+
+MsmPlan msm_make_plan(uint32_t n, int c) {
+    MsmPlan p;
+    p.n = n;
+    p.c = (c >= 4 && c <= 22) ? c : pick_c(n);
+    p.W = windows_for(p.c);
+    p.B = 1u << (p.c - 1);
+    p.NB = (uint32_t)p.W * p.B;
+    const uint64_t max_entries = (uint64_t)n * p.W;
+    const uint64_t target_threads = 148ull * 4 * 128;
+    uint64_t L = (max_entries + target_threads - 1) / target_threads;
+    if (L < 8) L = 8;
+    p.L = (uint32_t)L;
+    p.nacc = (uint32_t)((max_entries + L - 1) / L);
+    if (p.nacc == 0) p.nacc = 1;
+    // about 16K reduction threads in total, at most 512 segments per window
+    uint32_t G = 1;
+    while (G < 512 && (uint64_t)G * 2 * p.W <= 16384 && G * 2 <= p.B) G *= 2;
+    p.G = G;
+    p.seg = p.B / G;
+    return p;
+}
+
+static size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+size_t msm_u32_words(const MsmPlan& p) {
+    size_t w = 0;
+    w += align_up(p.NB, 64);
+    w += align_up(p.NB + 1, 64);
+    w += align_up(scan_tmp_words(p.NB), 64);
+    w += align_up((size_t)p.n * p.W, 64);
+    w += align_up((size_t)2 * p.nacc, 64);
+    return w;
+}
+
+size_t msm_point_count(const MsmPlan& p) { return (size_t)2 * p.nacc + p.NB + (size_t)p.W * p.G + p.W; }
+
+size_t msm_scratch_bytes(const MsmPlan& p) {
+    return align_up(msm_u32_words(p) * 4, 256) + msm_point_count(p) * sizeof(Xyzz);
+}
+
+void msm_layout_split(const MsmPlan& p, uint32_t* words, Xyzz* points, MsmScratch* s) {
+    uint32_t* w = words;
+    s->count = w;
+    w += align_up(p.NB, 64);
+    s->offset = w;
+    w += align_up(p.NB + 1, 64);
+    s->scan_tmp = w;
+    w += align_up(scan_tmp_words(p.NB), 64);
+    s->entries = w;
+    w += align_up((size_t)p.n * p.W, 64);
+    s->part_key = w;
+    Xyzz* q = points;
+    s->part_pt = q;
+    q += (size_t)2 * p.nacc;
+    s->buckets = q;
+    q += p.NB;
+    s->segsum = q;
+    q += (size_t)p.W * p.G;
+    s->winsum = q;
+}
+
+void msm_layout(const MsmPlan& p, void* base, MsmScratch* s) {
+    uint32_t* words = reinterpret_cast<uint32_t*>(base);
+    Xyzz* pts = reinterpret_cast<Xyzz*>(reinterpret_cast<char*>(base) + align_up(msm_u32_words(p) * 4, 256));
+    msm_layout_split(p, words, pts, s);
+}
+
+cudaError_t msm_run(Jac* out, const Aff* bases, const Fr* scalars, const MsmPlan& p, const MsmScratch& s,
+                    cudaStream_t st) {
+    if (p.n == 0) {
+        // empty sum: the identity
+        msm_final_kernel<<<1, 1, 0, st>>>(nullptr, 0, p.c, out);
+        return cudaGetLastError();
+    }
+    const uint32_t tb = 256;
+    const uint32_t nblk = (p.n + tb - 1) / tb;
+    ZK_CHECK(cudaMemsetAsync(s.count, 0, sizeof(uint32_t) * p.NB, st));
+    msm_count_kernel<<<nblk, tb, 0, st>>>(scalars, p.n, p.c, p.W, s.count);
+    ZK_CHECK(cudaGetLastError());
+    ZK_CHECK(scan_u32(s.count, s.offset, p.NB, s.scan_tmp, st));
+    msm_scatter_kernel<<<nblk, tb, 0, st>>>(scalars, p.n, p.c, p.W, s.offset, s.count, s.entries);
+    ZK_CHECK(cudaGetLastError());
+    msm_accumulate_kernel<<<(p.nacc + 127) / 128, 128, 0, st>>>(s.entries, s.offset, p.NB, bases, p.L, p.nacc,
+                                                                s.buckets, s.part_key, s.part_pt);
+    ZK_CHECK(cudaGetLastError());
+    msm_merge_kernel<<<(p.nacc + 127) / 128, 128, 0, st>>>(s.part_key, s.part_pt, p.nacc, s.buckets);
+    ZK_CHECK(cudaGetLastError());
+    const uint32_t nred = (uint32_t)p.W * p.G;
+    msm_reduce_kernel<<<(nred + 127) / 128, 128, 0, st>>>(s.buckets, s.offset, p.W, p.B, p.seg, p.G, s.segsum);
+    ZK_CHECK(cudaGetLastError());
+    const size_t wsm = (size_t)p.G * sizeof(Xyzz);
+    static bool attr = false;
+    if (!attr) {
+        ZK_CHECK(cudaFuncSetAttribute(msm_window_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 512 * (int)sizeof(Xyzz)));
+        attr = true;
+    }
+    msm_window_kernel<<<p.W, p.G, wsm, st>>>(s.segsum, p.G, s.winsum);
+    ZK_CHECK(cudaGetLastError());
+    msm_final_kernel<<<1, 1, 0, st>>>(s.winsum, p.W, p.c, out);
+    return cudaGetLastError();
+}
+
+}  // namespace zk

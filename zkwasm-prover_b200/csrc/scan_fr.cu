@@ -1,0 +1,375 @@
+// Device scans over BN254 Fr: batch inversion (Montgomery's trick), exclusive
+// prefix products and sums with a carried-in initial value, and the grand
+// products / sums of the permutation, shuffle and logup arguments built on them.
+//
+// Reference behaviour replaced:
+//   logup_sum_input_inv        cuda/bn254.cu:19-61, 1914-1934 (one serial chunk
+//                              and one inversion per thread)
+//   eval_logup_z_compose/pure  cuda/bn254.cu:63-220, 1936-1993 (5 launches, a
+//                              single-thread middle level)
+//   permutation product        src/permutation.rs:16-150 (CPU, rayon)
+//   shuffle product            src/shuffle.rs:143-212 (CPU, rayon)
+#include "common.cuh"
+#include "kernels.h"
+
+namespace zk {
+
+static constexpr int ST = 256;  // threads per block
+static constexpr int SK = 8;    // elements per thread
+static constexpr int SBLK = ST * SK;
+
+enum { OP_ADD = 0, OP_MUL = 1 };
+
+__device__ __forceinline__ Fr op_apply(int op, const Fr& a, const Fr& b) {
+    return op == OP_MUL ? fe_mul<FrCfg>(a, b) : fe_add<FrCfg>(a, b);
+}
+__device__ __forceinline__ Fr op_ident(int op) { return op == OP_MUL ? fe_one<FrCfg>() : fe_zero<FrCfg>(); }
+
+__device__ __forceinline__ Fr shfl_up_fr(const Fr& v, int o) {
+    Fr r;
+#pragma unroll
+    for (int j = 0; j < 8; j++) r.v[j] = __shfl_up_sync(0xffffffffu, v.v[j], o);
+    return r;
+}
+
+// block-wide exclusive scan of one value per thread (thread order);
+// wsm holds at least 32 elements
+__device__ Fr block_excl_scan_fr(int op, const Fr& v, Fr* wsm, Fr& total) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    Fr x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        Fr y = shfl_up_fr(x, o);
+        if (lane >= o) x = op_apply(op, y, x);
+    }
+    Fr e = shfl_up_fr(x, 1);
+    if (lane == 0) e = op_ident(op);
+    if (lane == 31) wsm[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+        Fr w = lane < nw ? wsm[lane] : op_ident(op);
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            Fr y = shfl_up_fr(w, o);
+            if (lane >= o) w = op_apply(op, y, w);
+        }
+        if (lane < nw) wsm[lane] = w;
+    }
+    __syncthreads();
+    total = wsm[nw - 1];
+    Fr r = wid ? op_apply(op, wsm[wid - 1], e) : e;
+    __syncthreads();
+    return r;
+}
+
+// ------------------------------------------------------------ batch inverse
+// Montgomery's trick over a block of ST * SK elements: one field inversion per
+// block.  Thread t owns elements base + t + ST*k (coalesced); its chunk
+// product is combined with the exclusive prefix E_t and suffix S_t of the
+// other threads' products, so inv(chunk_t) = inv(total) * S_t * E_t, and the
+// chunk is unwound locally.  The element value comes from a functor that is
+// evaluated twice (forward and backward) instead of being stored, so the
+// kernel needs no scratch memory.  Zero elements invert to zero.
+
+struct SrcPlus {  // in[i] + c  (c optional)
+    const Fr* in;
+    const Fr* c;
+    __device__ __forceinline__ Fr operator()(uint32_t i) const {
+        Fr a = ld_elem<FrCfg>(in + i);
+        return c ? fe_add<FrCfg>(a, ld_elem<FrCfg>(c)) : a;
+    }
+};
+
+struct SrcPointDiff {  // prod_j (omegas[i] - points[j])
+    const Fr* omegas;
+    const Fr* points;
+    int np;
+    __device__ __forceinline__ Fr operator()(uint32_t i) const {
+        const Fr w = ld_elem<FrCfg>(omegas + i);
+        Fr t = fe_sub<FrCfg>(w, ld_elem<FrCfg>(points));
+        for (int j = 1; j < np; j++) t = fe_mul<FrCfg>(t, fe_sub<FrCfg>(w, ld_elem<FrCfg>(points + j)));
+        return t;
+    }
+};
+
+struct DstStore {  // out[i] = (acc ? out[i] : 0) + inv
+    Fr* out;
+    int acc;
+    __device__ __forceinline__ void operator()(uint32_t i, const Fr& v) const {
+        st_elem<FrCfg>(out + i, acc ? fe_add<FrCfg>(v, ld_elem<FrCfg>(out + i)) : v);
+    }
+};
+
+struct DstScale {  // out[i] *= inv
+    Fr* out;
+    __device__ __forceinline__ void operator()(uint32_t i, const Fr& v) const {
+        st_elem<FrCfg>(out + i, fe_mul<FrCfg>(ld_elem<FrCfg>(out + i), v));
+    }
+};
+
+template <class Src, class Dst>
+__global__ void __launch_bounds__(ST) batch_inv_kernel(Src src, Dst dst, uint32_t n) {
+    __shared__ Fr wsm[32];
+    __shared__ Fr rev[ST];
+    __shared__ Fr inv_tot;
+    const size_t base = (size_t)blockIdx.x * SBLK;
+    const int t = threadIdx.x;
+    const Fr one = fe_one<FrCfg>();
+    Fr pre[SK];
+    Fr run = one;
+#pragma unroll
+    for (int k = 0; k < SK; k++) {
+        const size_t i = base + t + (size_t)ST * k;
+        Fr a = one;
+        if (i < n) {
+            a = src((uint32_t)i);
+            if (fe_is_zero<FrCfg>(a)) a = one;
+        }
+        run = fe_mul<FrCfg>(run, a);
+        pre[k] = run;
+    }
+    Fr tot;
+    Fr E = block_excl_scan_fr(OP_MUL, run, wsm, tot);
+    rev[ST - 1 - t] = run;
+    __syncthreads();
+    Fr rv = rev[t];
+    __syncthreads();
+    Fr tot2;
+    Fr Srev = block_excl_scan_fr(OP_MUL, rv, wsm, tot2);
+    rev[ST - 1 - t] = Srev;
+    __syncthreads();
+    Fr S = rev[t];
+    if (t == 0) inv_tot = fe_inv<FrCfg>(tot);
+    __syncthreads();
+    Fr cur = fe_mul<FrCfg>(fe_mul<FrCfg>(inv_tot, S), E);
+#pragma unroll
+    for (int k = SK - 1; k >= 0; k--) {
+        const size_t i = base + t + (size_t)ST * k;
+        Fr a = one;
+        bool zero = true;
+        if (i < n) {
+            a = src((uint32_t)i);
+            zero = fe_is_zero<FrCfg>(a);
+            if (zero) a = one;
+        }
+        Fr inv_k = k ? fe_mul<FrCfg>(cur, pre[k - 1]) : cur;
+        cur = fe_mul<FrCfg>(cur, a);
+        if (i < n) dst((uint32_t)i, zero ? fe_zero<FrCfg>() : inv_k);
+    }
+}
+
+template <class Src, class Dst>
+static cudaError_t launch_batch_inv(Src src, Dst dst, uint32_t n, cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    const uint32_t nb = (n + SBLK - 1) / SBLK;
+    batch_inv_kernel<Src, Dst><<<nb, ST, 0, s>>>(src, dst, n);
+    return cudaGetLastError();
+}
+
+cudaError_t batch_inverse(Fr* out, const Fr* in, const Fr* c, uint32_t n, int accumulate, cudaStream_t s) {
+    return launch_batch_inv(SrcPlus{in, c}, DstStore{out, accumulate}, n, s);
+}
+
+// values[i] /= prod_j (omegas[i] - points[j])
+cudaError_t div_by_point_diffs(Fr* values, const Fr* omegas, const Fr* points, int np, uint32_t n, cudaStream_t s) {
+    if (np <= 0) return cudaSuccess;
+    return launch_batch_inv(SrcPointDiff{omegas, points, np}, DstScale{values}, n, s);
+}
+
+// ------------------------------------------------------------ exclusive scan
+// Phase 1: block-local exclusive scan written to out, block totals to tmp.
+// Phase 2: exclusive scan of block totals (recursive) with the initial value.
+// Phase 3: out[i] = prefix(block) op out[i].
+
+__global__ void __launch_bounds__(ST) scan_local_kernel(Fr* out, const Fr* in, uint32_t n, int op, Fr* btot) {
+    __shared__ Fr wsm[32];
+    const size_t base = (size_t)blockIdx.x * SBLK + (size_t)threadIdx.x * SK;
+    Fr v[SK];
+    Fr run = op_ident(op);
+#pragma unroll
+    for (int k = 0; k < SK; k++) {
+        Fr a = (base + k < n) ? ld_elem<FrCfg>(in + base + k) : op_ident(op);
+        v[k] = run;  // exclusive within the thread
+        run = op_apply(op, run, a);
+    }
+    Fr tot;
+    Fr e = block_excl_scan_fr(op, run, wsm, tot);
+#pragma unroll
+    for (int k = 0; k < SK; k++)
+        if (base + k < n) st_elem<FrCfg>(out + base + k, op_apply(op, e, v[k]));
+    if (threadIdx.x == 0) st_elem<FrCfg>(btot + blockIdx.x, tot);
+}
+
+__global__ void __launch_bounds__(ST) scan_apply_kernel(Fr* out, uint32_t n, int op, const Fr* bpre) {
+    const Fr p = ld_elem<FrCfg>(bpre + blockIdx.x);
+    const size_t base = (size_t)blockIdx.x * SBLK;
+    for (int k = threadIdx.x; k < SBLK; k += ST) {
+        const size_t i = base + k;
+        if (i < n) st_elem<FrCfg>(out + i, op_apply(op, p, ld_elem<FrCfg>(out + i)));
+    }
+}
+
+// single block: exclusive scan of m <= SBLK values with init, in place; optional total
+__global__ void __launch_bounds__(ST) scan_small_kernel(Fr* x, uint32_t m, int op, const Fr* init) {
+    __shared__ Fr wsm[32];
+    const size_t base = (size_t)threadIdx.x * SK;
+    Fr v[SK];
+    Fr run = op_ident(op);
+#pragma unroll
+    for (int k = 0; k < SK; k++) {
+        Fr a = (base + k < m) ? ld_elem<FrCfg>(x + base + k) : op_ident(op);
+        v[k] = run;
+        run = op_apply(op, run, a);
+    }
+    Fr tot;
+    Fr e = block_excl_scan_fr(op, run, wsm, tot);
+    const Fr i0 = init ? ld_elem<FrCfg>(init) : op_ident(op);
+    e = op_apply(op, i0, e);
+#pragma unroll
+    for (int k = 0; k < SK; k++)
+        if (base + k < m) st_elem<FrCfg>(x + base + k, op_apply(op, e, v[k]));
+}
+
+size_t fr_scan_tmp_elems(uint32_t n) {
+    size_t t = 0;
+    uint32_t m = n;
+    while (m > (uint32_t)SBLK) {
+        m = (m + SBLK - 1) / SBLK;
+        t += m;
+    }
+    return t + 1;
+}
+
+// out[i] = init op x_0 op ... op x_{i-1}; out may alias in
+cudaError_t fr_scan_excl(Fr* out, const Fr* in, uint32_t n, const Fr* init, int op, Fr* tmp, cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    if (n <= (uint32_t)SBLK) {
+        if (out != in) ZK_CHECK(cudaMemcpyAsync(out, in, (size_t)n * sizeof(Fr), cudaMemcpyDeviceToDevice, s));
+        scan_small_kernel<<<1, ST, 0, s>>>(out, n, op, init);
+        return cudaGetLastError();
+    }
+    const uint32_t nb = (n + SBLK - 1) / SBLK;
+    Fr* btot = tmp;
+    scan_local_kernel<<<nb, ST, 0, s>>>(out, in, n, op, btot);
+    ZK_CHECK(cudaGetLastError());
+    ZK_CHECK(fr_scan_excl(btot, btot, nb, init, op, tmp + nb, s));
+    scan_apply_kernel<<<nb, ST, 0, s>>>(out, n, op, btot);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------- logup
+
+__global__ void logup_step2_kernel(Fr* z, const Fr* sum, const Fr* m, uint32_t n) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        st_elem<FrCfg>(z + i, fe_sub<FrCfg>(ld_elem<FrCfg>(sum + i), fe_mul<FrCfg>(ld_elem<FrCfg>(m + i), ld_elem<FrCfg>(z + i))));
+}
+
+__global__ void copy_elem_kernel(Fr* dst, const Fr* src) {
+    if (threadIdx.x == 0) st_elem<FrCfg>(dst, ld_elem<FrCfg>(src));
+}
+
+// z = exclusive prefix sum of z starting at *last_z; then *last_z = z[last_index]
+cudaError_t logup_z_scan(Fr* z, Fr* last_z, int last_index, uint32_t n, Fr* tmp, cudaStream_t s) {
+    ZK_CHECK(fr_scan_excl(z, z, n, last_z, OP_ADD, tmp, s));
+    if (last_index >= 0 && (uint32_t)last_index < n) {
+        copy_elem_kernel<<<1, 32, 0, s>>>(last_z, z + last_index);
+        ZK_CHECK(cudaGetLastError());
+    }
+    return cudaSuccess;
+}
+
+cudaError_t logup_z_compose(Fr* z, const Fr* sum, const Fr* table, const Fr* m, const Fr* beta, Fr* last_z,
+                            int last_index, uint32_t n, Fr* tmp, cudaStream_t s) {
+    ZK_CHECK(batch_inverse(z, table, beta, n, 0, s));
+    unsigned nb = (n + 255) / 256;
+    if (nb > 148 * 32) nb = 148 * 32;
+    logup_step2_kernel<<<nb, 256, 0, s>>>(z, sum, m, n);
+    ZK_CHECK(cudaGetLastError());
+    return logup_z_scan(z, last_z, last_index, n, tmp, s);
+}
+
+// ------------------------------------------------ permutation / shuffle ratio
+// d[i] = prod_c (v_c[i] + beta*delta^c*w^i + gamma) / prod_c (v_c[i] + beta*sigma_c[i] + gamma)
+// with delta^c for the chunk's columns given as dpow[c] (c < ncols).
+
+__global__ void perm_den_kernel(Fr* den, const Fr* const* cols, const Fr* const* sig, int ncols, const Fr* beta,
+                                const Fr* gamma, uint32_t n) {
+    const Fr b = ld_elem<FrCfg>(beta), g = ld_elem<FrCfg>(gamma);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        Fr acc = fe_one<FrCfg>();
+        for (int c = 0; c < ncols; c++) {
+            Fr t = fe_add<FrCfg>(fe_add<FrCfg>(fe_mul<FrCfg>(ld_elem<FrCfg>(sig[c] + i), b), g),
+                                 ld_elem<FrCfg>(cols[c] + i));
+            acc = fe_mul<FrCfg>(acc, t);
+        }
+        st_elem<FrCfg>(den + i, acc);
+    }
+}
+
+// d[i] = inv_den[i] * prod_c (v_c[i] + beta*delta^c*w^i + gamma); omega table w^i
+__global__ void perm_num_kernel(Fr* d, const Fr* const* cols, const Fr* dbeta, int ncols, const Fr* gamma,
+                                const Fr* omegas, uint32_t n) {
+    const Fr g = ld_elem<FrCfg>(gamma);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const Fr w = ld_elem<FrCfg>(omegas + i);
+        Fr acc = ld_elem<FrCfg>(d + i);
+        for (int c = 0; c < ncols; c++) {
+            Fr t = fe_add<FrCfg>(fe_add<FrCfg>(fe_mul<FrCfg>(w, ld_elem<FrCfg>(dbeta + c)), g),
+                                 ld_elem<FrCfg>(cols[c] + i));
+            acc = fe_mul<FrCfg>(acc, t);
+        }
+        st_elem<FrCfg>(d + i, acc);
+    }
+}
+
+static unsigned grid_n(uint32_t n) {
+    unsigned nb = (n + 255) / 256;
+    if (nb > 148 * 32) nb = 148 * 32;
+    return nb ? nb : 1;
+}
+
+// one chunk of the permutation argument: z = exclusive prefix product of the
+// ratio, starting at *init (1 for the first chunk, the previous chunk's z at
+// the last usable row otherwise).  dbeta[c] = beta * delta^(chunk_offset + c).
+cudaError_t permutation_chunk_z(Fr* z, const Fr* const* cols, const Fr* const* sig, int ncols, const Fr* beta,
+                                const Fr* gamma, const Fr* dbeta, const Fr* omegas, const Fr* init, uint32_t n,
+                                Fr* tmp, cudaStream_t s) {
+    perm_den_kernel<<<grid_n(n), 256, 0, s>>>(z, cols, sig, ncols, beta, gamma, n);
+    ZK_CHECK(cudaGetLastError());
+    ZK_CHECK(batch_inverse(z, z, nullptr, n, 0, s));
+    perm_num_kernel<<<grid_n(n), 256, 0, s>>>(z, cols, dbeta, ncols, gamma, omegas, n);
+    ZK_CHECK(cudaGetLastError());
+    return fr_scan_excl(z, z, n, init, OP_MUL, tmp, s);
+}
+
+// shuffle: z = exclusive prefix product of prod_g (input_g + beta_g) / prod_g (table_g + beta_g)
+__global__ void shuffle_terms_kernel(Fr* den, Fr* num, const Fr* const* inputs, const Fr* const* tables,
+                                     const Fr* betas, int groups, uint32_t n) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        Fr a = fe_one<FrCfg>(), b = fe_one<FrCfg>();
+        for (int g = 0; g < groups; g++) {
+            const Fr bg = ld_elem<FrCfg>(betas + g);
+            a = fe_mul<FrCfg>(a, fe_add<FrCfg>(ld_elem<FrCfg>(inputs[g] + i), bg));
+            b = fe_mul<FrCfg>(b, fe_add<FrCfg>(ld_elem<FrCfg>(tables[g] + i), bg));
+        }
+        st_elem<FrCfg>(num + i, a);
+        st_elem<FrCfg>(den + i, b);
+    }
+}
+
+__global__ void mul_inplace_kernel(Fr* a, const Fr* b, uint32_t n) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        st_elem<FrCfg>(a + i, fe_mul<FrCfg>(ld_elem<FrCfg>(a + i), ld_elem<FrCfg>(b + i)));
+}
+
+cudaError_t shuffle_z(Fr* z, const Fr* const* inputs, const Fr* const* tables, const Fr* betas, int groups,
+                      uint32_t n, Fr* num_tmp, Fr* tmp, cudaStream_t s) {
+    shuffle_terms_kernel<<<grid_n(n), 256, 0, s>>>(z, num_tmp, inputs, tables, betas, groups, n);
+    ZK_CHECK(cudaGetLastError());
+    ZK_CHECK(batch_inverse(z, z, nullptr, n, 0, s));
+    mul_inplace_kernel<<<grid_n(n), 256, 0, s>>>(z, num_tmp, n);
+    ZK_CHECK(cudaGetLastError());
+    return fr_scan_excl(z, z, n, nullptr, OP_MUL, tmp, s);
+}
+
+}  // namespace zk

@@ -1,0 +1,227 @@
+"""Host-side mirror of the reference's GPU wrappers for the proving hot path.
+
+Function names, arguments and buffer sizing follow the reference's Rust
+wrappers (src/cuda/ntt.rs, src/cuda/msm.rs, src/cuda/bn254.rs); device buffers
+are torch tensors (int64 storage, 4 words per field element, 8 per affine
+point, 12 per Jacobian point).  Every call goes through the C ABI of
+libzkwasm_prover_kernel.so and raises on a CUDA error status.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+
+from . import abi
+
+MAX_DEG = 8  # src/cuda/ntt.rs:13
+
+
+def lib():
+    return abi.load_library()
+
+
+def _require_cuda():
+    if not torch.cuda.is_available():
+        raise RuntimeError("zkwasm-prover_b200 needs a CUDA device; there is no CPU fallback")
+
+
+def stream_handle(stream=None) -> int:
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return s.cuda_stream
+
+
+def to_device(arr, device="cuda") -> torch.Tensor:
+    """numpy uint64 array -> int64 tensor on the device (same bits)."""
+    _require_cuda()
+    a = np.ascontiguousarray(np.asarray(arr, dtype=np.uint64))
+    return torch.from_numpy(a.view(np.int64)).to(device)
+
+
+def to_host(t: torch.Tensor) -> np.ndarray:
+    return t.detach().cpu().contiguous().numpy().view(np.uint64)
+
+
+def empty_fr(n: int, device="cuda") -> torch.Tensor:
+    _require_cuda()
+    return torch.empty((n, 4), dtype=torch.int64, device=device)
+
+
+def zeros_fr(n: int, device="cuda") -> torch.Tensor:
+    _require_cuda()
+    return torch.zeros((n, 4), dtype=torch.int64, device=device)
+
+
+def ptr(t) -> int:
+    return 0 if t is None else t.data_ptr()
+
+
+def ptr_array(tensors) -> torch.Tensor:
+    """Device array of device pointers (the reference's T** arguments)."""
+    _require_cuda()
+    return torch.tensor([t.data_ptr() for t in tensors], dtype=torch.int64, device="cuda")
+
+
+# ---------------------------------------------------------------- ntt.rs
+
+
+def generate_omega_buffers(omega, log_n: int, may_bit_reversed: bool = True, stream=None) -> torch.Tensor:
+    """src/cuda/ntt.rs:15-34: upload [1, omega] and expand to w^i, i < 2^log_n."""
+    buf = zeros_fr(1 << log_n)
+    one = np.asarray(omega, np.uint64).reshape(1, 4)
+    from_host = np.zeros((2, 4), np.uint64)
+    from_host[0] = _mont_one()
+    from_host[1] = one
+    buf[:2].copy_(to_device(from_host))
+    torch.cuda.synchronize()
+    abi.check(lib().expand_omega_buffer(ptr(buf), log_n, int(may_bit_reversed)), "expand_omega_buffer")
+    torch.cuda.synchronize()
+    return buf
+
+
+def _mont_one():
+    # 2^256 mod r as 4 u64 limbs
+    r = 0x30644E72E131A029B85045B68181585D2833E84879B9709143E1F593F0000001
+    one = (1 << 256) % r
+    return np.array([(one >> (64 * i)) & 0xFFFFFFFFFFFFFFFF for i in range(4)], np.uint64)
+
+
+def generate_ntt_buffers(omega, log_n: int):
+    """src/cuda/ntt.rs:36-59: (omegas_buf, pq_buf).  The pq table is unused by
+    this library's ntt and kept as a one-element placeholder."""
+    omegas = generate_omega_buffers(omega, log_n, True)
+    pq = zeros_fr(1)
+    return omegas, pq
+
+
+def ntt_raw(s_buf, tmp_buf, pq_buf, omegas_buf, log_n: int, intt_divisor=None, stream=None):
+    """src/cuda/ntt.rs:61-93: returns (s_buf, tmp_buf), swapped when the result
+    landed in tmp."""
+    swap = ctypes.c_bool(False)
+    err = lib().ntt(ptr(s_buf), ptr(tmp_buf), ptr(pq_buf), ptr(omegas_buf), ptr(intt_divisor), log_n, MAX_DEG,
+                    ctypes.addressof(swap), stream_handle(stream))
+    abi.check(err, "ntt")
+    if swap.value:
+        return tmp_buf, s_buf
+    return s_buf, tmp_buf
+
+
+def extended_prepare(s, coset_powers, coset_powers_n: int, size: int, extended_size: int, to_coset: bool,
+                     stream=None):
+    """src/cuda/ntt.rs:111-135."""
+    abi.check(lib().extended_prepare(ptr(s), ptr(coset_powers), coset_powers_n, size, extended_size,
+                                     1 if to_coset else 0, stream_handle(stream)), "extended_prepare")
+
+
+# ---------------------------------------------------------------- msm.rs
+
+
+def msm_window_bits(msm_count: int, length: int) -> int:
+    """src/cuda/msm.rs:105: the reference's window heuristic (its scratch sizing)."""
+    def log2_ceil(x):
+        return max(0, (x - 1).bit_length())
+    return min(log2_ceil(msm_count), 3) + 10 + max(log2_ceil(length), 22) - 22
+
+
+def batch_msm(points_buf, scalar_bufs, length: int, stream=None):
+    """src/cuda/msm.rs:239-455 through the drop-in msm + batch_msm_collect
+    symbols, with the reference's scratch sizing.  Returns Jacobian points as a
+    numpy (B, 12) uint64 array."""
+    threads, bits = 64, 254
+    count = len(scalar_bufs)
+    c = msm_window_bits(count, length)
+    windows = (bits + c - 1) // c
+    bucket_size = windows << c
+    max_worker = 128 * 512
+    worker = (length + threads - 1) // threads * threads if length < max_worker else max_worker
+    curve_buf_size = bucket_size + worker * 2
+    curve_buf = torch.empty((count * curve_buf_size, 12), dtype=torch.int64, device="cuda")
+    single = length * windows
+    sort_buf = torch.empty(max(1, single * 3), dtype=torch.int32, device="cuda")
+    idx = [torch.empty(max(1, single), dtype=torch.int32, device="cuda") for _ in range(4)]
+    acc_idx = [torch.empty(max(1, worker * 2), dtype=torch.int32, device="cuda") for _ in range(count)]
+    st = stream_handle(stream)
+    for i, s in enumerate(scalar_bufs):
+        err = lib().msm(curve_buf.data_ptr() + i * curve_buf_size * 96, ptr(points_buf), ptr(s), ptr(idx[0]),
+                        ptr(idx[1]), ptr(idx[2]), ptr(idx[3]), ptr(sort_buf), ptr(acc_idx[i]), length, windows, c,
+                        threads, worker, sort_buf.numel() * 4, 1, st)
+        abi.check(err, "msm")
+    abi.check(lib().batch_msm_collect(None, None, None, None, None, worker, windows, c, count, st),
+              "batch_msm_collect")
+    torch.cuda.synchronize()
+    rows = [curve_buf[i * curve_buf_size] for i in range(count)]
+    return to_host(torch.stack(rows))
+
+
+def msm_scratch(n: int, window_bits: int = 0) -> torch.Tensor:
+    nbytes = lib().zkp_msm_scratch_bytes(n, window_bits)
+    return torch.empty(max(1, nbytes), dtype=torch.uint8, device="cuda")
+
+
+def msm(points_buf, scalars_buf, n: int | None = None, window_bits: int = 0, scratch=None, out=None, stream=None):
+    """One MSM through zkp_msm; returns the 96-byte Jacobian result as a (12,)
+    int64 device tensor (no host synchronisation)."""
+    n = scalars_buf.shape[0] if n is None else n
+    if scratch is None:
+        scratch = msm_scratch(n, window_bits)
+    if out is None:
+        out = torch.empty(12, dtype=torch.int64, device="cuda")
+    err = lib().zkp_msm(ptr(out), ptr(points_buf), ptr(scalars_buf), n, window_bits, ptr(scratch),
+                        scratch.numel(), stream_handle(stream))
+    abi.check(err, "zkp_msm")
+    return out
+
+
+# ---------------------------------------------------------------- batched phases
+
+
+def twist_tables(shift, w_ext, log_n: int, ext_bits: int, stream=None) -> torch.Tensor:
+    t = empty_fr((1 << ext_bits) << log_n)
+    sh = to_device(np.asarray(shift, np.uint64).reshape(1, 4))
+    we = to_device(np.asarray(w_ext, np.uint64).reshape(1, 4))
+    abi.check(lib().zkp_coset_twist_tables(ptr(t), ptr(sh), ptr(we), log_n, ext_bits, None, stream_handle(stream)),
+              "zkp_coset_twist_tables")
+    torch.cuda.synchronize()
+    return t
+
+
+def extend_batch(ext_out, coeff_out, lagrange_in, ncols: int, log_n: int, ext_bits: int, tw_inv, n_inv, tw, twist,
+                 scratch, stage_events=None, stream=None):
+    """zkp_extend_batch: iNTT of ncols Lagrange columns, then the coset
+    evaluation on the 2^ext_bits-times larger domain.  stage_events: optional
+    ctypes array of 5 cudaEvent_t handles recorded around the stages."""
+    abi.check(lib().zkp_extend_batch(ptr(ext_out), ptr(coeff_out), ptr(lagrange_in), ncols, log_n, ext_bits,
+                                     ptr(tw_inv), ptr(n_inv), ptr(tw), ptr(twist), ptr(scratch),
+                                     None if stage_events is None else ctypes.addressof(stage_events),
+                                     stream_handle(stream)), "zkp_extend_batch")
+
+
+def ntt_batch(buf, tmp, omegas, log_n: int, ncols: int, scale=None, stream=None):
+    res = ctypes.c_int(0)
+    abi.check(lib().zkp_ntt_batch(ptr(buf), ptr(tmp), ptr(omegas), ptr(scale), log_n, ncols, 1 << log_n,
+                                  ctypes.addressof(res), stream_handle(stream)), "zkp_ntt_batch")
+    return tmp if res.value else buf
+
+
+def scan_scratch(n: int) -> torch.Tensor:
+    return empty_fr(max(1, lib().zkp_scan_scratch_elems(n)))
+
+
+def batch_inverse(out, inp, c=None, accumulate=False, stream=None):
+    abi.check(lib().zkp_batch_inverse(ptr(out), ptr(inp), ptr(c), inp.shape[0], int(accumulate),
+                                      stream_handle(stream)), "zkp_batch_inverse")
+
+
+def grand_product(out, inp, init=None, scratch=None, stream=None):
+    n = inp.shape[0]
+    scratch = scan_scratch(n) if scratch is None else scratch
+    abi.check(lib().zkp_grand_product(ptr(out), ptr(inp), n, ptr(init), ptr(scratch), stream_handle(stream)),
+              "zkp_grand_product")
+
+
+def grand_sum(out, inp, init=None, scratch=None, stream=None):
+    n = inp.shape[0]
+    scratch = scan_scratch(n) if scratch is None else scratch
+    abi.check(lib().zkp_grand_sum(ptr(out), ptr(inp), n, ptr(init), ptr(scratch), stream_handle(stream)),
+              "zkp_grand_sum")
