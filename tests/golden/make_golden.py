@@ -12,6 +12,7 @@ is called the way the reference's Rust host calls it:
   eval_logup_z_compose        src/lib.rs:662
 """
 import ctypes
+import json
 import os
 import sys
 
@@ -124,7 +125,35 @@ def main(out):
     torch.cuda.synchronize()
     g["logup_table"], g["logup_m"], g["logup_z"], g["logup_last_z"] = table, m, host(z), host(last)
     np.savez_compressed(out, **g)
+    write_json(g, os.path.join(os.path.dirname(out), "reference_kernels.json"))
     print("wrote", out, sorted(g))
+
+
+def sha(a):
+    import hashlib
+
+    return hashlib.sha256(np.ascontiguousarray(a, np.uint64).tobytes()).hexdigest()
+
+
+def write_json(g, path):
+    """Compact fixture: seeds of the inputs, hashes of large outputs, small
+    outputs in full."""
+    out = {"generator": "tests/golden/make_golden.py on a B200 (reference cuda/bn254.cu + cuda/msm.cu rebuilt "
+                        "for sm_100a)",
+           "inputs": "oracle.rand_fr(n, seed) (splitmix64, rejection below r, Montgomery form)",
+           "ntt": [], "msm": [], "logup": {}}
+    for k in (10, 13):
+        out["ntt"].append({"log_n": k, "seed": 7000 + k, "forward_sha256": sha(g[f"ntt_out_{k}"]),
+                           "inverse_sha256": sha(g[f"intt_out_{k}"])})
+    for tag, n in (("msm_small", 100), ("msm_2_14", 1 << 14)):
+        out["msm"].append({"n": n, "dlog_seed": 8000 + n, "scalar_seed": 9000 + n,
+                           "jacobian_out": [int(x) for x in g[f"{tag}_out"].reshape(-1)]})
+    n = 1 << 16
+    out["logup"] = {"n": n, "input_seed": 10001, "beta_seed": 10002, "table_seed": 10003, "m": "i % 5",
+                    "last_z_index": n - 17, "sum_sha256": sha(g["logup_sum"]), "z_sha256": sha(g["logup_z"]),
+                    "last_z": [int(x) for x in g["logup_last_z"].reshape(-1)]}
+    with open(path, "w") as f:
+        json.dump(out, f, indent=1)
 
 
 if __name__ == "__main__":
