@@ -145,7 +145,8 @@ def test_lookup_eval_h(env):
     e, O = env, env.O
     c = e.cols
     res0, res = _res(e, 7)
-    assert e.L.lookup_eval_h(P(res), *[P(e.dev(x)) for x in c[:8]], P(e.dev(c[0])), P(e.dev(e.y)),
+    # res, input, table, permuted_input, permuted_table, z, l0, l_last, l_active_row, y, beta, gamma
+    assert e.L.lookup_eval_h(P(res), *[P(e.dev(x)) for x in c[:8]], P(e.dev(e.y)),
                              P(e.dev(e.beta)), P(e.dev(e.gamma)), 1, N, e.st) == 0
     # restated from cuda/bn254.cu:798-865
     inp, tab, pin, ptab, z, l0, ll, la = c[0], c[1], c[2], c[3], c[4], c[5], c[6], c[7]
@@ -156,13 +157,13 @@ def test_lookup_eval_h(env):
     t = O.mul(t, e.y)
     u = O.mul(O.mul(O.add(pin, e.beta), O.add(ptab, e.gamma)), O._rot(z, 1))
     u = O.sub(u, O.mul(z, O.mul(inp, tab)))
-    t = O.add(t, O.mul(u, c[0]))
+    t = O.add(t, O.mul(u, la))
     t = O.mul(t, e.y)
     p = O.sub(pin, ptab)
     t = O.add(t, O.mul(l0, p))
     t = O.mul(t, e.y)
     u = O.mul(O.sub(pin, O._rot(pin, -1)), p)
-    t = O.add(t, O.mul(u, c[0]))
+    t = O.add(t, O.mul(u, la))
     assert (_get(e, res) == t).all()
 
 

@@ -72,6 +72,33 @@ class CudaError(RuntimeError):
     pass
 
 
+class _Strict:
+    """The CDLL with every declared function wrapped in an exact-arity check:
+    ctypes otherwise passes surplus arguments as varargs, which silently
+    shifts every later argument (a stream handle becomes garbage)."""
+
+    def __init__(self, cdll):
+        self._cdll = cdll
+        for name, sig in SIGNATURES.items():
+            fn = getattr(cdll, name)
+            argtypes, restype = sig if isinstance(sig, tuple) else (sig, E)
+            fn.argtypes, fn.restype = argtypes, restype
+            setattr(self, name, self._wrap(name, fn, len(argtypes)))
+
+    @staticmethod
+    def _wrap(name, fn, arity):
+        def call(*args):
+            if len(args) != arity:
+                raise TypeError(f"{name} takes {arity} arguments, got {len(args)}")
+            return fn(*args)
+
+        call.__name__ = name
+        return call
+
+    def __getattr__(self, name):
+        return getattr(self._cdll, name)
+
+
 def load_library(path: str = LIB_PATH):
     """Load the kernel library; raises if it has not been built."""
     global _lib
@@ -79,13 +106,7 @@ def load_library(path: str = LIB_PATH):
         return _lib
     if not os.path.exists(path):
         raise ImportError(f"{path} is missing: run __graft_entry__.build() (make -C csrc)")
-    lib = ctypes.CDLL(path, mode=ctypes.RTLD_GLOBAL)
-    for name, sig in SIGNATURES.items():
-        fn = getattr(lib, name)
-        if isinstance(sig, tuple):
-            fn.argtypes, fn.restype = sig
-        else:
-            fn.argtypes, fn.restype = sig, E
+    lib = _Strict(ctypes.CDLL(path, mode=ctypes.RTLD_GLOBAL))
     if path == LIB_PATH:
         _lib = lib
     return lib

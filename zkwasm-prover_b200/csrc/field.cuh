@@ -219,27 +219,100 @@ ZK_HD void fe_reduce_once(uint32_t t[8]) {
     select8(t, br, t, u);
 }
 
+// acc[0..8] += a[P] * b, a[P+2] * b, a[P+4] * b, a[P+6] * b with the four
+// 64-bit products laid side by side (lo at word 2k, hi at word 2k+1): one
+// carry chain.  P = 0 gives the even-limb products (positions 0..7 of the
+// running sum), P = 1 the odd-limb ones (positions 1..8, stored from word 0).
+template <int P>
+ZK_HD void chain4(uint32_t acc[9], const uint32_t a[8], uint32_t b) {
+#if defined(__CUDA_ARCH__)
+    asm("mad.lo.cc.u32  %0, %9,  %13, %0;\n\t"
+        "madc.hi.cc.u32 %1, %9,  %13, %1;\n\t"
+        "madc.lo.cc.u32 %2, %10, %13, %2;\n\t"
+        "madc.hi.cc.u32 %3, %10, %13, %3;\n\t"
+        "madc.lo.cc.u32 %4, %11, %13, %4;\n\t"
+        "madc.hi.cc.u32 %5, %11, %13, %5;\n\t"
+        "madc.lo.cc.u32 %6, %12, %13, %6;\n\t"
+        "madc.hi.cc.u32 %7, %12, %13, %7;\n\t"
+        "addc.u32       %8, %8, 0;"
+        : "+r"(acc[0]), "+r"(acc[1]), "+r"(acc[2]), "+r"(acc[3]), "+r"(acc[4]), "+r"(acc[5]), "+r"(acc[6]),
+          "+r"(acc[7]), "+r"(acc[8])
+        : "r"(a[P]), "r"(a[P + 2]), "r"(a[P + 4]), "r"(a[P + 6]), "r"(b));
+#else
+    uint64_t c = 0;
+    for (int k = 0; k < 4; k++) {
+        const uint64_t p = (uint64_t)a[P + 2 * k] * b;
+        uint64_t s = (uint64_t)acc[2 * k] + (uint32_t)p + c;
+        acc[2 * k] = (uint32_t)s;
+        c = s >> 32;
+        s = (uint64_t)acc[2 * k + 1] + (uint32_t)(p >> 32) + c;
+        acc[2 * k + 1] = (uint32_t)s;
+        c = s >> 32;
+    }
+    acc[8] = (uint32_t)(acc[8] + c);
+#endif
+}
+
+// o[0..7] += e[1..8], carry into o[8]
+ZK_HD void merge_shift(uint32_t o[9], const uint32_t e[9]) {
+#if defined(__CUDA_ARCH__)
+    asm("add.cc.u32  %0, %0, %9;\n\t"
+        "addc.cc.u32 %1, %1, %10;\n\t"
+        "addc.cc.u32 %2, %2, %11;\n\t"
+        "addc.cc.u32 %3, %3, %12;\n\t"
+        "addc.cc.u32 %4, %4, %13;\n\t"
+        "addc.cc.u32 %5, %5, %14;\n\t"
+        "addc.cc.u32 %6, %6, %15;\n\t"
+        "addc.cc.u32 %7, %7, %16;\n\t"
+        "addc.u32    %8, %8, 0;"
+        : "+r"(o[0]), "+r"(o[1]), "+r"(o[2]), "+r"(o[3]), "+r"(o[4]), "+r"(o[5]), "+r"(o[6]), "+r"(o[7]),
+          "+r"(o[8])
+        : "r"(e[1]), "r"(e[2]), "r"(e[3]), "r"(e[4]), "r"(e[5]), "r"(e[6]), "r"(e[7]), "r"(e[8]));
+#else
+    uint64_t c = 0;
+    for (int j = 0; j < 8; j++) {
+        uint64_t s = (uint64_t)o[j] + e[j + 1] + c;
+        o[j] = (uint32_t)s;
+        c = s >> 32;
+    }
+    o[8] = (uint32_t)(o[8] + c);
+#endif
+}
+
 // Montgomery product a * b * 2^-256 mod m; a, b < 2m, result < m.
+//
+// Operand scanning with the running sum T split into an even accumulator E
+// (products of even limbs of a) and an odd accumulator O (odd limbs, one word
+// up): T = E + 2^32 O.  Each row adds a * b_i and q * m (q = E_0 * -m^-1) as
+// four independent carry chains of alternating mad.lo / mad.hi over the same
+// operands, then folds E >> 32 into O, which becomes the next row's E.  This
+// measured about 1.5x the rate of the lo-chain / hi-chain row form on B200.
 template <class C>
 ZK_HD Fe<C> fe_mul(const Fe<C>& a, const Fe<C>& b) {
-    uint32_t t[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     uint32_t m[8];
 #pragma unroll
     for (int j = 0; j < 8; j++) m[j] = C::M(j);
+    uint32_t e[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    uint32_t o[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll
     for (int i = 0; i < 8; i++) {
-        row_mad(t, a.v, b.v[i]);
-        uint32_t q = t[0] * C::INV;
-        row_mad(t, m, q);
-        // t[0] is now zero: shift one word down
+        chain4<0>(e, a.v, b.v[i]);
+        chain4<1>(o, a.v, b.v[i]);
+        const uint32_t q = e[0] * C::INV;
+        chain4<0>(e, m, q);
+        chain4<1>(o, m, q);
+        // e[0] is now zero: T / 2^32 = (E >> 32) + O
+        merge_shift(o, e);
 #pragma unroll
-        for (int j = 0; j < 8; j++) t[j] = t[j + 1];
-        t[8] = 0;
+        for (int j = 0; j < 9; j++) {
+            e[j] = o[j];
+            o[j] = 0;
+        }
     }
-    fe_reduce_once<C>(t);
+    fe_reduce_once<C>(e);
     Fe<C> r;
 #pragma unroll
-    for (int j = 0; j < 8; j++) r.v[j] = t[j];
+    for (int j = 0; j < 8; j++) r.v[j] = e[j];
     return r;
 }
 
