@@ -254,6 +254,19 @@ cudaError_t zkp_permutation_z(void *z, const void *cols, const void *sigmas, int
 cudaError_t zkp_shuffle_z(void *z, const void *inputs, const void *tables, const void *betas, int groups, uint32_t n,
                           void *scratch, cudaStream_t stream);
 
+/* No counterpart in the reference.  zkp_msm without caller-supplied scratch,
+ * for callers that cannot allocate device memory: a host whose device memory
+ * is all owned by its own pool, code running during CUDA-graph capture, or a
+ * latency-critical path that cannot afford cudaMalloc's implicit device
+ * synchronisation.  out (96-byte Jacobian) = sum_i [scalars_i] bases_i for
+ * n <= 16384 points; larger n returns cudaErrorInvalidValue without launching.
+ * The scratch is a 9 MiB __device__ array inside the library (one per GPU
+ * that loads it, held until exit) shared by every call: calls that overlap on
+ * the GPU race, so order them on one stream.  The first call on a device looks
+ * up the array's address (cudaGetSymbolAddress) and should come before any
+ * stream capture.  Calls cudaMalloc, cudaFree or no allocating routine. */
+cudaError_t zkp_msm_static(void *out, const void *bases, const void *scalars, uint32_t n, cudaStream_t stream);
+
 /* ======================================================================
  * Part 3: calibration
  * ==================================================================== */

@@ -62,6 +62,7 @@ SIGNATURES = {
     "zkp_grand_sum": [P, P, U, P, P, S],
     "zkp_permutation_z": [P, P, P, I, P, P, P, P, P, U, P, S],
     "zkp_shuffle_z": [P, P, P, P, I, U, P, S],
+    "zkp_msm_static": [P, P, P, U, S],
     "zkp_calib_mont_rate": [P, U, U, S],
 }
 
