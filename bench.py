@@ -231,6 +231,42 @@ def cpu_baseline_port(log_n=20, ext_bits=3, reps=1):
                       f"{sec:.2f} s each"}
 
 
+def msm_inputs(zkp, n, seed, device):
+    """n bases [k_i]G with seeded 64-bit k_i (generated on the device) and n
+    seeded scalars below 2^253."""
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    k = torch.randint(0, 2 ** 62, (n,), dtype=torch.int64, device=device, generator=g)
+    bases = torch.empty((n, 8), dtype=torch.int64, device=device)
+    zkp.abi.check(zkp.load_library().zkp_g1_multiples(bases.data_ptr(), k.data_ptr(), n,
+                                                        torch.cuda.current_stream().cuda_stream), "g1_multiples")
+    return bases, random_fr(n, seed + 1, device)
+
+
+def run_msm(zkp, device, sizes=(1 << 18, 1 << 22), reps=5):
+    """Single MSMs through zkp_msm on device-resident bases and scalars."""
+    H = zkp.host
+    res = []
+    for n in sizes:
+        bases, scalars = msm_inputs(zkp, n, 77 + n.bit_length(), device)
+        scratch = H.msm_scratch(n)
+        out = torch.empty(12, dtype=torch.int64, device=device)
+        for _ in range(2):
+            H.msm(bases, scalars, n=n, scratch=scratch, out=out)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(reps):
+            H.msm(bases, scalars, n=n, scratch=scratch, out=out)
+        b.record()
+        b.synchronize()
+        ms = a.elapsed_time(b) / reps
+        c = zkp.load_library().zkp_msm_default_window(n)
+        res.append({"n": n, "ms": round(ms, 4), "mpts_per_s": round(n / ms / 1e3, 2), "window_bits": c})
+        del bases, scalars, scratch
+    return res
+
+
 def run_e2e(ph, steps):
     """Same phase through the C ABI with host buffers: pinned Lagrange columns
     copied in and coefficients copied out every step, overlapped by chunk on
@@ -364,6 +400,7 @@ def run_ours(args):
             with open(prof) as f:
                 traffic = json.load(f).get("stage_traffic_bytes", [None] * 4)[dom]
         cpu = cpu_baseline_port(args.log_n, args.ext_bits) if not args.no_cpu_baseline else None
+        msm = run_msm(zkp, device) if not args.no_msm else None
         out = {
             "metric": f"NTT HBM GB/s: batched iNTT 2^{args.log_n} -> coset NTT 2^{args.log_n + args.ext_bits}, "
                       f"{args.columns} columns",
@@ -402,6 +439,7 @@ def run_ours(args):
             },
             "stage_ms": [round(x, 4) for x in stage_ms],
             "cpu_baseline": cpu,
+            "msm": msm,
         }
         if clk:
             out["clocks"] = clk
@@ -411,6 +449,119 @@ def run_ours(args):
         dist.destroy_process_group()
     if out is not None:
         print(json.dumps(out))
+
+
+def reference_gpu_timings(args):
+    """The reference's own CUDA kernels (cuda/bn254.cu + cuda/msm.cu, rebuilt
+    unmodified for sm_100a into oracle/_ref/) on the same phase, called the
+    way its Rust host calls them: per column ntt (iNTT, src/cuda/ntt.rs:61-93),
+    extended_prepare + ntt at the extended size (src/eval_h.rs:255-265), and
+    msm + batch_msm_collect (src/cuda/msm.rs:239-455) for single MSMs."""
+    path = os.path.join(ROOT, "oracle", "_ref", "libzkwasm_prover_kernel_ref.so")
+    if not os.path.exists(path) or not torch.cuda.is_available():
+        return {"unavailable": "oracle/_ref not built or no GPU"}
+    import numpy as np
+
+    L = ctypes.CDLL(path)
+    VP = ctypes.c_void_p
+    dev = torch.device("cuda", 0)
+    st = torch.cuda.current_stream().cuda_stream
+    p = lambda t: ctypes.c_void_p(t.data_ptr()) if t is not None else None
+
+    def tables(log_n, inverse):
+        n = 1 << log_n
+        w = omega(log_n)
+        if inverse:
+            w = pow(w, -1, R_MOD)
+        om = torch.zeros((n, 4), dtype=torch.int64, device=dev)
+        om[:2] = fr_tensor([1, w], dev)
+        torch.cuda.synchronize()
+        assert L.expand_omega_buffer(p(om), log_n, 1) == 0
+        md = min(8, log_n)
+        tw = pow(w, n >> md, R_MOD)
+        pq = fr_tensor([pow(tw, i, R_MOD) for i in range((1 << md) >> 1)], dev)
+        torch.cuda.synchronize()
+        return om, pq
+
+    out = {}
+    # NTT phase: C columns, iNTT 2^k then zeta-coset extension to 2^(k+e)
+    k, e, C = args.log_n, args.ext_bits, args.columns
+    n, N = 1 << k, 1 << (k + e)
+    om_i, pq_i = tables(k, True)
+    om_f, pq_f = tables(k + e, False)
+    ninv = fr_tensor([pow(n, -1, R_MOD)], dev)
+    zeta = pow(GENERATOR, (R_MOD - 1) // 3, R_MOD)
+    cp = fr_tensor([zeta, zeta * zeta % R_MOD], dev)
+    lag = random_fr(C * n, 5, dev)
+    tmp = torch.empty((n, 4), dtype=torch.int64, device=dev)
+    ext = torch.empty((N, 4), dtype=torch.int64, device=dev)
+    text = torch.empty((N, 4), dtype=torch.int64, device=dev)
+    swap = ctypes.c_bool(False)
+
+    def phase():
+        for c in range(C):
+            col = lag[c * n:(c + 1) * n]
+            assert L.ntt(p(col), p(tmp), p(pq_i), p(om_i), p(ninv), k, 8, ctypes.byref(swap), VP(st)) == 0
+            coeff = tmp if swap.value else col
+            ext[:n].copy_(coeff)
+            assert L.extended_prepare(p(ext), p(cp), 3, n, N, 0, VP(st)) == 0
+            assert L.ntt(p(ext), p(text), p(pq_f), p(om_f), None, k + e, 8, ctypes.byref(swap), VP(st)) == 0
+
+    phase()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    phase()
+    b.record()
+    b.synchronize()
+    ms = a.elapsed_time(b)
+    out["ntt_phase"] = {"ms_per_step": round(ms, 3),
+                        "value": round(C * (3 + (1 << e)) * n * 32 / (ms / 1e3) / 1e9, 3), "unit": "GB/s",
+                        "flow": "per column: ntt(iNTT 2^k) -> copy -> extended_prepare(zeta) -> ntt(2^(k+e))"}
+    del lag, tmp, ext, text
+    # single MSMs
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    res = []
+    for nn in (1 << 18, 1 << 22):
+        d = O.rand_fr(nn, 901)
+        bases = torch.from_numpy(O.g1_gen_bases(d).view(np.int64)).to(dev)
+        sc = torch.from_numpy(O.rand_fr(nn, 902).view(np.int64)).to(dev)
+        c = 10 + max((nn - 1).bit_length(), 22) - 22
+        windows = (254 + c - 1) // c
+        bucket = windows << c
+        worker = (nn + 63) // 64 * 64 if nn < 128 * 512 else 128 * 512
+        curve = torch.empty((bucket + 2 * worker, 12), dtype=torch.int64, device=dev)
+        single = nn * windows
+        idx = [torch.empty(single, dtype=torch.int32, device=dev) for _ in range(4)]
+        sort = torch.empty(3 * single, dtype=torch.int32, device=dev)
+        acc = torch.empty(2 * worker, dtype=torch.int32, device=dev)
+        ptrs = lambda xs: torch.tensor(xs, dtype=torch.int64, device=dev)
+        base = curve.data_ptr()
+        ri, nri = ptrs([acc.data_ptr()]), ptrs([acc.data_ptr() + worker * 4])
+        ra, nra = ptrs([base + bucket * 96]), ptrs([base + (bucket + worker) * 96])
+        bk = ptrs([base])
+
+        def one():
+            assert L.msm(p(curve), p(bases), p(sc), p(idx[0]), p(idx[1]), p(idx[2]), p(idx[3]), p(sort), p(acc),
+                         nn, windows, c, 64, worker, 3 * single * 4, 1, VP(st)) == 0
+            assert L.batch_msm_collect(p(ri), p(ra), p(nri), p(nra), p(bk), worker, windows, c, 1, VP(st)) == 0
+
+        one()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        reps = 3
+        for _ in range(reps):
+            one()
+        torch.cuda.synchronize()
+        ms = (time.perf_counter() - t0) / reps * 1e3
+        ok = bool((O.g1_jac_to_aff(curve[0:1].cpu().numpy().view(np.uint64)) == O.msm_known_dlog(d, O.rand_fr(nn, 902))).all())
+        res.append({"n": nn, "ms": round(ms, 3), "mpts_per_s": round(nn / ms / 1e3, 2), "window_bits": c,
+                    "matches_oracle": ok})
+        del bases, sc, curve, idx, sort, acc
+    out["msm"] = res
+    return out
 
 
 def run_reference(args):
@@ -439,6 +590,8 @@ def run_reference(args):
         "cpu_baseline": cb,
         "e2e": {"value": round(v, 4), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    if not args.no_reference_gpu:
+        out["reference_gpu_sm100a"] = reference_gpu_timings(args)
     print(json.dumps(out))
 
 
@@ -453,6 +606,8 @@ def main():
     ap.add_argument("--ext-bits", type=int, default=3)
     ap.add_argument("--chunk", type=int, default=8)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-msm", action="store_true")
+    ap.add_argument("--no-reference-gpu", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

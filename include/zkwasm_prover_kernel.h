@@ -230,6 +230,11 @@ cudaError_t zkp_extend_batch(void *ext_out, void *coeff_out, const void *lagrang
 cudaError_t zkp_batch_inverse(void *out, const void *in, const void *c, uint32_t n, int accumulate,
                               cudaStream_t stream);
 
+/* out[i] = [k64[i]] G as affine points (identity (0, 0) for k = 0), with
+ * G = (1, 2) the BN254 G1 generator and k64 a device array of n u64: bases
+ * with known discrete logarithms for benchmarks and SRS-style test data. */
+cudaError_t zkp_g1_multiples(void *out, const void *k64, uint32_t n, cudaStream_t stream);
+
 /* Scratch elements (32 bytes each) the prefix scans need for n elements. */
 size_t zkp_scan_scratch_elems(uint32_t n);
 

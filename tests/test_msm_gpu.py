@@ -87,6 +87,22 @@ def test_msm_known_dlog_2_18(O, gpu):
     assert (_jac_to_aff(O, _run(gpu, bases, s)) == O.msm_known_dlog(d, s)).all()
 
 
+def test_g1_multiples_generator(O, gpu):
+    # device-generated bases with known 64-bit discrete logs (benchmark data)
+    H = gpu.host
+    rng = np.random.default_rng(5)
+    k = rng.integers(0, 2 ** 63, 4096, dtype=np.int64).astype(np.uint64)
+    k[:3] = [0, 1, 2]
+    kd = torch.from_numpy(k.view(np.int64)).cuda()
+    out = torch.empty((k.shape[0], 8), dtype=torch.int64, device="cuda")
+    gpu.abi.check(gpu.load_library().zkp_g1_multiples(out.data_ptr(), kd.data_ptr(), k.shape[0], H.stream_handle()))
+    got = H.to_host(out)
+    dl = O.fr_vec([int(x) for x in k])
+    assert (got == O.g1_gen_bases(dl)).all()
+    s = O.rand_fr(k.shape[0], 6)
+    assert (_jac_to_aff(O, _run(gpu, got, s)) == O.msm_known_dlog(dl, s)).all()
+
+
 def test_reference_abi_batch_msm(O, gpu):
     # msm() per column + batch_msm_collect, buffers sized like src/cuda/msm.rs
     H = gpu.host

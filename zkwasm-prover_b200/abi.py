@@ -58,6 +58,7 @@ SIGNATURES = {
     "zkp_extend_batch": [P, P, P, U, I, I, P, P, P, P, P, P, S],
     "zkp_batch_inverse": [P, P, P, U, I, S],
     "zkp_scan_scratch_elems": ([U], SZ),
+    "zkp_g1_multiples": [P, P, U, S],
     "zkp_grand_product": [P, P, U, P, P, S],
     "zkp_grand_sum": [P, P, U, P, P, S],
     "zkp_permutation_z": [P, P, P, I, P, P, P, P, P, U, P, S],

@@ -30,6 +30,34 @@ __global__ void twist_kernel(Fr* twist, const Fr* shift, const Fr* w_ext, uint32
     }
 }
 
+// out[i] = [k_i] G (affine, Montgomery form) for 64-bit k_i; G = (1, 2)
+__global__ void g1_multiples_kernel(Aff* out, const uint64_t* k64, uint32_t n) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint64_t k = k64[i];
+    Fq g1 = fe_zero<FqCfg>(), g2 = fe_zero<FqCfg>();
+    g1.v[0] = 1;
+    g2.v[0] = 2;
+    g1 = fe_to_mont<FqCfg>(g1);
+    g2 = fe_to_mont<FqCfg>(g2);
+    Xyzz acc = xyzz_identity();
+    for (int b = 63; b >= 0; b--) {
+        acc = xyzz_dbl(acc);
+        if ((k >> b) & 1) acc = xyzz_add_aff(acc, g1, g2);
+    }
+    Aff a;
+    if (xyzz_is_id(acc)) {
+        a.x = fe_zero<FqCfg>();
+        a.y = fe_zero<FqCfg>();
+    } else {
+        const Fq inv = fe_inv<FqCfg>(fe_mul<FqCfg>(acc.zz, acc.zzz));
+        a.x = fe_mul<FqCfg>(fe_mul<FqCfg>(acc.x, acc.zzz), inv);
+        a.y = fe_mul<FqCfg>(fe_mul<FqCfg>(acc.y, acc.zz), inv);
+    }
+    st_elem<FqCfg>(&out[i].x, a.x);
+    st_elem<FqCfg>(&out[i].y, a.y);
+}
+
 }  // namespace zk
 
 extern "C" {
@@ -434,6 +462,14 @@ cudaError_t zkp_batch_inverse(void* out, const void* in, const void* c, uint32_t
 }
 
 size_t zkp_scan_scratch_elems(uint32_t n) { return fr_scan_tmp_elems(n); }
+
+cudaError_t zkp_g1_multiples(void* out, const void* k64, uint32_t n, cudaStream_t stream) {
+    if (n && (!out || !k64)) return cudaErrorInvalidValue;
+    if (n == 0) return cudaSuccess;
+    zk::g1_multiples_kernel<<<(n + 127) / 128, 128, 0, stream>>>(reinterpret_cast<Aff*>(out),
+                                                                 reinterpret_cast<const uint64_t*>(k64), n);
+    return cudaGetLastError();
+}
 
 cudaError_t zkp_grand_product(void* out, const void* in, uint32_t n, const void* init, void* scratch,
                               cudaStream_t stream) {

@@ -59,8 +59,27 @@ __device__ __forceinline__ void dft8_dif(Fr v[8], const Fr& w8, const Fr& w4, co
     dft4_dif(v[4], v[5], v[6], v[7], w4);
 }
 
-__device__ __forceinline__ Fr sm_ld(const Fr* p) { return ld_elem<FrCfg>(p); }
-__device__ __forceinline__ void sm_st(Fr* p, const Fr& v) { st_elem<FrCfg>(p, v); }
+// Shared-memory tiles hold 32-byte elements as two 16-byte halves.  Element
+// p, half h lives at 16-byte slot 2 * (p ^ ((p >> 3) & 3)) + (h ^ (((p >> 2) ^
+// (p >> 5)) & 1)): a bijection on each tile that gives the eight threads of a
+// quarter-warp eight distinct bank groups both for runs of consecutive elements
+// and for the stride-8 writes of the first radix-8 sub-stage.
+__device__ __forceinline__ uint4* sm_slot(Fr* x, uint32_t p, uint32_t h) {
+    const uint32_t pp = p ^ ((p >> 3) & 3u);
+    const uint32_t hh = h ^ (((p >> 2) ^ (p >> 5)) & 1u);
+    return reinterpret_cast<uint4*>(x) + 2 * pp + hh;
+}
+__device__ __forceinline__ Fr sm_ld(Fr* x, uint32_t p) {
+    const uint4 a = *sm_slot(x, p, 0), b = *sm_slot(x, p, 1);
+    Fr r;
+    r.v[0] = a.x; r.v[1] = a.y; r.v[2] = a.z; r.v[3] = a.w;
+    r.v[4] = b.x; r.v[5] = b.y; r.v[6] = b.z; r.v[7] = b.w;
+    return r;
+}
+__device__ __forceinline__ void sm_st(Fr* x, uint32_t p, const Fr& v) {
+    *sm_slot(x, p, 0) = make_uint4(v.v[0], v.v[1], v.v[2], v.v[3]);
+    *sm_slot(x, p, 1) = make_uint4(v.v[4], v.v[5], v.v[6], v.v[7]);
+}
 
 // output-side work of the last sub-stage: the inter-pass twiddle w_n^{P*Q*y}
 // and the optional scale
@@ -86,7 +105,7 @@ __device__ __forceinline__ void stage8(Fr* x, int u, int log_ps, bool last, cons
     constexpr int S = R / 8;
     Fr v[8];
 #pragma unroll
-    for (int i = 0; i < 8; i++) v[i] = sm_ld(x + u + S * i);
+    for (int i = 0; i < 8; i++) v[i] = sm_ld(x, u + S * i);
     __syncthreads();
     if (in_mul) {
 #pragma unroll
@@ -111,7 +130,7 @@ __device__ __forceinline__ void stage8(Fr* x, int u, int log_ps, bool last, cons
             y = fe_mul<FrCfg>(y, ldg_elem<FrCfg>(tw + ((size_t)((ilo * j) << log_ps) << sh)));
         const int pos = J + (j << log_ps) + (ilo << (log_ps + 3));
         if (last) y = finish_out(po, y, (uint32_t)pos);
-        sm_st(x + pos, y);
+        sm_st(x, pos, y);
     }
     __syncthreads();
 }
@@ -128,7 +147,7 @@ __device__ __forceinline__ void stage4_last(Fr* x, int lt, const Fr* tw, int log
     for (int k = 0; k < 2; k++) {
         int u = lt + k * TH;
 #pragma unroll
-        for (int i = 0; i < 4; i++) v[4 * k + i] = sm_ld(x + u + S * i);
+        for (int i = 0; i < 4; i++) v[4 * k + i] = sm_ld(x, u + S * i);
     }
     __syncthreads();
     const int sh = log_n - LOGR;
@@ -147,7 +166,7 @@ __device__ __forceinline__ void stage4_last(Fr* x, int lt, const Fr* tw, int log
 #pragma unroll
         for (int j = 0; j < 4; j++) {
             const int pos = u + S * j;  // J = u, P_s = S, ilo = 0
-            sm_st(x + pos, finish_out(po, v[4 * k + rev[j]], (uint32_t)pos));
+            sm_st(x, pos, finish_out(po, v[4 * k + rev[j]], (uint32_t)pos));
         }
     }
     __syncthreads();
@@ -163,16 +182,16 @@ __device__ __forceinline__ void stage2_last(Fr* x, int lt, const PassOut& po) {
 #pragma unroll
     for (int k = 0; k < 4; k++) {
         int u = lt + k * TH;
-        v[2 * k] = sm_ld(x + u);
-        v[2 * k + 1] = sm_ld(x + u + S);
+        v[2 * k] = sm_ld(x, u);
+        v[2 * k + 1] = sm_ld(x, u + S);
     }
     __syncthreads();
 #pragma unroll
     for (int k = 0; k < 4; k++) {
         int u = lt + k * TH;
         dft2(v[2 * k], v[2 * k + 1]);
-        sm_st(x + u, finish_out(po, v[2 * k], (uint32_t)u));
-        sm_st(x + u + S, finish_out(po, v[2 * k + 1], (uint32_t)(u + S)));
+        sm_st(x, u, finish_out(po, v[2 * k], (uint32_t)u));
+        sm_st(x, u + S, finish_out(po, v[2 * k + 1], (uint32_t)(u + S)));
     }
     __syncthreads();
 }
@@ -196,7 +215,7 @@ ntt_pass_kernel(NttPassArgs a) {
         const int h = c & 1, e = c >> 1;
         const int g = e % G, i = e / G;
         const size_t gi = (size_t)(q0 + g) + ((size_t)i << log_items);
-        reinterpret_cast<uint4*>(sm + g * R + i)[h] = reinterpret_cast<const uint4*>(src + gi)[h];
+        *sm_slot(sm + g * R, i, h) = reinterpret_cast<const uint4*>(src + gi)[h];
     }
     __syncthreads();
 
@@ -239,7 +258,7 @@ ntt_pass_kernel(NttPassArgs a) {
         const uint32_t qq = q0 + gg;
         const size_t pos = (size_t)(qq & pm) + ((size_t)j << a.log_p) + ((size_t)(qq >> a.log_p) << (a.log_p + LOGR));
         const size_t o = (pos << a.out_shift) + zoff;
-        reinterpret_cast<uint4*>(dst + o)[h] = reinterpret_cast<const uint4*>(sm + gg * R + j)[h];
+        reinterpret_cast<uint4*>(dst + o)[h] = *sm_slot(sm + gg * R, j, h);
     }
 }
 
