@@ -144,7 +144,7 @@ class ExtendPhase:
         self.tw = H.generate_omega_buffers(mont(w), log_n)
         self.tw_inv = H.generate_omega_buffers(mont(pow(w, -1, R_MOD)), log_n)
         self.n_inv = fr_tensor([pow(n, -1, R_MOD)], device)
-        self.twist = H.twist_tables(mont(GENERATOR), mont(omega(log_n + ext_bits)), log_n, ext_bits)
+        self.twist = H.twist_tables(mont(GENERATOR), mont(omega(log_n + ext_bits)), log_n, ext_bits, self.tw)
         self.lag = random_fr(columns * n, seed, device)
         self.coeff = torch.empty((columns * n, 4), dtype=torch.int64, device=device)
         self.ext = torch.empty((columns * E * n, 4), dtype=torch.int64, device=device)
@@ -160,14 +160,31 @@ class ExtendPhase:
         ntt = (n // 2) * lg
         return ntt + n + E * (ntt + n)  # iNTT + n^-1 scale, E sub-transforms + twist
 
+    def fused(self):
+        """zkp_extend_batch fuses the last inverse pass with the first coset
+        passes when its coset table carries the per-radix factors."""
+        return self.zkp.load_library().zkp_coset_table_elems(self.log_n, self.e) > self.E * self.n
+
+    def stage_names(self):
+        if self.fused():
+            return ["intt_pass1", "none", "fused_intt_pass2_coset_pass1", "coset_pass2"]
+        return ["intt_pass1", "intt_pass2", "coset_pass1", "coset_pass2"]
+
     def stage_bytes(self):
         """unique bytes each stage launch must read + write (one chunk)."""
         c, n, E = self.chunk, self.n, self.E
+        if self.fused():
+            return [2 * c * n * 32, 0, (2 + 2 * E) * c * n * 32, 2 * E * c * n * 32]
         return [2 * c * n * 32, 2 * c * n * 32, (2 + E) * c * n * 32, 2 * E * c * n * 32]
 
     def stage_mults(self):
+        """algorithmic Fr products per stage launch: (n/2) log2 n per
+        transform split evenly over its two passes, n for the n^-1 scale and n
+        for each coset twist."""
         c, n, E, lg = self.chunk, self.n, self.E, self.log_n
         half = (n // 2) * lg // 2
+        if self.fused():
+            return [c * half, 0, c * (half + n + E * (half + n)), c * E * half]
         return [c * half, c * (half + n), c * E * (half + n), c * E * half]
 
     def launches_per_step(self):
@@ -425,7 +442,7 @@ def run_ours(args):
             "roofline": {
                 "bound": "hbm", "achieved": round(achieved, 2), "peak": peak_hbm, "unit": "GB/s",
                 "frac": round(achieved / peak_hbm, 4), "traffic": traffic,
-                "kernel": ["intt_pass1", "intt_pass2", "coset_pass1", "coset_pass2"][dom],
+                "kernel": ph.stage_names()[dom],
                 "peak_kind": peak_kind,
                 "note": "integer-pipe bound: see roofline_int",
             },

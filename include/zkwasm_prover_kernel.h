@@ -205,12 +205,18 @@ cudaError_t zkp_ntt_batch(void *buf, void *tmp, const void *omegas, const void *
 /* out[i] = base * w^i for i < n (base and w device scalars). */
 cudaError_t zkp_powers(void *out, const void *base, const void *w, uint32_t n, cudaStream_t stream);
 
-/* Coset-extension twist tables: twist[j * n + k] = (shift * w_N^j)^k for
- * j < 2^ext_bits, k < n = 2^log_n, where w_N is a primitive
- * 2^(log_n + ext_bits)-th root of unity (device scalars shift and w_ext).
- * Scratch: 2^ext_bits elements. */
+/* Elements of the coset table zkp_extend_batch needs for (log_n, ext_bits). */
+size_t zkp_coset_table_elems(int log_n, int ext_bits);
+
+/* Coset-extension tables for the evaluation on shift * <w_N>, w_N a primitive
+ * 2^(log_n + ext_bits)-th root of unity (device scalars shift and w_ext), tw the
+ * natural w_n table.  With t_j = shift * w_N^j and R = 2^r the second radix of
+ * the two-pass plan of 2^log_n: when 2^9 <= R <= 2^11 the table holds
+ * W_j[q R + y] = w_n^(q y) t_j^q (2^ext_bits * n entries) followed by
+ * S_j[i] = (t_j^(n/R))^i (2^ext_bits * R entries); otherwise it holds the
+ * twists t_j^k (2^ext_bits * n entries). */
 cudaError_t zkp_coset_twist_tables(void *twist, const void *shift, const void *w_ext, int log_n, int ext_bits,
-                                   void *scratch, cudaStream_t stream);
+                                   const void *tw, cudaStream_t stream);
 
 /* Extended-domain phase for ncols columns of 2^log_n Lagrange values:
  *   coeff = iNTT(lagrange)            (tw_inv = natural table of w_n^-1, n_inv)

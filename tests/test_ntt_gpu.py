@@ -93,7 +93,8 @@ def test_ntt_batch_columns(O, gpu, log_n, ncols):
         assert (got[c * n:(c + 1) * n] == O.ntt(a[c * n:(c + 1) * n], log_n)).all()
 
 
-@pytest.mark.parametrize("log_n,ext_bits,ncols", [(4, 3, 2), (10, 3, 3), (13, 3, 2), (16, 2, 2)])
+@pytest.mark.parametrize("log_n,ext_bits,ncols", [(4, 3, 2), (10, 3, 3), (13, 3, 2), (16, 2, 2),
+                                                  (18, 3, 2), (19, 2, 1), (20, 3, 1)])
 def test_extend_batch_matches_coset_ntt(O, gpu, log_n, ext_bits, ncols):
     H = gpu.host
     n = 1 << log_n
@@ -102,7 +103,7 @@ def test_extend_batch_matches_coset_ntt(O, gpu, log_n, ext_bits, ncols):
     tw_inv = H.generate_omega_buffers(_omega_mont(O, log_n, True), log_n)
     tw = H.generate_omega_buffers(_omega_mont(O, log_n), log_n)
     n_inv = H.to_device(O.fr(pow(n, -1, O.R_MOD)))
-    twist = H.twist_tables(O.fr(shift), O.fr(O.omega(log_n + ext_bits)), log_n, ext_bits)
+    twist = H.twist_tables(O.fr(shift), O.fr(O.omega(log_n + ext_bits)), log_n, ext_bits, tw)
     E = 1 << ext_bits
     ext = H.empty_fr(ncols * E * n)
     coeff = H.empty_fr(ncols * n)

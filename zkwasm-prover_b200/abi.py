@@ -54,6 +54,7 @@ SIGNATURES = {
     "zkp_msm": [P, P, P, U, I, P, SZ, S],
     "zkp_ntt_batch": [P, P, P, P, I, U, SZ, P, S],
     "zkp_powers": [P, P, P, U, S],
+    "zkp_coset_table_elems": ([I, I], SZ),
     "zkp_coset_twist_tables": [P, P, P, I, I, P, S],
     "zkp_extend_batch": [P, P, P, U, I, I, P, P, P, P, P, P, S],
     "zkp_batch_inverse": [P, P, P, U, I, S],

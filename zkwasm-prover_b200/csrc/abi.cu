@@ -348,14 +348,35 @@ cudaError_t zkp_powers(void* out, const void* base, const void* w, uint32_t n, c
     return zk::geometric(F(out), CF(base), CF(w), n, stream);
 }
 
+// the fused stage applies when the transform takes two passes whose second
+// radix is 2^9..2^11 (two tiles of that radix fit in shared memory)
+static bool extend_fused(int log_n, int* rad) {
+    const int np = ntt_plan(log_n, rad);
+    return np == 2 && rad[1] >= 9 && rad[1] <= 11;
+}
+
+size_t zkp_coset_table_elems(int log_n, int ext_bits) {
+    if (log_n < 1 || log_n > 28 || ext_bits < 0 || ext_bits > 6) return 0;
+    int rad[4];
+    const size_t n = (size_t)1 << log_n, E = (size_t)1 << ext_bits;
+    return extend_fused(log_n, rad) ? E * n + E * ((size_t)1 << rad[1]) : E * n;
+}
+
 cudaError_t zkp_coset_twist_tables(void* twist, const void* shift, const void* w_ext, int log_n, int ext_bits,
-                                   void* scratch, cudaStream_t stream) {
-    (void)scratch;
-    if (log_n < 1 || log_n > 28 || ext_bits < 0 || ext_bits > 6) return cudaErrorInvalidValue;
-    const uint32_t n = 1u << log_n, chunk = 16;
-    const uint32_t threads = (n + chunk - 1) / chunk;
+                                   const void* tw, cudaStream_t stream) {
+    if (log_n < 1 || log_n > 28 || ext_bits < 0 || ext_bits > 6 || !twist || !shift || !w_ext)
+        return cudaErrorInvalidValue;
+    int rad[4];
+    const size_t n = (size_t)1 << log_n;
+    if (extend_fused(log_n, rad)) {
+        if (!tw) return cudaErrorInvalidValue;
+        return zk::ntt_fused_tables(F(twist), F(twist) + (n << ext_bits), CF(tw), CF(shift), CF(w_ext), log_n, rad[1],
+                                    ext_bits, stream);
+    }
+    const uint32_t chunk = 16;
+    const uint32_t threads = (uint32_t)((n + chunk - 1) / chunk);
     dim3 grid((threads + 127) / 128, 1u << ext_bits);
-    zk::twist_kernel<<<grid, 128, 0, stream>>>(F(twist), CF(shift), CF(w_ext), n, chunk);
+    zk::twist_kernel<<<grid, 128, 0, stream>>>(F(twist), CF(shift), CF(w_ext), (uint32_t)n, chunk);
     return cudaGetLastError();
 }
 
@@ -374,6 +395,51 @@ cudaError_t zkp_extend_batch(void* ext_out, void* coeff_out, const void* lagrang
     int rad[4];
     const int np = ntt_plan(log_n, rad);
     if (np > 2) return cudaErrorInvalidValue;
+    if (coeff_out && extend_fused(log_n, rad)) {
+        // 1. first inverse pass: lagrange -> coeff_out (intermediate, transformed in place next)
+        NttPassArgs a = {};
+        a.src = CF(lagrange_in);
+        a.dst = F(coeff_out);
+        a.tw = CF(tw_inv);
+        a.log_n = log_n;
+        a.src_ys = n;
+        a.dst_ys = n;
+        ZK_CHECK(ntt_pass(a, rad[0], ncols, 1, stream));
+        ZK_MARK(1);
+        ZK_MARK(2);
+        // 2. fused: last inverse pass + first pass of each coset's forward transform
+        FusedExtendArgs f = {};
+        f.src = F(coeff_out);
+        f.coeff = F(coeff_out);
+        f.sub = F(scratch);
+        f.tw_inv = CF(tw_inv);
+        f.n_inv = CF(n_inv);
+        f.tw = CF(tw);
+        f.wtab = CF(twist);
+        f.stab = CF(twist) + ((size_t)E * n);
+        f.log_n = log_n;
+        f.E = (int)E;
+        f.src_ys = n;
+        f.coeff_ys = n;
+        f.sub_ys = n * E;
+        ZK_CHECK(ntt_fused_extend(f, rad[1], ncols, stream));
+        ZK_MARK(3);
+        // 3. last pass of each coset's forward transform, interleaved output
+        NttPassArgs b = {};
+        b.tw = CF(tw);
+        b.log_n = log_n;
+        b.log_p = rad[1];
+        b.src = F(scratch);
+        b.dst = F(ext_out);
+        b.src_ys = n * E;
+        b.src_zs = n;
+        b.dst_ys = n * E;
+        b.out_shift = ext_bits;
+        b.out_off_z = 1;
+        ZK_CHECK(ntt_pass(b, rad[0], ncols, E, stream));
+        ZK_MARK(4);
+        return cudaGetLastError();
+    }
     Fr* scr = F(scratch);
     Fr* coeff = coeff_out ? F(coeff_out) : scr + (size_t)ncols * (E - 1) * n;
     // 1. inverse transform: lagrange -> (scratch) -> coefficients, scaled by n^-1

@@ -16,6 +16,20 @@
 
 namespace zk {
 
+// Fq product used by the point formulas.  On the device it is one
+// out-of-line function: a mixed addition alone is ten products of ~350
+// instructions each, and inlining every product of the accumulation loop
+// overflows the instruction cache.
+#if defined(__CUDA_ARCH__)
+#if defined(ZK_CURVE_INLINE_MUL)
+__device__ __forceinline__ Fq cmul(const Fq& a, const Fq& b) { return fe_mul<FqCfg>(a, b); }
+#else
+__device__ __noinline__ Fq cmul(const Fq a, const Fq b) { return fe_mul<FqCfg>(a, b); }
+#endif
+#else
+inline Fq cmul(const Fq& a, const Fq& b) { return fe_mul<FqCfg>(a, b); }
+#endif
+
 struct Aff {
     Fq x, y;
 };
@@ -53,14 +67,14 @@ ZK_HD Xyzz xyzz_from_aff(const Aff& a) {
 // 2 * (x, y) for affine (x, y), as XYZZ (mdbl-2008-s-1)
 ZK_HD Xyzz aff_dbl(const Fq& x, const Fq& y) {
     Fq u = fe_dbl<FqCfg>(y);
-    Fq v = fe_sqr<FqCfg>(u);
-    Fq w = fe_mul<FqCfg>(u, v);
-    Fq s = fe_mul<FqCfg>(x, v);
-    Fq xx = fe_sqr<FqCfg>(x);
+    Fq v = cmul(u, u);
+    Fq w = cmul(u, v);
+    Fq s = cmul(x, v);
+    Fq xx = cmul(x, x);
     Fq mm = fe_add<FqCfg>(fe_dbl<FqCfg>(xx), xx);
     Xyzz r;
-    r.x = fe_sub<FqCfg>(fe_sub<FqCfg>(fe_sqr<FqCfg>(mm), s), s);
-    r.y = fe_sub<FqCfg>(fe_mul<FqCfg>(mm, fe_sub<FqCfg>(s, r.x)), fe_mul<FqCfg>(w, y));
+    r.x = fe_sub<FqCfg>(fe_sub<FqCfg>(cmul(mm, mm), s), s);
+    r.y = fe_sub<FqCfg>(cmul(mm, fe_sub<FqCfg>(s, r.x)), cmul(w, y));
     r.zz = v;
     r.zzz = w;
     return r;
@@ -70,16 +84,16 @@ ZK_HD Xyzz aff_dbl(const Fq& x, const Fq& y) {
 ZK_HD Xyzz xyzz_dbl(const Xyzz& p) {
     if (xyzz_is_id(p)) return p;
     Fq u = fe_dbl<FqCfg>(p.y);
-    Fq v = fe_sqr<FqCfg>(u);
-    Fq w = fe_mul<FqCfg>(u, v);
-    Fq s = fe_mul<FqCfg>(p.x, v);
-    Fq xx = fe_sqr<FqCfg>(p.x);
+    Fq v = cmul(u, u);
+    Fq w = cmul(u, v);
+    Fq s = cmul(p.x, v);
+    Fq xx = cmul(p.x, p.x);
     Fq mm = fe_add<FqCfg>(fe_dbl<FqCfg>(xx), xx);
     Xyzz r;
-    r.x = fe_sub<FqCfg>(fe_sub<FqCfg>(fe_sqr<FqCfg>(mm), s), s);
-    r.y = fe_sub<FqCfg>(fe_mul<FqCfg>(mm, fe_sub<FqCfg>(s, r.x)), fe_mul<FqCfg>(w, p.y));
-    r.zz = fe_mul<FqCfg>(v, p.zz);
-    r.zzz = fe_mul<FqCfg>(w, p.zzz);
+    r.x = fe_sub<FqCfg>(fe_sub<FqCfg>(cmul(mm, mm), s), s);
+    r.y = fe_sub<FqCfg>(cmul(mm, fe_sub<FqCfg>(s, r.x)), cmul(w, p.y));
+    r.zz = cmul(v, p.zz);
+    r.zzz = cmul(w, p.zzz);
     return r;
 }
 
@@ -93,22 +107,22 @@ ZK_HD Xyzz xyzz_add_aff(const Xyzz& p, const Fq& x2, const Fq& y2) {
         r.zzz = fe_one<FqCfg>();
         return r;
     }
-    Fq u2 = fe_mul<FqCfg>(x2, p.zz);
-    Fq s2 = fe_mul<FqCfg>(y2, p.zzz);
+    Fq u2 = cmul(x2, p.zz);
+    Fq s2 = cmul(y2, p.zzz);
     Fq pp_ = fe_sub<FqCfg>(u2, p.x);
     Fq rr = fe_sub<FqCfg>(s2, p.y);
     if (fe_is_zero<FqCfg>(pp_)) {
         if (fe_is_zero<FqCfg>(rr)) return aff_dbl(x2, y2);
         return xyzz_identity();
     }
-    Fq pp = fe_sqr<FqCfg>(pp_);
-    Fq ppp = fe_mul<FqCfg>(pp_, pp);
-    Fq q = fe_mul<FqCfg>(p.x, pp);
+    Fq pp = cmul(pp_, pp_);
+    Fq ppp = cmul(pp_, pp);
+    Fq q = cmul(p.x, pp);
     Xyzz r;
-    r.x = fe_sub<FqCfg>(fe_sub<FqCfg>(fe_sub<FqCfg>(fe_sqr<FqCfg>(rr), ppp), q), q);
-    r.y = fe_sub<FqCfg>(fe_mul<FqCfg>(rr, fe_sub<FqCfg>(q, r.x)), fe_mul<FqCfg>(p.y, ppp));
-    r.zz = fe_mul<FqCfg>(p.zz, pp);
-    r.zzz = fe_mul<FqCfg>(p.zzz, ppp);
+    r.x = fe_sub<FqCfg>(fe_sub<FqCfg>(fe_sub<FqCfg>(cmul(rr, rr), ppp), q), q);
+    r.y = fe_sub<FqCfg>(cmul(rr, fe_sub<FqCfg>(q, r.x)), cmul(p.y, ppp));
+    r.zz = cmul(p.zz, pp);
+    r.zzz = cmul(p.zzz, ppp);
     return r;
 }
 
@@ -116,24 +130,24 @@ ZK_HD Xyzz xyzz_add_aff(const Xyzz& p, const Fq& x2, const Fq& y2) {
 ZK_HD Xyzz xyzz_add(const Xyzz& p, const Xyzz& q) {
     if (xyzz_is_id(p)) return q;
     if (xyzz_is_id(q)) return p;
-    Fq u1 = fe_mul<FqCfg>(p.x, q.zz);
-    Fq u2 = fe_mul<FqCfg>(q.x, p.zz);
-    Fq s1 = fe_mul<FqCfg>(p.y, q.zzz);
-    Fq s2 = fe_mul<FqCfg>(q.y, p.zzz);
+    Fq u1 = cmul(p.x, q.zz);
+    Fq u2 = cmul(q.x, p.zz);
+    Fq s1 = cmul(p.y, q.zzz);
+    Fq s2 = cmul(q.y, p.zzz);
     Fq pp_ = fe_sub<FqCfg>(u2, u1);
     Fq rr = fe_sub<FqCfg>(s2, s1);
     if (fe_is_zero<FqCfg>(pp_)) {
         if (fe_is_zero<FqCfg>(rr)) return xyzz_dbl(p);
         return xyzz_identity();
     }
-    Fq pp = fe_sqr<FqCfg>(pp_);
-    Fq ppp = fe_mul<FqCfg>(pp_, pp);
-    Fq qq = fe_mul<FqCfg>(u1, pp);
+    Fq pp = cmul(pp_, pp_);
+    Fq ppp = cmul(pp_, pp);
+    Fq qq = cmul(u1, pp);
     Xyzz r;
-    r.x = fe_sub<FqCfg>(fe_sub<FqCfg>(fe_sub<FqCfg>(fe_sqr<FqCfg>(rr), ppp), qq), qq);
-    r.y = fe_sub<FqCfg>(fe_mul<FqCfg>(rr, fe_sub<FqCfg>(qq, r.x)), fe_mul<FqCfg>(s1, ppp));
-    r.zz = fe_mul<FqCfg>(fe_mul<FqCfg>(p.zz, q.zz), pp);
-    r.zzz = fe_mul<FqCfg>(fe_mul<FqCfg>(p.zzz, q.zzz), ppp);
+    r.x = fe_sub<FqCfg>(fe_sub<FqCfg>(fe_sub<FqCfg>(cmul(rr, rr), ppp), qq), qq);
+    r.y = fe_sub<FqCfg>(cmul(rr, fe_sub<FqCfg>(qq, r.x)), cmul(s1, ppp));
+    r.zz = cmul(cmul(p.zz, q.zz), pp);
+    r.zzz = cmul(cmul(p.zzz, q.zzz), ppp);
     return r;
 }
 
@@ -162,10 +176,10 @@ ZK_HD Jac xyzz_to_jac(const Xyzz& p) {
         r.z = fe_zero<FqCfg>();
         return r;
     }
-    Fq zz2 = fe_sqr<FqCfg>(p.zz);
-    Fq zz3 = fe_mul<FqCfg>(zz2, p.zz);
-    r.x = fe_mul<FqCfg>(p.x, zz2);
-    r.y = fe_mul<FqCfg>(p.y, zz3);
+    Fq zz2 = cmul(p.zz, p.zz);
+    Fq zz3 = cmul(zz2, p.zz);
+    r.x = cmul(p.x, zz2);
+    r.y = cmul(p.y, zz3);
     r.z = p.zzz;
     return r;
 }

@@ -25,6 +25,23 @@ struct NttPassArgs {
 };
 
 cudaError_t ntt_pass(const NttPassArgs& a, int log_r, unsigned ny, unsigned nz, cudaStream_t s);
+
+// fused last inverse pass + first pass of every coset's forward transform
+struct FusedExtendArgs {
+    const Fr* src;     // inverse-transform intermediate (may alias coeff)
+    Fr* coeff;         // coefficients, natural order
+    Fr* sub;           // per-coset first-pass outputs, E * n per column
+    const Fr* tw_inv;  // w^-i, n entries
+    const Fr* n_inv;
+    const Fr* tw;      // w^i, n entries
+    const Fr* wtab;    // E * n
+    const Fr* stab;    // E * 2^log_r
+    int log_n, E;
+    size_t src_ys, coeff_ys, sub_ys;
+};
+cudaError_t ntt_fused_extend(const FusedExtendArgs& a, int log_r, unsigned ncols, cudaStream_t s);
+cudaError_t ntt_fused_tables(Fr* wtab, Fr* stab, const Fr* tw, const Fr* shift, const Fr* w_ext, int log_n, int log_r,
+                             int ext_bits, cudaStream_t s);
 int ntt_plan(int log_n, int radices[4]);
 // Full transform of ncols columns (stride col_stride elements) by the twiddle
 // table tw; result in buf or tmp (*result_in_tmp), multiplied by *scale if given.

@@ -27,6 +27,15 @@
 
 namespace zk {
 
+// Every Fr product of the pass kernels goes through one out-of-line function:
+// inlined, the ~30 product sites of a pass (each ~350 instructions) overflow
+// the instruction cache and warps stall on instruction fetch.
+#if defined(ZK_NTT_INLINE_MUL)
+__device__ __forceinline__ Fr nt_mul(const Fr& a, const Fr& b) { return fe_mul<FrCfg>(a, b); }
+#else
+__device__ __noinline__ Fr nt_mul(const Fr a, const Fr b) { return fe_mul<FrCfg>(a, b); }
+#endif
+
 // ---------------------------------------------------------------- small DFTs
 // Decimation in frequency, natural input; outputs land bit-reversed and are
 // relabelled by the caller.
@@ -41,7 +50,7 @@ __device__ __forceinline__ void dft2(Fr& a, Fr& b) {
 __device__ __forceinline__ void dft4_dif(Fr& v0, Fr& v1, Fr& v2, Fr& v3, const Fr& w4) {
     dft2(v0, v2);
     dft2(v1, v3);
-    v3 = fe_mul<FrCfg>(v3, w4);
+    v3 = nt_mul(v3, w4);
     dft2(v0, v1);
     dft2(v2, v3);
 }
@@ -52,9 +61,9 @@ __device__ __forceinline__ void dft8_dif(Fr v[8], const Fr& w8, const Fr& w4, co
     dft2(v[1], v[5]);
     dft2(v[2], v[6]);
     dft2(v[3], v[7]);
-    v[5] = fe_mul<FrCfg>(v[5], w8);
-    v[6] = fe_mul<FrCfg>(v[6], w4);
-    v[7] = fe_mul<FrCfg>(v[7], w83);
+    v[5] = nt_mul(v[5], w8);
+    v[6] = nt_mul(v[6], w4);
+    v[7] = nt_mul(v[7], w83);
     dft4_dif(v[0], v[1], v[2], v[3], w4);
     dft4_dif(v[4], v[5], v[6], v[7], w4);
 }
@@ -88,11 +97,13 @@ struct PassOut {
     int log_p;       // global P
     uint32_t qhi;    // Q = q >> log_p for this thread's DFT
     const Fr* scale;
+    const Fr* wrow;  // when set: output y is multiplied by wrow[y] instead
 };
 
 __device__ __forceinline__ Fr finish_out(const PassOut& o, Fr v, uint32_t y) {
-    if (o.qhi != 0 && y != 0) v = fe_mul<FrCfg>(v, ldg_elem<FrCfg>(o.tw + ((size_t)(o.qhi * y) << o.log_p)));
-    if (o.scale) v = fe_mul<FrCfg>(v, ldg_elem<FrCfg>(o.scale));
+    if (o.wrow) return nt_mul(v, ldg_elem<FrCfg>(o.wrow + y));
+    if (o.qhi != 0 && y != 0) v = nt_mul(v, ldg_elem<FrCfg>(o.tw + ((size_t)(o.qhi * y) << o.log_p)));
+    if (o.scale) v = nt_mul(v, ldg_elem<FrCfg>(o.scale));
     return v;
 }
 
@@ -110,7 +121,7 @@ __device__ __forceinline__ void stage8(Fr* x, int u, int log_ps, bool last, cons
     if (in_mul) {
 #pragma unroll
         for (int i = 0; i < 8; i++)
-            v[i] = fe_mul<FrCfg>(v[i], ldg_elem<FrCfg>(in_mul + in_base + ((size_t)(u + S * i) << log_items)));
+            v[i] = nt_mul(v[i], ldg_elem<FrCfg>(in_mul + in_base + ((size_t)(u + S * i) << log_items)));
     }
     const int sh = log_n - LOGR;  // w_R^e = tw[e << sh]
     {
@@ -127,7 +138,7 @@ __device__ __forceinline__ void stage8(Fr* x, int u, int log_ps, bool last, cons
     for (int j = 0; j < 8; j++) {
         Fr y = v[rev[j]];
         if (j != 0 && ilo != 0)
-            y = fe_mul<FrCfg>(y, ldg_elem<FrCfg>(tw + ((size_t)((ilo * j) << log_ps) << sh)));
+            y = nt_mul(y, ldg_elem<FrCfg>(tw + ((size_t)((ilo * j) << log_ps) << sh)));
         const int pos = J + (j << log_ps) + (ilo << (log_ps + 3));
         if (last) y = finish_out(po, y, (uint32_t)pos);
         sm_st(x, pos, y);
@@ -158,7 +169,7 @@ __device__ __forceinline__ void stage4_last(Fr* x, int lt, const Fr* tw, int log
         if (in_mul) {
 #pragma unroll
             for (int i = 0; i < 4; i++)
-                v[4 * k + i] = fe_mul<FrCfg>(
+                v[4 * k + i] = nt_mul(
                     v[4 * k + i], ldg_elem<FrCfg>(in_mul + in_base + ((size_t)(u + S * i) << log_items)));
         }
         dft4_dif(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3], w4);
@@ -227,6 +238,7 @@ ntt_pass_kernel(NttPassArgs a) {
     po.log_p = a.log_p;
     po.qhi = q >> a.log_p;
     po.scale = a.scale;
+    po.wrow = nullptr;
     const Fr* in_mul = a.in_mul ? a.in_mul + blockIdx.z * a.in_mul_zs : nullptr;
     const size_t in_base = q;  // natural input position = q + (i << log_items)
 
@@ -262,6 +274,142 @@ ntt_pass_kernel(NttPassArgs a) {
     }
 }
 
+// in-CTA DFT of size 2^LOGR on tile x (natural order in and out)
+template <int LOGR>
+__device__ __forceinline__ void dft_tile(Fr* x, int lt, const Fr* tw, int log_n, const PassOut& po) {
+    constexpr int NS8 = LOGR / 3;
+    constexpr int REM = LOGR % 3;
+    int log_ps = 0;
+#pragma unroll 1
+    for (int s = 0; s < NS8; s++) {
+        stage8<LOGR>(x, lt, log_ps, (s == NS8 - 1) && (REM == 0), tw, log_n, nullptr, 0, 0, po);
+        log_ps += 3;
+    }
+    if (REM == 2) stage4_last<LOGR>(x, lt, tw, log_n, po, nullptr, 0, 0);
+    if (REM == 1) stage2_last<LOGR>(x, lt, po);
+}
+
+// Fused extended-domain stage.  For one column and work item q it runs
+//   (1) the last pass of the inverse transform: radix R = 2^LOGR, P = n/R,
+//       input tmp[q + (n/R) i], output the coefficients c[q + (n/R) j] * n^-1,
+//       written to coeff;
+//   (2) for each coset z, the first pass of that coset's forward transform in
+//       the reversed radix order (radix R first, P = 1), whose item q reads
+//       exactly the same coefficients c[q + (n/R) i], twisted by
+//       t_z^(q + (n/R) i) = t_z^q * S_z[i]: the tile is multiplied by S_z,
+//       transformed, and output y is multiplied by W_z[q R + y] = w^(q y) t_z^q
+//       (inter-pass twiddle and the item's twist constant), then written to
+//       sub[z n + y + R q].
+// The coefficients stay in shared memory across the 2^e cosets, so they are
+// read once instead of 2^e times with a strided pattern.
+template <int LOGR>
+__global__ void __launch_bounds__((1 << LOGR) / 8, ((1 << LOGR) / 8) >= 512 ? 1 : 3)
+ntt_fused_extend_kernel(FusedExtendArgs a) {
+    constexpr int R = 1 << LOGR;
+    constexpr int T = R / 8;
+    extern __shared__ uint4 smem_u4[];
+    Fr* A = reinterpret_cast<Fr*>(smem_u4);
+    Fr* B = A + R;
+    const int tid = threadIdx.x;
+    const int log_items = a.log_n - LOGR;
+    const uint32_t q = blockIdx.x;
+    const size_t n = (size_t)1 << a.log_n;
+    const Fr* src = a.src + blockIdx.y * a.src_ys;
+    Fr* coeff = a.coeff + blockIdx.y * a.coeff_ys;
+    Fr* sub = a.sub + blockIdx.y * a.sub_ys;
+
+    for (int c = tid; c < R * 2; c += T) {
+        const int h = c & 1, i = c >> 1;
+        *sm_slot(A, i, h) = reinterpret_cast<const uint4*>(src + q + ((size_t)i << log_items))[h];
+    }
+    __syncthreads();
+    PassOut po;
+    po.tw = a.tw_inv;
+    po.log_p = log_items;
+    po.qhi = 0;
+    po.scale = a.n_inv;
+    po.wrow = nullptr;
+    dft_tile<LOGR>(A, tid, a.tw_inv, a.log_n, po);
+    for (int c = tid; c < R * 2; c += T) {
+        const int h = c & 1, j = c >> 1;
+        reinterpret_cast<uint4*>(coeff + q + ((size_t)j << log_items))[h] = *sm_slot(A, j, h);
+    }
+    for (int z = 0; z < a.E; z++) {
+        const Fr* S = a.stab + (size_t)z * R;
+        for (int i = tid; i < R; i += T) sm_st(B, i, nt_mul(sm_ld(A, i), ldg_elem<FrCfg>(S + i)));
+        __syncthreads();
+        PassOut pf;
+        pf.tw = a.tw;
+        pf.log_p = 0;
+        pf.qhi = 0;
+        pf.scale = nullptr;
+        pf.wrow = a.wtab + (size_t)z * n + (size_t)q * R;
+        dft_tile<LOGR>(B, tid, a.tw, a.log_n, pf);
+        Fr* out = sub + (size_t)z * n + (size_t)q * R;
+        for (int c = tid; c < R * 2; c += T) {
+            const int h = c & 1, y = c >> 1;
+            reinterpret_cast<uint4*>(out + y)[h] = *sm_slot(B, y, h);
+        }
+        __syncthreads();
+    }
+}
+
+template <int LOGR>
+static cudaError_t launch_fused(const FusedExtendArgs& a, unsigned ncols, cudaStream_t s) {
+    constexpr int R = 1 << LOGR;
+    const size_t smem = (size_t)2 * R * sizeof(Fr);
+    static bool attr_set = false;
+    if (!attr_set) {
+        ZK_CHECK(cudaFuncSetAttribute(ntt_fused_extend_kernel<LOGR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem));
+        attr_set = true;
+    }
+    dim3 grid(1u << (a.log_n - LOGR), ncols, 1);
+    ntt_fused_extend_kernel<LOGR><<<grid, R / 8, smem, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t ntt_fused_extend(const FusedExtendArgs& a, int log_r, unsigned ncols, cudaStream_t s) {
+    switch (log_r) {
+        case 9: return launch_fused<9>(a, ncols, s);
+        case 10: return launch_fused<10>(a, ncols, s);
+        case 11: return launch_fused<11>(a, ncols, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+// Tables of the fused stage for radix R = 2^log_r: wtab[z n + q R + y] =
+// w^(q y) t_z^q (q < n/R, y < R) and stab[z R + i] = (t_z^(n/R))^i, with
+// t_z = shift * w_ext^z and w^k read from the natural table tw.
+__global__ void fused_tables_kernel(Fr* wtab, Fr* stab, const Fr* tw, const Fr* shift, const Fr* w_ext, int log_n,
+                                    int log_r) {
+    const uint32_t z = blockIdx.y;
+    const uint32_t R = 1u << log_r;
+    const uint32_t items = 1u << (log_n - log_r);
+    const size_t n = (size_t)1 << log_n;
+    const Fr tz = nt_mul(ld_elem<FrCfg>(shift), fe_pow_u32<FrCfg>(ld_elem<FrCfg>(w_ext), z));
+    for (uint32_t q = blockIdx.x; q < items; q += gridDim.x) {
+        const Fr tq = fe_pow_u32<FrCfg>(tz, q);
+        for (uint32_t y = threadIdx.x; y < R; y += blockDim.x) {
+            const Fr w = ld_elem<FrCfg>(tw + (size_t)q * y);
+            st_elem<FrCfg>(wtab + (size_t)z * n + (size_t)q * R + y, y == 0 ? tq : nt_mul(w, tq));
+        }
+    }
+    if (blockIdx.x == 0) {
+        const Fr s = fe_pow_u32<FrCfg>(tz, items);
+        for (uint32_t i = threadIdx.x; i < R; i += blockDim.x)
+            st_elem<FrCfg>(stab + (size_t)z * R + i, fe_pow_u32<FrCfg>(s, i));
+    }
+}
+
+cudaError_t ntt_fused_tables(Fr* wtab, Fr* stab, const Fr* tw, const Fr* shift, const Fr* w_ext, int log_n, int log_r,
+                             int ext_bits, cudaStream_t s) {
+    const uint32_t items = 1u << (log_n - log_r);
+    dim3 grid(items < 4096 ? items : 4096, 1u << ext_bits);
+    fused_tables_kernel<<<grid, 256, 0, s>>>(wtab, stab, tw, shift, w_ext, log_n, log_r);
+    return cudaGetLastError();
+}
+
 // tiny transforms (n <= 4): direct O(n^2) evaluation by one thread per column
 __global__ void ntt_tiny_kernel(NttPassArgs a) {
     const int n = 1 << a.log_n;
@@ -271,17 +419,17 @@ __global__ void ntt_tiny_kernel(NttPassArgs a) {
     Fr x[4], y[4];
     for (int i = 0; i < n; i++) {
         x[i] = ld_elem<FrCfg>(src + i);
-        if (a.in_mul) x[i] = fe_mul<FrCfg>(x[i], ld_elem<FrCfg>(a.in_mul + i));
+        if (a.in_mul) x[i] = nt_mul(x[i], ld_elem<FrCfg>(a.in_mul + i));
     }
     for (int j = 0; j < n; j++) {
         Fr acc = fe_zero<FrCfg>();
         for (int i = 0; i < n; i++) {
             Fr t = x[i];
             int e = (i * j) & (n - 1);
-            if (e) t = fe_mul<FrCfg>(t, ld_elem<FrCfg>(a.tw + e));
+            if (e) t = nt_mul(t, ld_elem<FrCfg>(a.tw + e));
             acc = fe_add<FrCfg>(acc, t);
         }
-        if (a.scale) acc = fe_mul<FrCfg>(acc, ld_elem<FrCfg>(a.scale));
+        if (a.scale) acc = nt_mul(acc, ld_elem<FrCfg>(a.scale));
         y[j] = acc;
     }
     for (int j = 0; j < n; j++) st_elem<FrCfg>(dst + ((size_t)j << a.out_shift), y[j]);
@@ -384,7 +532,7 @@ __global__ void expand_powers_kernel(Fr* buf, uint32_t n, uint32_t chunk) {
     Fr cur = fe_pow_u32<FrCfg>(w, s);
     for (uint32_t i = s; i < e; i++) {
         st_elem<FrCfg>(buf + i, cur);
-        cur = fe_mul<FrCfg>(cur, w);
+        cur = nt_mul(cur, w);
     }
 }
 
@@ -403,10 +551,10 @@ __global__ void geometric_kernel(Fr* out, const Fr* base, const Fr* w, uint32_t 
     if (e > n) e = n;
     if (s >= e) return;
     Fr ww = ld_elem<FrCfg>(w);
-    Fr cur = fe_mul<FrCfg>(ld_elem<FrCfg>(base), fe_pow_u32<FrCfg>(ww, s));
+    Fr cur = nt_mul(ld_elem<FrCfg>(base), fe_pow_u32<FrCfg>(ww, s));
     for (uint32_t i = s; i < e; i++) {
         st_elem<FrCfg>(out + i, cur);
-        cur = fe_mul<FrCfg>(cur, ww);
+        cur = nt_mul(cur, ww);
     }
 }
 

@@ -176,12 +176,13 @@ def msm(points_buf, scalars_buf, n: int | None = None, window_bits: int = 0, scr
 # ---------------------------------------------------------------- batched phases
 
 
-def twist_tables(shift, w_ext, log_n: int, ext_bits: int, stream=None) -> torch.Tensor:
-    t = empty_fr((1 << ext_bits) << log_n)
+def twist_tables(shift, w_ext, log_n: int, ext_bits: int, tw, stream=None) -> torch.Tensor:
+    """Coset tables for zkp_extend_batch (tw: natural w_n table)."""
+    t = empty_fr(lib().zkp_coset_table_elems(log_n, ext_bits))
     sh = to_device(np.asarray(shift, np.uint64).reshape(1, 4))
     we = to_device(np.asarray(w_ext, np.uint64).reshape(1, 4))
-    abi.check(lib().zkp_coset_twist_tables(ptr(t), ptr(sh), ptr(we), log_n, ext_bits, None, stream_handle(stream)),
-              "zkp_coset_twist_tables")
+    abi.check(lib().zkp_coset_twist_tables(ptr(t), ptr(sh), ptr(we), log_n, ext_bits, ptr(tw),
+                                           stream_handle(stream)), "zkp_coset_twist_tables")
     torch.cuda.synchronize()
     return t
 
