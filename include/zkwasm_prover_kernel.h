@@ -196,6 +196,21 @@ int zkp_msm_default_window(uint32_t n);
 cudaError_t zkp_msm(void *out, const void *bases, const void *scalars, uint32_t n, int window_bits, void *scratch,
                     size_t scratch_bytes, cudaStream_t stream);
 
+/* Scratch bytes of zkp_msm_batch for `count` MSMs of n[i] points with window
+ * widths window_bits[i] (host arrays; window_bits NULL or 0 entries pick the
+ * default width for each size). */
+size_t zkp_msm_batch_scratch_bytes(const uint32_t *n, const int *window_bits, uint32_t count);
+
+/* A batch of MSMs over one base array in one pipeline (replaces the per-column
+ * msm loop and batch_msm_collect of src/cuda/msm.rs:256-455):
+ * out[i] (96-byte Jacobian, contiguous) = sum_{j < n[i]} [scalars[i][j]] bases[j],
+ * scalars a device array of `count` device pointers, n and window_bits host
+ * arrays.  The descriptor table is uploaded with one cudaMemcpyAsync from
+ * host memory; no allocation and no host synchronisation. */
+cudaError_t zkp_msm_batch(void *out, const void *bases, const void *scalars, const uint32_t *n,
+                          const int *window_bits, uint32_t count, void *scratch, size_t scratch_bytes,
+                          cudaStream_t stream);
+
 /* Batched NTT of ncols columns (column c at buf + c * col_stride elements)
  * by the natural twiddle table `omegas` (2^log_n entries), optional output
  * scale.  *result_in_tmp (host) tells whether the result is in tmp. */
@@ -241,6 +256,10 @@ cudaError_t zkp_batch_inverse(void *out, const void *in, const void *c, uint32_t
  * with known discrete logarithms for benchmarks and SRS-style test data. */
 cudaError_t zkp_g1_multiples(void *out, const void *k64, uint32_t n, cudaStream_t stream);
 
+/* out[i] = in[i] * R mod r: canonical Fr values (below r) to Montgomery form;
+ * out may alias in. */
+cudaError_t zkp_fr_to_mont(void *out, const void *in, uint32_t n, cudaStream_t stream);
+
 /* Scratch elements (32 bytes each) the prefix scans need for n elements. */
 size_t zkp_scan_scratch_elems(uint32_t n);
 
@@ -277,6 +296,43 @@ cudaError_t zkp_shuffle_z(void *z, const void *inputs, const void *tables, const
  * up the array's address (cudaGetSymbolAddress) and should come before any
  * stream capture.  Calls cudaMalloc, cudaFree or no allocating routine. */
 cudaError_t zkp_msm_static(void *out, const void *bases, const void *scalars, uint32_t n, cudaStream_t stream);
+
+/* ----------------------------------------------------------------------
+ * MSM schedule selection (no counterpart in the reference, whose window width
+ * is the fixed formula of src/cuda/msm.rs:105).  The schedule only picks the
+ * window width; results never depend on it.
+ * -------------------------------------------------------------------- */
+
+/* Bit-length histogram of n Montgomery-form scalars, accumulated into
+ * hist[0..6] (device u32): zero, 1-16, 17-32, 33-64, 65-128, 129-192, 193-254. */
+cudaError_t zkp_scalar_histogram(const void *scalars, uint32_t n, uint32_t *hist, cudaStream_t stream);
+
+/* Exhaustive search: times zkp_msm for each window c in [c_min, c_max] whose
+ * scratch fits, reps runs after one warm-up, times_ms[c - c_min] = mean ms or
+ * -1 when skipped; returns the fastest c (-1 on error).  out: 96-byte result.
+ * Synchronises the stream. */
+int zkp_msm_autotune(const void *bases, const void *scalars, uint32_t n, int c_min, int c_max, int reps,
+                     void *scratch, size_t scratch_bytes, float *times_ms, void *out, cudaStream_t stream);
+
+/* MLP cost model (FP32, inputs -> 64 -> 64 -> 1, ReLU) predicting log(ms) of
+ * one MSM from [log2 n / 24, log2 batch / 8, 7 histogram fractions,
+ * (c - 12) / 8].  Parameters, gradients and Adam moments are device float
+ * arrays of zkp_mlp_param_count() entries; X is B x zkp_mlp_input_dim(). */
+int zkp_mlp_input_dim(void);
+size_t zkp_mlp_param_count(void);
+size_t zkp_mlp_scratch_floats(uint32_t B);
+cudaError_t zkp_mlp_init(float *params, uint64_t seed, cudaStream_t stream);
+cudaError_t zkp_mlp_forward(const float *params, const float *X, uint32_t B, float *y, cudaStream_t stream);
+/* mean squared error over the batch and its gradient (loss: device float) */
+cudaError_t zkp_mlp_grad(const float *params, const float *X, const float *t, uint32_t B, float *grads, float *loss,
+                         float *scratch, cudaStream_t stream);
+/* one Adam step, step >= 1 */
+cudaError_t zkp_mlp_train_step(float *params, float *grads, float *m, float *v, const float *X, const float *t,
+                               uint32_t B, float lr, int step, float *loss, float *scratch, cudaStream_t stream);
+/* window with the smallest predicted time for the nine shape features
+ * (host array); scratch: 256 device floats; synchronises the stream */
+int zkp_msm_schedule_predict(const float *params, const float *features, int c_min, int c_max, float *scratch,
+                             cudaStream_t stream);
 
 /* ======================================================================
  * Part 3: calibration

@@ -103,6 +103,33 @@ def test_g1_multiples_generator(O, gpu):
     assert (_jac_to_aff(O, _run(gpu, got, s)) == O.msm_known_dlog(dl, s)).all()
 
 
+def test_msm_batch_uneven(O, gpu):
+    # uneven sizes over one base array, mixed scalar distributions, mixed
+    # window widths, an empty MSM and a single-point MSM
+    H = gpu.host
+    nmax = 1 << 13
+    d = O.rand_fr(nmax, 91)
+    bases = H.to_device(O.g1_gen_bases(d))
+    rng = np.random.default_rng(92)
+    ns = [nmax, 1000, 1, 0, 4096, 300, 2048, 5000]
+    ws = [0, 9, 4, 0, 13, 6, 0, 11]
+    cols = []
+    for i, n in enumerate(ns):
+        s = O.rand_fr(max(n, 1), 100 + i)[:n]
+        if i == 4:  # small, witness-like scalars
+            s = O.fr_vec([int(x) for x in rng.integers(0, 1 << 20, n)])
+        if i == 6:  # sparse
+            s[rng.random(n) < 0.9] = 0
+        cols.append(s)
+    dev_cols = [H.to_device(c) if c.shape[0] else H.empty_fr(1) for c in cols]
+    out = H.msm_batch(bases, dev_cols, ns, ws)
+    torch.cuda.synchronize()
+    got = H.to_host(out)
+    for i, (n, s) in enumerate(zip(ns, cols)):
+        exp = O.msm_known_dlog(d[:n], s) if n else np.zeros((1, 8), np.uint64)
+        assert (_jac_to_aff(O, got[i]) == exp).all(), i
+
+
 def test_reference_abi_batch_msm(O, gpu):
     # msm() per column + batch_msm_collect, buffers sized like src/cuda/msm.rs
     H = gpu.host

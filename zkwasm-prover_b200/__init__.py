@@ -29,6 +29,7 @@ def build(jobs: int = 8) -> str:
 
 from . import abi  # noqa: E402
 from . import host  # noqa: E402
+from . import schedule  # noqa: E402
 from .abi import load_library  # noqa: E402
 
-__all__ = ["build", "load_library", "abi", "host", "LIB_PATH"]
+__all__ = ["build", "load_library", "abi", "host", "schedule", "LIB_PATH"]

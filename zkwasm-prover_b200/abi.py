@@ -52,6 +52,8 @@ SIGNATURES = {
     "zkp_msm_scratch_bytes": ([U, I], SZ),
     "zkp_msm_default_window": ([U], I),
     "zkp_msm": [P, P, P, U, I, P, SZ, S],
+    "zkp_msm_batch_scratch_bytes": ([P, P, U], SZ),
+    "zkp_msm_batch": [P, P, P, P, P, U, P, SZ, S],
     "zkp_ntt_batch": [P, P, P, P, I, U, SZ, P, S],
     "zkp_powers": [P, P, P, U, S],
     "zkp_coset_table_elems": ([I, I], SZ),
@@ -60,11 +62,22 @@ SIGNATURES = {
     "zkp_batch_inverse": [P, P, P, U, I, S],
     "zkp_scan_scratch_elems": ([U], SZ),
     "zkp_g1_multiples": [P, P, U, S],
+    "zkp_fr_to_mont": [P, P, U, S],
     "zkp_grand_product": [P, P, U, P, P, S],
     "zkp_grand_sum": [P, P, U, P, P, S],
     "zkp_permutation_z": [P, P, P, I, P, P, P, P, P, U, P, S],
     "zkp_shuffle_z": [P, P, P, P, I, U, P, S],
     "zkp_msm_static": [P, P, P, U, S],
+    "zkp_scalar_histogram": [P, U, P, S],
+    "zkp_msm_autotune": ([P, P, U, I, I, I, P, SZ, P, P, S], I),
+    "zkp_mlp_input_dim": ([], I),
+    "zkp_mlp_param_count": ([], SZ),
+    "zkp_mlp_scratch_floats": ([U], SZ),
+    "zkp_mlp_init": [P, ctypes.c_uint64, S],
+    "zkp_mlp_forward": [P, P, U, P, S],
+    "zkp_mlp_grad": [P, P, P, U, P, P, P, S],
+    "zkp_mlp_train_step": [P, P, P, P, P, P, U, ctypes.c_float, I, P, P, S],
+    "zkp_msm_schedule_predict": ([P, P, I, I, P, S], I),
     "zkp_calib_mont_rate": [P, U, U, S],
 }
 

@@ -30,6 +30,11 @@ __global__ void twist_kernel(Fr* twist, const Fr* shift, const Fr* w_ext, uint32
     }
 }
 
+__global__ void to_mont_kernel(Fr* out, const Fr* in, uint32_t n) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) st_elem<FrCfg>(out + i, fe_to_mont<FrCfg>(ld_elem<FrCfg>(in + i)));
+}
+
 // out[i] = [k_i] G (affine, Montgomery form) for 64-bit k_i; G = (1, 2)
 __global__ void g1_multiples_kernel(Aff* out, const uint64_t* k64, uint32_t n) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -331,6 +336,21 @@ cudaError_t zkp_msm(void* out, const void* bases, const void* scalars, uint32_t 
     return msm_run(reinterpret_cast<Jac*>(out), reinterpret_cast<const Aff*>(bases), CF(scalars), pl, sc, stream);
 }
 
+size_t zkp_msm_batch_scratch_bytes(const uint32_t* n, const int* window_bits, uint32_t count) {
+    if (!n) return 0;
+    return msm_batch_scratch_bytes(n, window_bits, count);
+}
+
+cudaError_t zkp_msm_batch(void* out, const void* bases, const void* scalars, const uint32_t* n,
+                          const int* window_bits, uint32_t count, void* scratch, size_t scratch_bytes,
+                          cudaStream_t stream) {
+    if (count == 0) return cudaSuccess;
+    if (!out || !bases || !scalars || !n || !scratch) return cudaErrorInvalidValue;
+    return msm_batch_run(reinterpret_cast<Jac*>(out), reinterpret_cast<const Aff*>(bases),
+                         reinterpret_cast<const Fr* const*>(scalars), n, window_bits, count, scratch, scratch_bytes,
+                         stream);
+}
+
 cudaError_t zkp_ntt_batch(void* buf, void* tmp, const void* omegas, const void* scale, int log_n, uint32_t ncols,
                           size_t col_stride, int* result_in_tmp, cudaStream_t stream) {
     if (log_n < 1 || log_n > 28 || !buf || !omegas || !result_in_tmp || ncols == 0 || ncols > 65535)
@@ -528,6 +548,13 @@ cudaError_t zkp_batch_inverse(void* out, const void* in, const void* c, uint32_t
 }
 
 size_t zkp_scan_scratch_elems(uint32_t n) { return fr_scan_tmp_elems(n); }
+
+cudaError_t zkp_fr_to_mont(void* out, const void* in, uint32_t n, cudaStream_t stream) {
+    if (n && (!out || !in)) return cudaErrorInvalidValue;
+    if (n == 0) return cudaSuccess;
+    zk::to_mont_kernel<<<(n + 255) / 256, 256, 0, stream>>>(F(out), CF(in), n);
+    return cudaGetLastError();
+}
 
 cudaError_t zkp_g1_multiples(void* out, const void* k64, uint32_t n, cudaStream_t stream) {
     if (n && (!out || !k64)) return cudaErrorInvalidValue;

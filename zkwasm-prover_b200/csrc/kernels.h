@@ -86,6 +86,14 @@ void msm_layout_split(const MsmPlan& p, uint32_t* words, Xyzz* points, MsmScratc
 cudaError_t msm_run(Jac* out, const Aff* bases, const Fr* scalars, const MsmPlan& p, const MsmScratch& s,
                     cudaStream_t st);
 
+cudaError_t msm_accumulate_merge(const uint32_t* entries, const uint32_t* offset, uint32_t NB, const Aff* bases,
+                                 uint32_t L, uint32_t nacc, Xyzz* buckets, uint32_t* part_key, Xyzz* part_pt,
+                                 cudaStream_t st);
+
+size_t msm_batch_scratch_bytes(const uint32_t* n, const int* c, uint32_t count);
+cudaError_t msm_batch_run(Jac* out, const Aff* bases, const Fr* const* scalars, const uint32_t* n, const int* c,
+                          uint32_t count, void* scratch, size_t scratch_bytes, cudaStream_t st);
+
 // ------------------------------------------------------------------ scans
 size_t scan_tmp_words(uint32_t n);
 // exclusive prefix sum of n u32 values; out[n] = total

@@ -284,6 +284,17 @@ void msm_layout(const MsmPlan& p, void* base, MsmScratch* s) {
     msm_layout_split(p, words, pts, s);
 }
 
+// stages 4 and 5 over any sorted key space (shared by the batched MSM)
+cudaError_t msm_accumulate_merge(const uint32_t* entries, const uint32_t* offset, uint32_t NB, const Aff* bases,
+                                 uint32_t L, uint32_t nacc, Xyzz* buckets, uint32_t* part_key, Xyzz* part_pt,
+                                 cudaStream_t st) {
+    msm_accumulate_kernel<<<(nacc + 127) / 128, 128, 0, st>>>(entries, offset, NB, bases, L, nacc, buckets, part_key,
+                                                              part_pt);
+    ZK_CHECK(cudaGetLastError());
+    msm_merge_kernel<<<(nacc + 127) / 128, 128, 0, st>>>(part_key, part_pt, nacc, buckets);
+    return cudaGetLastError();
+}
+
 cudaError_t msm_run(Jac* out, const Aff* bases, const Fr* scalars, const MsmPlan& p, const MsmScratch& s,
                     cudaStream_t st) {
     if (p.n == 0) {

@@ -1,0 +1,274 @@
+// A batch of MSMs of different sizes over one base array (an SRS prefix per
+// MSM) in one pipeline: one key space for every bucket of every MSM, one
+// counting sort, one accumulation pass, and the per-MSM window reductions and
+// final combinations running side by side.  Each MSM keeps its own window
+// width, so a schedule (autotuned or predicted) can pick it per size and scalar
+// distribution.
+//
+// Reference behaviour replaced: the per-column msm() loop of
+// src/cuda/msm.rs:319-350 followed by batch_msm_collect
+// (cuda/msm.cu:434-467), which sorts and reduces one MSM at a time and combines
+// windows on one thread per MSM.
+#include <vector>
+
+#include "common.cuh"
+#include "kernels.h"
+
+namespace zk {
+
+struct BatchDesc {
+    uint32_t n, c, W, B;
+    uint32_t key_off;  // first bucket key of this MSM
+    uint32_t sc_off;   // first global scalar index of this MSM
+    uint32_t G, seg;   // reduction segments per window and buckets per segment
+    uint32_t red_off;  // first reduction thread
+    uint32_t win_off;  // first window slot
+};
+
+// largest i in [0, count) with d[i].*field <= x
+template <uint32_t BatchDesc::*F>
+__device__ __forceinline__ uint32_t find_desc(const BatchDesc* d, uint32_t count, uint32_t x) {
+    uint32_t lo = 0, hi = count;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (d[mid].*F <= x)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+__global__ void batch_count_kernel(const BatchDesc* d, uint32_t count, const Fr* const* scalars, uint32_t total,
+                                   uint32_t* cnt) {
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < total; s += gridDim.x * blockDim.x) {
+        const uint32_t i = find_desc<&BatchDesc::sc_off>(d, count, s);
+        const BatchDesc q = d[i];
+        Fr k = fe_from_mont<FrCfg>(ldg_elem<FrCfg>(scalars[i] + (s - q.sc_off)));
+        uint32_t carry = 0;
+        for (uint32_t w = 0; w < q.W; w++) {
+            const int dg = msm_signed_digit(k.v, (int)w, (int)q.c, carry);
+            if (dg != 0) {
+                const uint32_t mag = dg > 0 ? (uint32_t)dg : (uint32_t)(-dg);
+                atomicAdd(&cnt[q.key_off + w * q.B + mag - 1], 1u);
+            }
+        }
+    }
+}
+
+__global__ void batch_scatter_kernel(const BatchDesc* d, uint32_t count, const Fr* const* scalars, uint32_t total,
+                                     const uint32_t* offset, uint32_t* cnt, uint32_t* entries) {
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < total; s += gridDim.x * blockDim.x) {
+        const uint32_t i = find_desc<&BatchDesc::sc_off>(d, count, s);
+        const BatchDesc q = d[i];
+        const uint32_t j = s - q.sc_off;
+        Fr k = fe_from_mont<FrCfg>(ldg_elem<FrCfg>(scalars[i] + j));
+        uint32_t carry = 0;
+        for (uint32_t w = 0; w < q.W; w++) {
+            const int dg = msm_signed_digit(k.v, (int)w, (int)q.c, carry);
+            if (dg != 0) {
+                const uint32_t mag = dg > 0 ? (uint32_t)dg : (uint32_t)(-dg);
+                const uint32_t key = q.key_off + w * q.B + mag - 1;
+                const uint32_t slot = atomicSub(&cnt[key], 1u) - 1u;
+                entries[offset[key] + slot] = j | (dg < 0 ? 0x80000000u : 0u);
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ Xyzz bld_xyzz(const Xyzz* p) {
+    Xyzz r;
+    r.x = ld_elem<FqCfg>(&p->x);
+    r.y = ld_elem<FqCfg>(&p->y);
+    r.zz = ld_elem<FqCfg>(&p->zz);
+    r.zzz = ld_elem<FqCfg>(&p->zzz);
+    return r;
+}
+
+__device__ __forceinline__ void bst_xyzz(Xyzz* p, const Xyzz& v) {
+    st_elem<FqCfg>(&p->x, v.x);
+    st_elem<FqCfg>(&p->y, v.y);
+    st_elem<FqCfg>(&p->zz, v.zz);
+    st_elem<FqCfg>(&p->zzz, v.zzz);
+}
+
+__global__ void __launch_bounds__(128) batch_reduce_kernel(const BatchDesc* d, uint32_t count, uint32_t total,
+                                                           const Xyzz* buckets, const uint32_t* offset,
+                                                           Xyzz* segsum) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= total) return;
+    const uint32_t i = find_desc<&BatchDesc::red_off>(d, count, t);
+    const BatchDesc q = d[i];
+    const uint32_t lt = t - q.red_off;
+    const uint32_t w = lt / q.G, g = lt % q.G;
+    const uint32_t lo = g * q.seg;
+    Xyzz T = xyzz_identity(), S = xyzz_identity();
+    for (uint32_t j = 0; j < q.seg; j++) {
+        const uint32_t key = q.key_off + w * q.B + lo + q.seg - 1 - j;
+        if (offset[key + 1] != offset[key]) T = xyzz_add(T, bld_xyzz(buckets + key));
+        S = xyzz_add(S, T);
+    }
+    if (lo) S = xyzz_add(S, xyzz_mul_u32(T, lo));
+    bst_xyzz(segsum + t, S);
+}
+
+// one CTA per (MSM, window); blockDim >= every G
+__global__ void batch_window_kernel(const BatchDesc* d, uint32_t count, const Xyzz* segsum, Xyzz* winsum) {
+    extern __shared__ uint4 smem_u4[];
+    Xyzz* sm = reinterpret_cast<Xyzz*>(smem_u4);
+    const uint32_t b = blockIdx.x, k = threadIdx.x;
+    const uint32_t i = find_desc<&BatchDesc::win_off>(d, count, b);
+    const BatchDesc q = d[i];
+    const uint32_t w = b - q.win_off;
+    sm[k] = k < q.G ? bld_xyzz(segsum + q.red_off + w * q.G + k) : xyzz_identity();
+    __syncthreads();
+    for (uint32_t h = blockDim.x >> 1; h > 0; h >>= 1) {
+        if (k < h) sm[k] = xyzz_add(sm[k], sm[k + h]);
+        __syncthreads();
+    }
+    if (k == 0) bst_xyzz(winsum + b, sm[0]);
+}
+
+__global__ void batch_final_kernel(const BatchDesc* d, uint32_t count, const Xyzz* winsum, Jac* out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const BatchDesc q = d[i];
+    Xyzz acc = xyzz_identity();
+    if (q.n) {
+        acc = bld_xyzz(winsum + q.win_off + q.W - 1);
+        for (int w = (int)q.W - 2; w >= 0; w--) {
+            for (uint32_t r = 0; r < q.c; r++) acc = xyzz_dbl(acc);
+            acc = xyzz_add(acc, bld_xyzz(winsum + q.win_off + w));
+        }
+    }
+    const Jac j = xyzz_to_jac(acc);
+    st_elem<FqCfg>(&out[i].x, j.x);
+    st_elem<FqCfg>(&out[i].y, j.y);
+    st_elem<FqCfg>(&out[i].z, j.z);
+}
+
+// ------------------------------------------------------------------ planning
+
+struct BatchLayout {
+    std::vector<BatchDesc> desc;
+    uint32_t NB = 0, total = 0, red_total = 0, win_total = 0, L = 8, nacc = 1, maxG = 1;
+    uint64_t entries = 0;
+    size_t off_desc = 0, off_cnt = 0, off_offset = 0, off_scan = 0, off_entries = 0, off_pkey = 0, off_ppt = 0,
+           off_buckets = 0, off_segsum = 0, off_winsum = 0, bytes = 0;
+};
+
+static size_t al(size_t x) { return (x + 255) / 256 * 256; }
+
+static bool batch_plan(const uint32_t* n, const int* c, uint32_t count, BatchLayout& L) {
+    L.desc.resize(count);
+    uint64_t key = 0, sc = 0, red = 0, win = 0, ent = 0;
+    for (uint32_t i = 0; i < count; i++) {
+        const MsmPlan p = msm_make_plan(n[i], c ? c[i] : 0);
+        BatchDesc& q = L.desc[i];
+        q.n = n[i];
+        q.c = (uint32_t)p.c;
+        q.W = (uint32_t)p.W;
+        q.B = p.B;
+        q.key_off = (uint32_t)key;
+        q.sc_off = (uint32_t)sc;
+        q.G = p.G;
+        q.seg = p.seg;
+        q.red_off = (uint32_t)red;
+        q.win_off = (uint32_t)win;
+        key += (uint64_t)p.W * p.B;
+        sc += n[i];
+        red += (uint64_t)p.W * p.G;
+        win += p.W;
+        ent += (uint64_t)n[i] * p.W;
+        if (p.G > L.maxG) L.maxG = p.G;
+    }
+    if (key >= 0xffffffffull || sc >= 0x7fffffffull || ent >= 0xffffffffull || red >= 0xffffffffull) return false;
+    L.NB = (uint32_t)key;
+    L.total = (uint32_t)sc;
+    L.red_total = (uint32_t)red;
+    L.win_total = (uint32_t)win;
+    L.entries = ent;
+    const uint64_t target = 148ull * 4 * 128;
+    uint64_t Lp = (ent + target - 1) / target;
+    if (Lp < 8) Lp = 8;
+    L.L = (uint32_t)Lp;
+    L.nacc = (uint32_t)((ent + Lp - 1) / Lp);
+    if (L.nacc == 0) L.nacc = 1;
+    size_t o = 0;
+    L.off_desc = o;
+    o = al(o + count * sizeof(BatchDesc));
+    L.off_cnt = o;
+    o = al(o + (size_t)L.NB * 4);
+    L.off_offset = o;
+    o = al(o + ((size_t)L.NB + 1) * 4);
+    L.off_scan = o;
+    o = al(o + scan_tmp_words(L.NB) * 4);
+    L.off_entries = o;
+    o = al(o + ent * 4);
+    L.off_pkey = o;
+    o = al(o + (size_t)2 * L.nacc * 4);
+    L.off_ppt = o;
+    o = al(o + (size_t)2 * L.nacc * sizeof(Xyzz));
+    L.off_buckets = o;
+    o = al(o + (size_t)L.NB * sizeof(Xyzz));
+    L.off_segsum = o;
+    o = al(o + (size_t)L.red_total * sizeof(Xyzz));
+    L.off_winsum = o;
+    o = al(o + (size_t)L.win_total * sizeof(Xyzz));
+    L.bytes = o;
+    return true;
+}
+
+size_t msm_batch_scratch_bytes(const uint32_t* n, const int* c, uint32_t count) {
+    BatchLayout L;
+    if (count == 0 || !batch_plan(n, c, count, L)) return 0;
+    return L.bytes;
+}
+
+cudaError_t msm_batch_run(Jac* out, const Aff* bases, const Fr* const* scalars, const uint32_t* n, const int* c,
+                          uint32_t count, void* scratch, size_t scratch_bytes, cudaStream_t st) {
+    if (count == 0) return cudaSuccess;
+    BatchLayout L;
+    if (!batch_plan(n, c, count, L)) return cudaErrorInvalidValue;
+    if (L.bytes > scratch_bytes || L.NB > 4096u * 4096u) return cudaErrorInvalidValue;
+    char* base = reinterpret_cast<char*>(scratch);
+    BatchDesc* d = reinterpret_cast<BatchDesc*>(base + L.off_desc);
+    uint32_t* cnt = reinterpret_cast<uint32_t*>(base + L.off_cnt);
+    uint32_t* offset = reinterpret_cast<uint32_t*>(base + L.off_offset);
+    uint32_t* scan = reinterpret_cast<uint32_t*>(base + L.off_scan);
+    uint32_t* entries = reinterpret_cast<uint32_t*>(base + L.off_entries);
+    uint32_t* pkey = reinterpret_cast<uint32_t*>(base + L.off_pkey);
+    Xyzz* ppt = reinterpret_cast<Xyzz*>(base + L.off_ppt);
+    Xyzz* buckets = reinterpret_cast<Xyzz*>(base + L.off_buckets);
+    Xyzz* segsum = reinterpret_cast<Xyzz*>(base + L.off_segsum);
+    Xyzz* winsum = reinterpret_cast<Xyzz*>(base + L.off_winsum);
+    // the descriptor table goes up from pageable host memory; the copy is
+    // staged before cudaMemcpyAsync returns, so the vector may go away after
+    ZK_CHECK(cudaMemcpyAsync(d, L.desc.data(), count * sizeof(BatchDesc), cudaMemcpyHostToDevice, st));
+    ZK_CHECK(cudaMemsetAsync(cnt, 0, (size_t)L.NB * 4, st));
+    unsigned g1 = (L.total + 255) / 256;
+    if (g1 > 148u * 64u) g1 = 148u * 64u;
+    if (g1 == 0) g1 = 1;
+    batch_count_kernel<<<g1, 256, 0, st>>>(d, count, scalars, L.total, cnt);
+    ZK_CHECK(cudaGetLastError());
+    ZK_CHECK(scan_u32(cnt, offset, L.NB, scan, st));
+    batch_scatter_kernel<<<g1, 256, 0, st>>>(d, count, scalars, L.total, offset, cnt, entries);
+    ZK_CHECK(cudaGetLastError());
+    ZK_CHECK(msm_accumulate_merge(entries, offset, L.NB, bases, L.L, L.nacc, buckets, pkey, ppt, st));
+    batch_reduce_kernel<<<(L.red_total + 127) / 128, 128, 0, st>>>(d, count, L.red_total, buckets, offset, segsum);
+    ZK_CHECK(cudaGetLastError());
+    uint32_t bd = 1;
+    while (bd < L.maxG) bd <<= 1;
+    static bool attr = false;
+    if (!attr) {
+        ZK_CHECK(cudaFuncSetAttribute(batch_window_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      512 * (int)sizeof(Xyzz)));
+        attr = true;
+    }
+    batch_window_kernel<<<L.win_total, bd, (size_t)bd * sizeof(Xyzz), st>>>(d, count, segsum, winsum);
+    ZK_CHECK(cudaGetLastError());
+    batch_final_kernel<<<(count + 31) / 32, 32, 0, st>>>(d, count, winsum, out);
+    return cudaGetLastError();
+}
+
+}  // namespace zk

@@ -173,6 +173,27 @@ def msm(points_buf, scalars_buf, n: int | None = None, window_bits: int = 0, scr
     return out
 
 
+def msm_batch(bases_buf, scalar_bufs, ns, windows=None, scratch=None, out=None, stream=None):
+    """zkp_msm_batch: one pipeline for len(scalar_bufs) MSMs over the prefix
+    bases_buf[:ns[i]]; returns (count, 12) int64 Jacobian points on the device."""
+    count = len(scalar_bufs)
+    n_arr = (ctypes.c_uint32 * count)(*[int(x) for x in ns])
+    c_arr = None if windows is None else (ctypes.c_int * count)(*[int(x) for x in windows])
+    ptrs = ptr_array(scalar_bufs)
+    if scratch is None:
+        nbytes = lib().zkp_msm_batch_scratch_bytes(ctypes.addressof(n_arr),
+                                                   None if c_arr is None else ctypes.addressof(c_arr), count)
+        scratch = torch.empty(max(1, nbytes), dtype=torch.uint8, device="cuda")
+    if out is None:
+        out = torch.empty((count, 12), dtype=torch.int64, device="cuda")
+    err = lib().zkp_msm_batch(ptr(out), ptr(bases_buf), ptr(ptrs), ctypes.addressof(n_arr),
+                              None if c_arr is None else ctypes.addressof(c_arr), count, ptr(scratch),
+                              scratch.numel(), stream_handle(stream))
+    abi.check(err, "zkp_msm_batch")
+    out._keep = (ptrs, scratch)  # keep device operands alive with the result
+    return out
+
+
 # ---------------------------------------------------------------- batched phases
 
 

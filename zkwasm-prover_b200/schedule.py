@@ -1,0 +1,238 @@
+"""MSM schedule selection: exhaustive autotuner, learned cost model, regret.
+
+The reference picks the MSM window width with a fixed formula
+(src/cuda/msm.rs:105).  Here three pickers exist:
+
+* ``default``  - the library's cost formula (``zkp_msm_default_window``);
+* ``autotune`` - ``zkp_msm_autotune``: time every candidate window on the
+  actual bases and scalars and keep the fastest (the judge of the others);
+* ``learned``  - an MLP cost model (``zkp_mlp_*`` kernels) trained on the
+  autotuner's own measurements, predicting log(ms) from the shape features
+  [log2 n / 24, log2 batch / 8, scalar bit-length histogram (7 bins),
+  (c - 12) / 8]; the window with the smallest prediction wins.
+
+A schedule only chooses the window width, so every picker gives the same
+MSM result; regret (ms) is measured against the autotuner's best.
+"""
+from __future__ import annotations
+
+import ctypes
+import json
+import math
+import os
+
+import numpy as np
+import torch
+
+from . import abi
+from . import host as H
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+MODEL_PATH = os.path.join(HERE, "msm_schedule_model.npz")
+C_MIN, C_MAX = 8, 20
+MIXES = ("uniform", "small", "sparse", "mixed")
+
+
+def lib():
+    return abi.load_library()
+
+
+# ------------------------------------------------------------------ inputs
+
+
+def bases_with_known_logs(n: int, seed: int, device="cuda"):
+    """[k_i] G for seeded 62-bit k_i, generated on the device."""
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    k = torch.randint(0, 2 ** 62, (n,), dtype=torch.int64, device=device, generator=g)
+    out = torch.empty((n, 8), dtype=torch.int64, device=device)
+    abi.check(lib().zkp_g1_multiples(out.data_ptr(), k.data_ptr(), n, H.stream_handle()), "zkp_g1_multiples")
+    return out, k
+
+
+def scalars(n: int, mix: str, seed: int, device="cuda") -> torch.Tensor:
+    """Montgomery-form scalars with the given distribution of canonical values:
+    uniform below 2^253, small (< 2^20, witness-like), sparse (90% zero, the
+    rest uniform), or mixed (50% uniform, 35% small, 15% sparse-uniform)."""
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    t = torch.randint(-(2 ** 63), 2 ** 63 - 1, (n, 4), dtype=torch.int64, device=device, generator=g)
+    t[:, 3] &= (1 << 61) - 1
+    u = torch.rand(n, device=device, generator=g)
+    if mix == "small":
+        t[:, 1:] = 0
+        t[:, 0] &= (1 << 20) - 1
+    elif mix == "sparse":
+        t[u < 0.9] = 0
+    elif mix == "mixed":
+        small = (u >= 0.5) & (u < 0.85)
+        t[small, 1:] = 0
+        t[small, 0] &= (1 << 20) - 1
+        zero = (u >= 0.85) & (torch.rand(n, device=device, generator=g) < 0.9)
+        t[zero] = 0
+    abi.check(lib().zkp_fr_to_mont(t.data_ptr(), t.data_ptr(), n, H.stream_handle()), "zkp_fr_to_mont")
+    return t
+
+
+def histogram(s: torch.Tensor) -> list:
+    h = torch.zeros(8, dtype=torch.int32, device=s.device)
+    abi.check(lib().zkp_scalar_histogram(s.data_ptr(), s.shape[0], h.data_ptr(), H.stream_handle()),
+              "zkp_scalar_histogram")
+    torch.cuda.synchronize()
+    v = h.cpu().numpy()[:7].astype(np.float64)
+    return list(v / max(1.0, v.sum()))
+
+
+def shape_features(n: int, batch: int, hist) -> list:
+    return [math.log2(max(n, 1)) / 24.0, math.log2(max(batch, 1)) / 8.0] + [float(x) for x in hist]
+
+
+def model_input(feats, c: int) -> list:
+    return list(feats) + [(c - 12) / 8.0]
+
+
+# ------------------------------------------------------------------ pickers
+
+
+def default_window(n: int) -> int:
+    return lib().zkp_msm_default_window(n)
+
+
+def reference_window(n: int, batch: int = 1) -> int:
+    """src/cuda/msm.rs:105"""
+    lg = lambda x: max(0, (x - 1).bit_length())
+    return min(lg(batch), 3) + 10 + max(lg(n), 22) - 22
+
+
+def autotune(bases, s, n: int, c_min=C_MIN, c_max=C_MAX, reps=2):
+    """Exhaustive search on the device; returns (best c, {c: ms})."""
+    L = lib()
+    need = max(L.zkp_msm_scratch_bytes(n, c) for c in range(c_min, c_max + 1))
+    scratch = torch.empty(need, dtype=torch.uint8, device="cuda")
+    out = torch.empty(12, dtype=torch.int64, device="cuda")
+    times = (ctypes.c_float * (c_max - c_min + 1))()
+    best = L.zkp_msm_autotune(bases.data_ptr(), s.data_ptr(), n, c_min, c_max, reps, scratch.data_ptr(), need,
+                              ctypes.addressof(times), out.data_ptr(), H.stream_handle())
+    if best < 0:
+        raise abi.CudaError("zkp_msm_autotune failed")
+    return best, {c: float(times[c - c_min]) for c in range(c_min, c_max + 1) if times[c - c_min] >= 0}
+
+
+class Model:
+    """The MLP parameters on the device plus its training / prediction calls."""
+
+    def __init__(self, params: torch.Tensor):
+        self.params = params
+
+    @classmethod
+    def fresh(cls, seed=1):
+        L = lib()
+        p = torch.empty(L.zkp_mlp_param_count(), dtype=torch.float32, device="cuda")
+        abi.check(L.zkp_mlp_init(p.data_ptr(), seed, H.stream_handle()), "zkp_mlp_init")
+        return cls(p)
+
+    @classmethod
+    def load(cls, path=MODEL_PATH):
+        d = np.load(path)
+        return cls(torch.from_numpy(d["params"].astype(np.float32)).cuda())
+
+    def save(self, path=MODEL_PATH, meta=None):
+        np.savez(path, params=self.params.cpu().numpy(), meta=json.dumps(meta or {}))
+
+    def predict(self, X: np.ndarray) -> np.ndarray:
+        x = torch.from_numpy(np.ascontiguousarray(X, np.float32)).cuda()
+        y = torch.empty(x.shape[0], dtype=torch.float32, device="cuda")
+        abi.check(lib().zkp_mlp_forward(self.params.data_ptr(), x.data_ptr(), x.shape[0], y.data_ptr(),
+                                        H.stream_handle()), "zkp_mlp_forward")
+        return y.cpu().numpy()
+
+    def train(self, X: np.ndarray, y: np.ndarray, steps=4000, lr=3e-3):
+        L = lib()
+        x = torch.from_numpy(np.ascontiguousarray(X, np.float32)).cuda()
+        t = torch.from_numpy(np.ascontiguousarray(y, np.float32)).cuda()
+        B = x.shape[0]
+        g = torch.zeros_like(self.params)
+        m = torch.zeros_like(self.params)
+        v = torch.zeros_like(self.params)
+        loss = torch.zeros(1, dtype=torch.float32, device="cuda")
+        scratch = torch.empty(L.zkp_mlp_scratch_floats(B), dtype=torch.float32, device="cuda")
+        st = H.stream_handle()
+        hist = []
+        for step in range(1, steps + 1):
+            abi.check(L.zkp_mlp_train_step(self.params.data_ptr(), g.data_ptr(), m.data_ptr(), v.data_ptr(),
+                                           x.data_ptr(), t.data_ptr(), B, lr, step, loss.data_ptr(),
+                                           scratch.data_ptr(), st), "zkp_mlp_train_step")
+            if step == 1 or step % 500 == 0:
+                hist.append((step, float(loss.item())))
+        return hist
+
+    def pick(self, feats, c_min=C_MIN, c_max=C_MAX) -> int:
+        f = (ctypes.c_float * 9)(*[float(x) for x in feats])
+        scratch = torch.empty(256, dtype=torch.float32, device="cuda")
+        c = lib().zkp_msm_schedule_predict(self.params.data_ptr(), ctypes.addressof(f), c_min, c_max,
+                                           scratch.data_ptr(), H.stream_handle())
+        if c < 0:
+            raise abi.CudaError("zkp_msm_schedule_predict failed")
+        return c
+
+
+# ------------------------------------------------------------------ dataset / evaluation
+
+
+def collect(sizes, mixes=MIXES, reps=2, seed=100, c_min=C_MIN, c_max=C_MAX):
+    """Autotune every (size, mix) shape; one record per shape."""
+    records = []
+    nmax = max(sizes)
+    bases, _ = bases_with_known_logs(nmax, seed)
+    for n in sizes:
+        for mi, mix in enumerate(mixes):
+            s = scalars(n, mix, seed + 17 * n.bit_length() + mi)
+            hist = histogram(s)
+            best, times = autotune(bases, s, n, c_min, c_max, reps)
+            records.append({"n": n, "batch": 1, "mix": mix, "hist": hist, "best": best, "times_ms": times})
+            del s
+    return records
+
+
+def training_set(records):
+    X, y = [], []
+    for r in records:
+        f = shape_features(r["n"], r["batch"], r["hist"])
+        for c, ms in r["times_ms"].items():
+            X.append(model_input(f, int(c)))
+            y.append(math.log(ms))
+    return np.array(X, np.float32), np.array(y, np.float32)
+
+
+def regret(records, picker):
+    """Total and per-shape regret (ms) of a picker against the fastest window."""
+    total, rows = 0.0, []
+    for r in records:
+        times = {int(c): v for c, v in r["times_ms"].items()}
+        best = min(times.values())
+        c = picker(r)
+        if c not in times:  # outside the measured range: charge the nearest measured window
+            c = min(times, key=lambda k: abs(k - c))
+        rows.append({"n": r["n"], "mix": r["mix"], "picked": c, "regret_ms": times[c] - best})
+        total += times[c] - best
+    return total, rows
+
+
+def mlp_forward_numpy(params: np.ndarray, X: np.ndarray) -> np.ndarray:
+    """CPU restatement of mlp_forward_kernel (same parameter layout)."""
+    D, H1, H2 = X.shape[1], 64, 64
+    o = 0
+    W1 = params[o:o + D * H1].reshape(D, H1)
+    o += D * H1
+    b1 = params[o:o + H1]
+    o += H1
+    W2 = params[o:o + H1 * H2].reshape(H1, H2)
+    o += H1 * H2
+    b2 = params[o:o + H2]
+    o += H2
+    W3 = params[o:o + H2]
+    o += H2
+    b3 = params[o]
+    h1 = np.maximum(X @ W1 + b1, 0)
+    h2 = np.maximum(h1 @ W2 + b2, 0)
+    return h2 @ W3 + b3
