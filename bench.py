@@ -284,6 +284,66 @@ def run_msm(zkp, device, sizes=(1 << 18, 1 << 22), reps=5):
     return res
 
 
+def run_msm_batch(zkp, device, count=32, lo=14, hi=20, seed=2024, reps=3):
+    """Batched uneven MSMs over one SRS (sizes 2^U, U uniform in [lo, hi];
+    per MSM the scalars are uniform (50%), small < 2^20 (35%) or 90%-sparse
+    (15%)): plain per-MSM zkp_msm launches against one zkp_msm_batch pipeline,
+    each with the library's default windows and with the learned schedule."""
+    import numpy as np
+
+    S, H = zkp.schedule, zkp.host
+    rng = np.random.default_rng(seed)
+    ns = [1 << int(u) for u in rng.integers(lo, hi + 1, count)]
+    mixes = ["uniform" if x < 0.5 else "small" if x < 0.85 else "sparse" for x in rng.random(count)]
+    bases, _ = S.bases_with_known_logs(max(ns), seed)
+    cols = [S.scalars(n, m, seed + 1 + i) for i, (n, m) in enumerate(zip(ns, mixes))]
+    model = S.Model.load()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    learned = [model.pick(S.shape_features(n, count, S.histogram(c))) for n, c in zip(ns, cols)]
+    pick_ms = (time.perf_counter() - t0) * 1e3
+    default = [S.default_window(n) for n in ns]
+    res = {"count": count, "sizes_log2": [n.bit_length() - 1 for n in ns], "mixes": mixes,
+           "total_points": int(sum(ns)), "learned_windows": learned, "default_windows": default,
+           "schedule_pick_ms": round(pick_ms, 2)}
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(reps):
+            fn()
+        b.record()
+        b.synchronize()
+        return a.elapsed_time(b) / reps
+
+    outs = {}
+    for name, ws in (("default", default), ("learned", learned)):
+        scratch = torch.empty(max(zkp.load_library().zkp_msm_scratch_bytes(n, c) for n, c in zip(ns, ws)),
+                              dtype=torch.uint8, device=device)
+        out = torch.empty((count, 12), dtype=torch.int64, device=device)
+
+        def plain():
+            for i, (n, c) in enumerate(zip(ns, ws)):
+                H.msm(bases, cols[i], n=n, window_bits=c, scratch=scratch, out=out[i])
+
+        res[f"plain_{name}_ms"] = round(timed(plain), 3)
+        del scratch
+        n_arr = (ctypes.c_uint32 * count)(*ns)
+        c_arr = (ctypes.c_int * count)(*ws)
+        bscr = torch.empty(zkp.load_library().zkp_msm_batch_scratch_bytes(ctypes.addressof(n_arr),
+                                                                            ctypes.addressof(c_arr), count),
+                           dtype=torch.uint8, device=device)
+        bout = torch.empty((count, 12), dtype=torch.int64, device=device)
+        res[f"batched_{name}_ms"] = round(timed(lambda: H.msm_batch(bases, cols, ns, ws, scratch=bscr, out=bout)), 3)
+        outs[name] = bout
+        del bscr
+    res["speedup_batched_learned_vs_plain_default"] = round(res["plain_default_ms"] / res["batched_learned_ms"], 3)
+    res["mpts_per_s_batched_learned"] = round(res["total_points"] / res["batched_learned_ms"] / 1e3, 2)
+    return res
+
+
 def run_e2e(ph, steps):
     """Same phase through the C ABI with host buffers: pinned Lagrange columns
     copied in and coefficients copied out every step, overlapped by chunk on
@@ -418,6 +478,7 @@ def run_ours(args):
                 traffic = json.load(f).get("stage_traffic_bytes", [None] * 4)[dom]
         cpu = cpu_baseline_port(args.log_n, args.ext_bits) if not args.no_cpu_baseline else None
         msm = run_msm(zkp, device) if not args.no_msm else None
+        msm_batch = run_msm_batch(zkp, device) if not args.no_msm else None
         out = {
             "metric": f"NTT HBM GB/s: batched iNTT 2^{args.log_n} -> coset NTT 2^{args.log_n + args.ext_bits}, "
                       f"{args.columns} columns",
@@ -457,6 +518,7 @@ def run_ours(args):
             "stage_ms": [round(x, 4) for x in stage_ms],
             "cpu_baseline": cpu,
             "msm": msm,
+            "msm_batch": msm_batch,
         }
         if clk:
             out["clocks"] = clk

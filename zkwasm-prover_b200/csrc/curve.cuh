@@ -64,40 +64,54 @@ ZK_HD Xyzz xyzz_from_aff(const Aff& a) {
     return r;
 }
 
+// Product policies for the point formulas: CurveMul calls cmul (out of line
+// on the device), CurveMulInline expands every product in place, for
+// single-thread latency-bound code where the compiler should overlap the
+// independent products of one formula.
+struct CurveMul {
+    static ZK_HD Fq mul(const Fq& a, const Fq& b) { return cmul(a, b); }
+};
+struct CurveMulInline {
+    static ZK_HD Fq mul(const Fq& a, const Fq& b) { return fe_mul<FqCfg>(a, b); }
+};
+
 // 2 * (x, y) for affine (x, y), as XYZZ (mdbl-2008-s-1)
+template <class M = CurveMul>
 ZK_HD Xyzz aff_dbl(const Fq& x, const Fq& y) {
     Fq u = fe_dbl<FqCfg>(y);
-    Fq v = cmul(u, u);
-    Fq w = cmul(u, v);
-    Fq s = cmul(x, v);
-    Fq xx = cmul(x, x);
+    Fq v = M::mul(u, u);
+    Fq w = M::mul(u, v);
+    Fq s = M::mul(x, v);
+    Fq xx = M::mul(x, x);
     Fq mm = fe_add<FqCfg>(fe_dbl<FqCfg>(xx), xx);
     Xyzz r;
-    r.x = fe_sub<FqCfg>(fe_sub<FqCfg>(cmul(mm, mm), s), s);
-    r.y = fe_sub<FqCfg>(cmul(mm, fe_sub<FqCfg>(s, r.x)), cmul(w, y));
+    r.x = fe_sub<FqCfg>(fe_sub<FqCfg>(M::mul(mm, mm), s), s);
+    r.y = fe_sub<FqCfg>(M::mul(mm, fe_sub<FqCfg>(s, r.x)), M::mul(w, y));
     r.zz = v;
     r.zzz = w;
     return r;
 }
 
 // 2 * p (dbl-2008-s-1)
+template <class M = CurveMul>
 ZK_HD Xyzz xyzz_dbl(const Xyzz& p) {
     if (xyzz_is_id(p)) return p;
     Fq u = fe_dbl<FqCfg>(p.y);
-    Fq v = cmul(u, u);
-    Fq w = cmul(u, v);
-    Fq s = cmul(p.x, v);
-    Fq xx = cmul(p.x, p.x);
+    Fq v = M::mul(u, u);
+    Fq w = M::mul(u, v);
+    Fq s = M::mul(p.x, v);
+    Fq xx = M::mul(p.x, p.x);
     Fq mm = fe_add<FqCfg>(fe_dbl<FqCfg>(xx), xx);
     Xyzz r;
-    r.x = fe_sub<FqCfg>(fe_sub<FqCfg>(cmul(mm, mm), s), s);
-    r.y = fe_sub<FqCfg>(cmul(mm, fe_sub<FqCfg>(s, r.x)), cmul(w, p.y));
-    r.zz = cmul(v, p.zz);
-    r.zzz = cmul(w, p.zzz);
+    r.x = fe_sub<FqCfg>(fe_sub<FqCfg>(M::mul(mm, mm), s), s);
+    r.y = fe_sub<FqCfg>(M::mul(mm, fe_sub<FqCfg>(s, r.x)), M::mul(w, p.y));
+    r.zz = M::mul(v, p.zz);
+    r.zzz = M::mul(w, p.zzz);
     return r;
 }
 
 // p + (x2, y2) with (x2, y2) affine and not the identity (madd-2008-s)
+template <class M = CurveMul>
 ZK_HD Xyzz xyzz_add_aff(const Xyzz& p, const Fq& x2, const Fq& y2) {
     if (xyzz_is_id(p)) {
         Xyzz r;
@@ -107,51 +121,53 @@ ZK_HD Xyzz xyzz_add_aff(const Xyzz& p, const Fq& x2, const Fq& y2) {
         r.zzz = fe_one<FqCfg>();
         return r;
     }
-    Fq u2 = cmul(x2, p.zz);
-    Fq s2 = cmul(y2, p.zzz);
+    Fq u2 = M::mul(x2, p.zz);
+    Fq s2 = M::mul(y2, p.zzz);
     Fq pp_ = fe_sub<FqCfg>(u2, p.x);
     Fq rr = fe_sub<FqCfg>(s2, p.y);
     if (fe_is_zero<FqCfg>(pp_)) {
-        if (fe_is_zero<FqCfg>(rr)) return aff_dbl(x2, y2);
+        if (fe_is_zero<FqCfg>(rr)) return aff_dbl<M>(x2, y2);
         return xyzz_identity();
     }
-    Fq pp = cmul(pp_, pp_);
-    Fq ppp = cmul(pp_, pp);
-    Fq q = cmul(p.x, pp);
+    Fq pp = M::mul(pp_, pp_);
+    Fq ppp = M::mul(pp_, pp);
+    Fq q = M::mul(p.x, pp);
     Xyzz r;
-    r.x = fe_sub<FqCfg>(fe_sub<FqCfg>(fe_sub<FqCfg>(cmul(rr, rr), ppp), q), q);
-    r.y = fe_sub<FqCfg>(cmul(rr, fe_sub<FqCfg>(q, r.x)), cmul(p.y, ppp));
-    r.zz = cmul(p.zz, pp);
-    r.zzz = cmul(p.zzz, ppp);
+    r.x = fe_sub<FqCfg>(fe_sub<FqCfg>(fe_sub<FqCfg>(M::mul(rr, rr), ppp), q), q);
+    r.y = fe_sub<FqCfg>(M::mul(rr, fe_sub<FqCfg>(q, r.x)), M::mul(p.y, ppp));
+    r.zz = M::mul(p.zz, pp);
+    r.zzz = M::mul(p.zzz, ppp);
     return r;
 }
 
 // p + q (add-2008-s)
+template <class M = CurveMul>
 ZK_HD Xyzz xyzz_add(const Xyzz& p, const Xyzz& q) {
     if (xyzz_is_id(p)) return q;
     if (xyzz_is_id(q)) return p;
-    Fq u1 = cmul(p.x, q.zz);
-    Fq u2 = cmul(q.x, p.zz);
-    Fq s1 = cmul(p.y, q.zzz);
-    Fq s2 = cmul(q.y, p.zzz);
+    Fq u1 = M::mul(p.x, q.zz);
+    Fq u2 = M::mul(q.x, p.zz);
+    Fq s1 = M::mul(p.y, q.zzz);
+    Fq s2 = M::mul(q.y, p.zzz);
     Fq pp_ = fe_sub<FqCfg>(u2, u1);
     Fq rr = fe_sub<FqCfg>(s2, s1);
     if (fe_is_zero<FqCfg>(pp_)) {
-        if (fe_is_zero<FqCfg>(rr)) return xyzz_dbl(p);
+        if (fe_is_zero<FqCfg>(rr)) return xyzz_dbl<M>(p);
         return xyzz_identity();
     }
-    Fq pp = cmul(pp_, pp_);
-    Fq ppp = cmul(pp_, pp);
-    Fq qq = cmul(u1, pp);
+    Fq pp = M::mul(pp_, pp_);
+    Fq ppp = M::mul(pp_, pp);
+    Fq qq = M::mul(u1, pp);
     Xyzz r;
-    r.x = fe_sub<FqCfg>(fe_sub<FqCfg>(fe_sub<FqCfg>(cmul(rr, rr), ppp), qq), qq);
-    r.y = fe_sub<FqCfg>(cmul(rr, fe_sub<FqCfg>(qq, r.x)), cmul(s1, ppp));
-    r.zz = cmul(cmul(p.zz, q.zz), pp);
-    r.zzz = cmul(cmul(p.zzz, q.zzz), ppp);
+    r.x = fe_sub<FqCfg>(fe_sub<FqCfg>(fe_sub<FqCfg>(M::mul(rr, rr), ppp), qq), qq);
+    r.y = fe_sub<FqCfg>(M::mul(rr, fe_sub<FqCfg>(qq, r.x)), M::mul(s1, ppp));
+    r.zz = M::mul(M::mul(p.zz, q.zz), pp);
+    r.zzz = M::mul(M::mul(p.zzz, q.zzz), ppp);
     return r;
 }
 
 // [k] p for a small unsigned k (double-and-add from the top bit)
+template <class M = CurveMul>
 ZK_HD Xyzz xyzz_mul_u32(const Xyzz& p, uint32_t k) {
     Xyzz r = xyzz_identity();
     if (k == 0 || xyzz_is_id(p)) return r;
@@ -159,8 +175,8 @@ ZK_HD Xyzz xyzz_mul_u32(const Xyzz& p, uint32_t k) {
     while (!((k >> top) & 1)) top--;
     r = p;
     for (int b = top - 1; b >= 0; b--) {
-        r = xyzz_dbl(r);
-        if ((k >> b) & 1) r = xyzz_add(r, p);
+        r = xyzz_dbl<M>(r);
+        if ((k >> b) & 1) r = xyzz_add<M>(r, p);
     }
     return r;
 }
@@ -168,6 +184,7 @@ ZK_HD Xyzz xyzz_mul_u32(const Xyzz& p, uint32_t k) {
 // XYZZ -> Jacobian without an inversion: with ZZ = z^2, ZZZ = z^3 the point
 // (X * ZZ^2, Y * ZZ^3, ZZZ) has X'/Z'^2 = X/ZZ and Y'/Z'^3 = Y/ZZZ.
 // The identity becomes (0, 1, 0), halo2's Jacobian identity.
+template <class M = CurveMul>
 ZK_HD Jac xyzz_to_jac(const Xyzz& p) {
     Jac r;
     if (xyzz_is_id(p)) {
@@ -176,10 +193,10 @@ ZK_HD Jac xyzz_to_jac(const Xyzz& p) {
         r.z = fe_zero<FqCfg>();
         return r;
     }
-    Fq zz2 = cmul(p.zz, p.zz);
-    Fq zz3 = cmul(zz2, p.zz);
-    r.x = cmul(p.x, zz2);
-    r.y = cmul(p.y, zz3);
+    Fq zz2 = M::mul(p.zz, p.zz);
+    Fq zz3 = M::mul(zz2, p.zz);
+    r.x = M::mul(p.x, zz2);
+    r.y = M::mul(p.y, zz3);
     r.z = p.zzz;
     return r;
 }

@@ -13,40 +13,23 @@
 //   6. reduce   per window, segments of buckets by running sums:
 //               sum_b (b+1) B_b = S_seg + lo * T_seg
 //   7. window   tree sum of the segment results per window
-//   8. final    Horner over windows (c doublings each) -> Jacobian output
+//   8. final    Horner over windows (c doublings each) -> Jacobian output,
+//               four warps evaluating the independent products of each formula
 //
 // Reference behaviour replaced: cuda/msm.cu:9-467 (unsigned digits, CUB radix
 // sort, Jacobian accumulation, one-thread window combine) behind the C entry
 // points msm / batch_msm_collect.
 #include "common.cuh"
 #include "kernels.h"
+#include "msm_common.cuh"
 
 namespace zk {
 
 static constexpr uint32_t KEY_NONE = 0xffffffffu;
 
-__device__ __forceinline__ Aff ld_aff(const Aff* p) {
-    Aff a;
-    a.x = ldg_elem<FqCfg>(&p->x);
-    a.y = ldg_elem<FqCfg>(&p->y);
-    return a;
-}
-
-__device__ __forceinline__ Xyzz ld_xyzz(const Xyzz* p) {
-    Xyzz r;
-    r.x = ld_elem<FqCfg>(&p->x);
-    r.y = ld_elem<FqCfg>(&p->y);
-    r.zz = ld_elem<FqCfg>(&p->zz);
-    r.zzz = ld_elem<FqCfg>(&p->zzz);
-    return r;
-}
-
-__device__ __forceinline__ void st_xyzz(Xyzz* p, const Xyzz& v) {
-    st_elem<FqCfg>(&p->x, v.x);
-    st_elem<FqCfg>(&p->y, v.y);
-    st_elem<FqCfg>(&p->zz, v.zz);
-    st_elem<FqCfg>(&p->zzz, v.zzz);
-}
+#ifndef ZK_MSM_REDUCE_THREADS
+#define ZK_MSM_REDUCE_THREADS 32768
+#endif
 
 __global__ void msm_count_kernel(const Fr* __restrict__ scalars, uint32_t n, int c, int W,
                                  uint32_t* __restrict__ count) {
@@ -83,6 +66,8 @@ __global__ void msm_scatter_kernel(const Fr* __restrict__ scalars, uint32_t n, i
     }
 }
 
+__device__ __forceinline__ void prefetch_l1(const void* p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
+
 // largest k in [lo, hi) with off[k] <= pos
 __device__ __forceinline__ uint32_t find_bucket(const uint32_t* off, uint32_t lo, uint32_t hi, uint32_t pos) {
     while (hi - lo > 1) {
@@ -110,12 +95,20 @@ __global__ void __launch_bounds__(128) msm_accumulate_kernel(const uint32_t* __r
         const uint32_t e = min(s + L, total);
         uint32_t key = find_bucket(offset, 0, NB, s);
         uint32_t pos = s;
+        // the base of the next entry is prefetched into L1 while the current
+        // one is added (a register copy would cost occupancy)
+        uint32_t ent_next = entries[pos];
+        prefetch_l1(bases + (ent_next & 0x7fffffffu));
         while (pos < e) {
             const uint32_t kbeg = offset[key], kend = offset[key + 1];
             const uint32_t rend = min(kend, e);
             Xyzz acc = xyzz_identity();
             for (uint32_t p = pos; p < rend; p++) {
-                const uint32_t ent = entries[p];
+                const uint32_t ent = ent_next;
+                if (p + 1 < e) {
+                    ent_next = entries[p + 1];
+                    prefetch_l1(bases + (ent_next & 0x7fffffffu));
+                }
                 Aff a = ld_aff(bases + (ent & 0x7fffffffu));
                 if (aff_is_id(a)) continue;
                 if (ent >> 31) a.y = fe_neg<FqCfg>(a.y);
@@ -133,7 +126,15 @@ __global__ void __launch_bounds__(128) msm_accumulate_kernel(const uint32_t* __r
                 st_xyzz(part_pt + 2 * t + 1, acc);
             }
             pos = rend;
-            if (pos < e) key = find_bucket(offset, key + 1, NB, pos);
+            if (pos < e) {
+                // the next non-empty bucket is usually within a few keys
+                uint32_t k = key + 1, tries = 0;
+                while (tries < 8 && offset[k + 1] <= pos) {
+                    k++;
+                    tries++;
+                }
+                key = (offset[k + 1] > pos) ? k : find_bucket(offset, k, NB, pos);
+            }
         }
     }
     part_key[2 * t] = head_key;
@@ -173,30 +174,33 @@ __global__ void __launch_bounds__(128) msm_reduce_kernel(const Xyzz* __restrict_
     st_xyzz(segsum + t, S);
 }
 
-__global__ void msm_window_kernel(const Xyzz* __restrict__ segsum, uint32_t G, Xyzz* __restrict__ winsum) {
+// one CTA per window; blockDim (a power of two, <= G) threads first add
+// G / blockDim segment results each, then reduce as a tree
+__global__ void __launch_bounds__(256) msm_window_kernel(const Xyzz* __restrict__ segsum, uint32_t G, Xyzz* __restrict__ winsum) {
     extern __shared__ uint4 smem_u4[];
     Xyzz* sm = reinterpret_cast<Xyzz*>(smem_u4);
-    const uint32_t w = blockIdx.x, i = threadIdx.x;
-    sm[i] = ld_xyzz(segsum + (size_t)w * G + i);
+    const uint32_t w = blockIdx.x, i = threadIdx.x, T = blockDim.x;
+    Xyzz acc = ld_xyzz(segsum + (size_t)w * G + i);
+    for (uint32_t k = i + T; k < G; k += T) acc = xyzz_add(acc, ld_xyzz(segsum + (size_t)w * G + k));
+    sm[i] = acc;
     __syncthreads();
-    for (uint32_t h = G >> 1; h > 0; h >>= 1) {
+    for (uint32_t h = T >> 1; h > 0; h >>= 1) {
         if (i < h) sm[i] = xyzz_add(sm[i], sm[i + h]);
         __syncthreads();
     }
     if (i == 0) st_xyzz(winsum + w, sm[0]);
 }
 
-__global__ void msm_final_kernel(const Xyzz* __restrict__ winsum, int W, int c, Jac* __restrict__ out) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    Xyzz acc = W > 0 ? ld_xyzz(winsum + W - 1) : xyzz_identity();
-    for (int w = W - 2; w >= 0; w--) {
-        for (int i = 0; i < c; i++) acc = xyzz_dbl(acc);
-        acc = xyzz_add(acc, ld_xyzz(winsum + w));
+// one CTA of COOP_THREADS threads
+__global__ void __launch_bounds__(COOP_THREADS) msm_final_kernel(const Xyzz* __restrict__ winsum, int W, int c,
+                                                                  Jac* __restrict__ out) {
+    __shared__ Fq buf[8];
+    const Jac j = coop_horner(buf, winsum, W, c);
+    if (threadIdx.x == 0) {
+        st_elem<FqCfg>(&out->x, j.x);
+        st_elem<FqCfg>(&out->y, j.y);
+        st_elem<FqCfg>(&out->z, j.z);
     }
-    Jac j = xyzz_to_jac(acc);
-    st_elem<FqCfg>(&out->x, j.x);
-    st_elem<FqCfg>(&out->y, j.y);
-    st_elem<FqCfg>(&out->z, j.z);
 }
 
 // ------------------------------------------------------------------ planning
@@ -231,9 +235,11 @@ MsmPlan msm_make_plan(uint32_t n, int c) {
     p.L = (uint32_t)L;
     p.nacc = (uint32_t)((max_entries + L - 1) / L);
     if (p.nacc == 0) p.nacc = 1;
-    // about 16K reduction threads in total, at most 512 segments per window
+    // up to ZK_MSM_REDUCE_THREADS reduction threads in total (the running-sum
+    // segments are latency bound, so they need many threads), at most 4096 per
+    // window
     uint32_t G = 1;
-    while (G < 512 && (uint64_t)G * 2 * p.W <= 16384 && G * 2 <= p.B) G *= 2;
+    while (G < 4096 && (uint64_t)G * 2 * p.W <= ZK_MSM_REDUCE_THREADS && G * 2 <= p.B) G *= 2;
     p.G = G;
     p.seg = p.B / G;
     return p;
@@ -299,7 +305,7 @@ cudaError_t msm_run(Jac* out, const Aff* bases, const Fr* scalars, const MsmPlan
                     cudaStream_t st) {
     if (p.n == 0) {
         // empty sum: the identity
-        msm_final_kernel<<<1, 1, 0, st>>>(nullptr, 0, p.c, out);
+        msm_final_kernel<<<1, COOP_THREADS, 0, st>>>(nullptr, 0, p.c, out);
         return cudaGetLastError();
     }
     const uint32_t tb = 256;
@@ -318,15 +324,15 @@ cudaError_t msm_run(Jac* out, const Aff* bases, const Fr* scalars, const MsmPlan
     const uint32_t nred = (uint32_t)p.W * p.G;
     msm_reduce_kernel<<<(nred + 127) / 128, 128, 0, st>>>(s.buckets, s.offset, p.W, p.B, p.seg, p.G, s.segsum);
     ZK_CHECK(cudaGetLastError());
-    const size_t wsm = (size_t)p.G * sizeof(Xyzz);
+    const size_t wsm = (size_t)(p.G < 256 ? p.G : 256) * sizeof(Xyzz);
     static bool attr = false;
     if (!attr) {
-        ZK_CHECK(cudaFuncSetAttribute(msm_window_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 512 * (int)sizeof(Xyzz)));
+        ZK_CHECK(cudaFuncSetAttribute(msm_window_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 256 * (int)sizeof(Xyzz)));
         attr = true;
     }
-    msm_window_kernel<<<p.W, p.G, wsm, st>>>(s.segsum, p.G, s.winsum);
+    msm_window_kernel<<<p.W, p.G < 256 ? p.G : 256, wsm, st>>>(s.segsum, p.G, s.winsum);
     ZK_CHECK(cudaGetLastError());
-    msm_final_kernel<<<1, 1, 0, st>>>(s.winsum, p.W, p.c, out);
+    msm_final_kernel<<<1, COOP_THREADS, 0, st>>>(s.winsum, p.W, p.c, out);
     return cudaGetLastError();
 }
 

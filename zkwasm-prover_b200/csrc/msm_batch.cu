@@ -13,6 +13,7 @@
 
 #include "common.cuh"
 #include "kernels.h"
+#include "msm_common.cuh"
 
 namespace zk {
 
@@ -76,21 +77,6 @@ __global__ void batch_scatter_kernel(const BatchDesc* d, uint32_t count, const F
     }
 }
 
-__device__ __forceinline__ Xyzz bld_xyzz(const Xyzz* p) {
-    Xyzz r;
-    r.x = ld_elem<FqCfg>(&p->x);
-    r.y = ld_elem<FqCfg>(&p->y);
-    r.zz = ld_elem<FqCfg>(&p->zz);
-    r.zzz = ld_elem<FqCfg>(&p->zzz);
-    return r;
-}
-
-__device__ __forceinline__ void bst_xyzz(Xyzz* p, const Xyzz& v) {
-    st_elem<FqCfg>(&p->x, v.x);
-    st_elem<FqCfg>(&p->y, v.y);
-    st_elem<FqCfg>(&p->zz, v.zz);
-    st_elem<FqCfg>(&p->zzz, v.zzz);
-}
 
 __global__ void __launch_bounds__(128) batch_reduce_kernel(const BatchDesc* d, uint32_t count, uint32_t total,
                                                            const Xyzz* buckets, const uint32_t* offset,
@@ -105,46 +91,45 @@ __global__ void __launch_bounds__(128) batch_reduce_kernel(const BatchDesc* d, u
     Xyzz T = xyzz_identity(), S = xyzz_identity();
     for (uint32_t j = 0; j < q.seg; j++) {
         const uint32_t key = q.key_off + w * q.B + lo + q.seg - 1 - j;
-        if (offset[key + 1] != offset[key]) T = xyzz_add(T, bld_xyzz(buckets + key));
+        if (offset[key + 1] != offset[key]) T = xyzz_add(T, ld_xyzz(buckets + key));
         S = xyzz_add(S, T);
     }
     if (lo) S = xyzz_add(S, xyzz_mul_u32(T, lo));
-    bst_xyzz(segsum + t, S);
+    st_xyzz(segsum + t, S);
 }
 
-// one CTA per (MSM, window); blockDim >= every G
-__global__ void batch_window_kernel(const BatchDesc* d, uint32_t count, const Xyzz* segsum, Xyzz* winsum) {
+// one CTA per (MSM, window); blockDim a power of two: each thread first adds
+// the segment results k, k + blockDim, ... of its window, then a tree
+__global__ void __launch_bounds__(256) batch_window_kernel(const BatchDesc* d, uint32_t count, const Xyzz* segsum, Xyzz* winsum) {
     extern __shared__ uint4 smem_u4[];
     Xyzz* sm = reinterpret_cast<Xyzz*>(smem_u4);
     const uint32_t b = blockIdx.x, k = threadIdx.x;
     const uint32_t i = find_desc<&BatchDesc::win_off>(d, count, b);
     const BatchDesc q = d[i];
     const uint32_t w = b - q.win_off;
-    sm[k] = k < q.G ? bld_xyzz(segsum + q.red_off + w * q.G + k) : xyzz_identity();
+    Xyzz acc = xyzz_identity();
+    for (uint32_t g = k; g < q.G; g += blockDim.x) acc = xyzz_add(acc, ld_xyzz(segsum + q.red_off + w * q.G + g));
+    sm[k] = acc;
     __syncthreads();
     for (uint32_t h = blockDim.x >> 1; h > 0; h >>= 1) {
         if (k < h) sm[k] = xyzz_add(sm[k], sm[k + h]);
         __syncthreads();
     }
-    if (k == 0) bst_xyzz(winsum + b, sm[0]);
+    if (k == 0) st_xyzz(winsum + b, sm[0]);
 }
 
-__global__ void batch_final_kernel(const BatchDesc* d, uint32_t count, const Xyzz* winsum, Jac* out) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= count) return;
+// one CTA of COOP_THREADS threads per MSM
+__global__ void __launch_bounds__(COOP_THREADS) batch_final_kernel(const BatchDesc* d, const Xyzz* winsum,
+                                                                    Jac* out) {
+    __shared__ Fq buf[8];
+    const uint32_t i = blockIdx.x;
     const BatchDesc q = d[i];
-    Xyzz acc = xyzz_identity();
-    if (q.n) {
-        acc = bld_xyzz(winsum + q.win_off + q.W - 1);
-        for (int w = (int)q.W - 2; w >= 0; w--) {
-            for (uint32_t r = 0; r < q.c; r++) acc = xyzz_dbl(acc);
-            acc = xyzz_add(acc, bld_xyzz(winsum + q.win_off + w));
-        }
+    const Jac j = coop_horner(buf, winsum + q.win_off, q.n ? (int)q.W : 0, (int)q.c);
+    if (threadIdx.x == 0) {
+        st_elem<FqCfg>(&out[i].x, j.x);
+        st_elem<FqCfg>(&out[i].y, j.y);
+        st_elem<FqCfg>(&out[i].z, j.z);
     }
-    const Jac j = xyzz_to_jac(acc);
-    st_elem<FqCfg>(&out[i].x, j.x);
-    st_elem<FqCfg>(&out[i].y, j.y);
-    st_elem<FqCfg>(&out[i].z, j.z);
 }
 
 // ------------------------------------------------------------------ planning
@@ -230,7 +215,7 @@ cudaError_t msm_batch_run(Jac* out, const Aff* bases, const Fr* const* scalars, 
     if (count == 0) return cudaSuccess;
     BatchLayout L;
     if (!batch_plan(n, c, count, L)) return cudaErrorInvalidValue;
-    if (L.bytes > scratch_bytes || L.NB > 4096u * 4096u) return cudaErrorInvalidValue;
+    if (L.bytes > scratch_bytes) return cudaErrorInvalidValue;
     char* base = reinterpret_cast<char*>(scratch);
     BatchDesc* d = reinterpret_cast<BatchDesc*>(base + L.off_desc);
     uint32_t* cnt = reinterpret_cast<uint32_t*>(base + L.off_cnt);
@@ -258,7 +243,7 @@ cudaError_t msm_batch_run(Jac* out, const Aff* bases, const Fr* const* scalars, 
     batch_reduce_kernel<<<(L.red_total + 127) / 128, 128, 0, st>>>(d, count, L.red_total, buckets, offset, segsum);
     ZK_CHECK(cudaGetLastError());
     uint32_t bd = 1;
-    while (bd < L.maxG) bd <<= 1;
+    while (bd < L.maxG && bd < 256) bd <<= 1;
     static bool attr = false;
     if (!attr) {
         ZK_CHECK(cudaFuncSetAttribute(batch_window_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -267,7 +252,7 @@ cudaError_t msm_batch_run(Jac* out, const Aff* bases, const Fr* const* scalars, 
     }
     batch_window_kernel<<<L.win_total, bd, (size_t)bd * sizeof(Xyzz), st>>>(d, count, segsum, winsum);
     ZK_CHECK(cudaGetLastError());
-    batch_final_kernel<<<(count + 31) / 32, 32, 0, st>>>(d, count, winsum, out);
+    batch_final_kernel<<<count, COOP_THREADS, 0, st>>>(d, winsum, out);
     return cudaGetLastError();
 }
 

@@ -1,6 +1,6 @@
 // Exclusive prefix sum of u32 counts (bucket offsets for the MSM counting sort).
 // Three launches: per-block scan of 4096 values, scan of the block totals,
-// and the add-back.  Supports n <= 4096 * 4096.
+// and the add-back.
 #include "common.cuh"
 #include "kernels.h"
 
@@ -61,24 +61,29 @@ __global__ void __launch_bounds__(SCAN_T) scan_block_kernel(const uint32_t* in, 
     if (threadIdx.x == 0) bsum[blockIdx.x] = tot;
 }
 
+// one CTA scans the block totals in chunks of SCAN_BLK, carrying the sum
 __global__ void __launch_bounds__(SCAN_T) scan_top_kernel(uint32_t* bsum, uint32_t nb, uint32_t* total_out) {
     __shared__ uint32_t wt[32];
-    const uint32_t base = threadIdx.x * SCAN_V;
-    uint32_t v[SCAN_V];
-    uint32_t s = 0;
+    uint32_t carry = 0;
+    for (uint32_t chunk = 0; chunk < nb; chunk += SCAN_BLK) {
+        const uint32_t base = chunk + threadIdx.x * SCAN_V;
+        uint32_t v[SCAN_V];
+        uint32_t s = 0;
 #pragma unroll
-    for (int i = 0; i < SCAN_V; i++) {
-        v[i] = (base + i < nb) ? bsum[base + i] : 0;
-        s += v[i];
-    }
-    uint32_t tot;
-    uint32_t pre = block_excl_scan(s, wt, tot);
+        for (int i = 0; i < SCAN_V; i++) {
+            v[i] = (base + i < nb) ? bsum[base + i] : 0;
+            s += v[i];
+        }
+        uint32_t tot;
+        uint32_t pre = carry + block_excl_scan(s, wt, tot);
 #pragma unroll
-    for (int i = 0; i < SCAN_V; i++) {
-        if (base + i < nb) bsum[base + i] = pre;
-        pre += v[i];
+        for (int i = 0; i < SCAN_V; i++) {
+            if (base + i < nb) bsum[base + i] = pre;
+            pre += v[i];
+        }
+        carry += tot;
     }
-    if (threadIdx.x == 0) *total_out = tot;
+    if (threadIdx.x == 0) *total_out = carry;
 }
 
 __global__ void __launch_bounds__(SCAN_T) scan_add_kernel(uint32_t* out, uint32_t n, const uint32_t* bsum) {
@@ -92,7 +97,6 @@ __global__ void __launch_bounds__(SCAN_T) scan_add_kernel(uint32_t* out, uint32_
 
 cudaError_t scan_u32(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* tmp, cudaStream_t s) {
     const uint32_t nb = (n + SCAN_BLK - 1) / SCAN_BLK;
-    if (nb > SCAN_BLK) return cudaErrorInvalidValue;
     if (nb == 0) return cudaMemsetAsync(out, 0, sizeof(uint32_t), s);
     scan_block_kernel<<<nb, SCAN_T, 0, s>>>(in, out, n, tmp);
     scan_top_kernel<<<1, SCAN_T, 0, s>>>(tmp, nb, out + n);
