@@ -63,6 +63,33 @@ def test_msm_all_scalars_equal(O, gpu):
     assert (_jac_to_aff(O, _run(gpu, bases, s)) == O.msm_known_dlog(d, s)).all()
 
 
+@pytest.mark.parametrize("c", [9, 12, 14, 18])
+def test_msm_narrow_top_window(O, gpu, c):
+    # 254 = q c + 1 or 2: the top window has 1-2 bits, so a handful of buckets
+    # there hold every point and the merge reduces runs over thousands of slices
+    n = 1 << 16
+    d = O.rand_fr(n, 53)
+    bases = O.g1_gen_bases(d)
+    s = O.rand_fr(n, 54 + c)
+    assert (_jac_to_aff(O, _run(gpu, bases, s, c)) == O.msm_known_dlog(d, s)).all()
+
+
+def test_msm_few_distinct_scalars(O, gpu):
+    # witness-like columns: 90% of the scalars take one of three values
+    n = 1 << 15
+    d = O.rand_fr(n, 55)
+    bases = O.g1_gen_bases(d)
+    s = O.rand_fr(n, 56)
+    rng = np.random.default_rng(57)
+    pick = rng.random(n)
+    vals = O.fr_vec([1, 2, (1 << 64) + 3])
+    s[pick < 0.3] = vals[0]
+    s[(pick >= 0.3) & (pick < 0.6)] = vals[1]
+    s[(pick >= 0.6) & (pick < 0.9)] = vals[2]
+    for c in (0, 10, 16):
+        assert (_jac_to_aff(O, _run(gpu, bases, s, c)) == O.msm_known_dlog(d, s)).all(), c
+
+
 def test_msm_zero_result_and_empty(O, gpu):
     d = O.rand_fr(2, 61)
     bases = O.g1_gen_bases(d)

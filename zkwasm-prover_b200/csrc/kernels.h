@@ -68,8 +68,8 @@ struct MsmScratch {
     uint32_t* offset;    // NB + 1
     uint32_t* scan_tmp;  // scan_tmp_words(NB)
     uint32_t* entries;   // n * W
-    uint32_t* part_key;  // 2 * nacc
-    Xyzz* part_pt;       // 2 * nacc
+    uint32_t* part_key;  // 2 * nacc + msm_merge_extra(nacc)
+    Xyzz* part_pt;       // 2 * nacc + msm_merge_extra(nacc)
     Xyzz* buckets;       // NB
     Xyzz* segsum;        // W * G
     Xyzz* winsum;        // W
@@ -86,6 +86,8 @@ void msm_layout_split(const MsmPlan& p, uint32_t* words, Xyzz* points, MsmScratc
 cudaError_t msm_run(Jac* out, const Aff* bases, const Fr* scalars, const MsmPlan& p, const MsmScratch& s,
                     cudaStream_t st);
 
+size_t msm_merge_extra(uint32_t nacc);  // merge-level items after the 2 * nacc partials
+// part_key / part_pt hold 2 * nacc + msm_merge_extra(nacc) items
 cudaError_t msm_accumulate_merge(const uint32_t* entries, const uint32_t* offset, uint32_t NB, const Aff* bases,
                                  uint32_t L, uint32_t nacc, Xyzz* buckets, uint32_t* part_key, Xyzz* part_pt,
                                  cudaStream_t st);

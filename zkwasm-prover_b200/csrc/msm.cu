@@ -9,7 +9,8 @@
 //   4. accumulate  every thread owns a fixed-length slice of the sorted entries
 //               and sums runs of equal key with XYZZ + affine additions; runs
 //               that cross a slice boundary are left as head / tail partials
-//   5. merge    each tail partial absorbs the following heads of the same key
+//   5. merge    partials of buckets split across slices: a reduction by key,
+//               warp-segmented scans level by level (log-depth in the split)
 //   6. reduce   per window, segments of buckets by running sums:
 //               sum_b (b+1) B_b = S_seg + lo * T_seg
 //   7. window   tree sum of the segment results per window
@@ -141,19 +142,124 @@ __global__ void __launch_bounds__(128) msm_accumulate_kernel(const uint32_t* __r
     part_key[2 * t + 1] = tail_key;
 }
 
-__global__ void __launch_bounds__(128) msm_merge_kernel(const uint32_t* __restrict__ part_key,
-                                                        const Xyzz* __restrict__ part_pt, uint32_t nacc,
-                                                        Xyzz* __restrict__ buckets) {
-    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= nacc) return;
-    const uint32_t key = part_key[2 * t + 1];
-    if (key == KEY_NONE) return;
-    Xyzz acc = ld_xyzz(part_pt + 2 * t + 1);
-    for (uint32_t u = t + 1; u < nacc; u++) {
-        if (part_key[2 * u] != key) break;
-        acc = xyzz_add(acc, ld_xyzz(part_pt + 2 * u));
+// ---------------------------------------------------------------- merge
+// Buckets split across accumulation slices are summed from the partials by a
+// reduction by key.  Level 0 has one item per slice t: key part_key[2t] (the
+// bucket its slice starts inside, or none) and the head partial, to which the
+// tail partial of slice t-1 is added (a tail is always continued by the next
+// slice's head).  Keys are sorted and an empty item never sits inside a run of
+// one key, so each warp does a segmented inclusive scan of 32 items with
+// shuffles; a run that starts and ends inside the warp is a finished bucket,
+// and the run that enters the warp from the left (slot 2w) or leaves it to the
+// right (slot 2w+1) is passed to the next level, which repeats the same on
+// 2 ceil(M / 32) items.  A bucket over m slices therefore costs O(log m)
+// dependent additions instead of m.
+
+__device__ __forceinline__ Xyzz shfl_up_xyzz(const Xyzz& p, unsigned d) {
+    Xyzz r;
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        r.x.v[i] = __shfl_up_sync(0xffffffffu, p.x.v[i], d);
+        r.y.v[i] = __shfl_up_sync(0xffffffffu, p.y.v[i], d);
+        r.zz.v[i] = __shfl_up_sync(0xffffffffu, p.zz.v[i], d);
+        r.zzz.v[i] = __shfl_up_sync(0xffffffffu, p.zzz.v[i], d);
     }
-    st_xyzz(buckets + key, acc);
+    return r;
+}
+
+template <bool LEVEL0>
+__device__ __forceinline__ uint32_t merge_key(const uint32_t* ikey, uint32_t i) {
+    return LEVEL0 ? ikey[2 * i] : ikey[i];
+}
+
+template <bool LEVEL0>
+__global__ void __launch_bounds__(128) msm_merge_level_kernel(const uint32_t* __restrict__ ikey,
+                                                              const Xyzz* __restrict__ ipt, uint32_t M,
+                                                              uint32_t* __restrict__ okey, Xyzz* __restrict__ opt,
+                                                              Xyzz* __restrict__ buckets) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t base = t - lane;
+    if (base >= M) return;  // whole warps only
+    uint32_t k = t < M ? merge_key<LEVEL0>(ikey, t) : KEY_NONE;
+    Xyzz P = xyzz_identity();
+    if (k != KEY_NONE) {
+        P = ld_xyzz(ipt + (LEVEL0 ? 2 * t : t));
+        if (LEVEL0 && t > 0 && ikey[2 * t - 1] == k) P = xyzz_add(ld_xyzz(ipt + 2 * t - 1), P);
+    }
+    for (unsigned d = 1; d < 32; d <<= 1) {
+        const uint32_t kj = __shfl_up_sync(0xffffffffu, k, d);
+        const Xyzz Q = shfl_up_xyzz(P, d);
+        if (lane >= d && kj == k && k != KEY_NONE) P = xyzz_add(Q, P);
+    }
+    const uint32_t last = (M - base < 32u ? M - base : 32u) - 1;  // last valid lane
+    const uint32_t prev = base > 0 ? merge_key<LEVEL0>(ikey, base - 1) : KEY_NONE;
+    const uint32_t next = base + 32 < M ? merge_key<LEVEL0>(ikey, base + 32) : KEY_NONE;
+    const uint32_t k0 = __shfl_sync(0xffffffffu, k, 0);
+    const uint32_t kl = __shfl_sync(0xffffffffu, k, last);
+    const uint32_t kn = __shfl_down_sync(0xffffffffu, k, 1);
+    const bool from_left = k0 != KEY_NONE && prev == k0;  // the first run started in an earlier warp
+    const bool to_right = kl != KEY_NONE && next == kl;   // the last run continues in a later warp
+    const uint32_t w2 = 2 * (base >> 5);
+    const bool run_end = lane == last || (lane < last && kn != k);
+    if (lane <= last && run_end && k != KEY_NONE) {
+        const bool first = from_left && k == k0, lastrun = to_right && k == kl;
+        if (first && lastrun) {  // the run spans the whole warp
+            okey[w2] = k;
+            st_xyzz(opt + w2, xyzz_identity());
+            okey[w2 + 1] = k;
+            st_xyzz(opt + w2 + 1, P);
+        } else if (first) {
+            okey[w2] = k;
+            st_xyzz(opt + w2, P);
+        } else if (lastrun) {
+            okey[w2 + 1] = k;
+            st_xyzz(opt + w2 + 1, P);
+        } else {
+            st_xyzz(buckets + k, P);
+        }
+    }
+    if (lane == 0 && okey) {
+        if (!from_left) okey[w2] = KEY_NONE;
+        if (!to_right) okey[w2 + 1] = KEY_NONE;
+    }
+}
+
+// items of the merge levels above level 0 (stored after the 2 * nacc partials)
+size_t msm_merge_extra(uint32_t nacc) {
+    size_t total = 0;
+    for (uint32_t M = nacc; M > 32;) {
+        M = 2 * ((M + 31) / 32);
+        total += M;
+    }
+    return total;
+}
+
+static cudaError_t msm_merge(uint32_t* part_key, Xyzz* part_pt, uint32_t nacc, Xyzz* buckets, cudaStream_t st) {
+    const uint32_t* ik = part_key;
+    const Xyzz* ip = part_pt;
+    uint32_t* ok = part_key + 2 * (size_t)nacc;
+    Xyzz* op = part_pt + 2 * (size_t)nacc;
+    uint32_t M = nacc;
+    for (bool level0 = true;; level0 = false) {
+        const bool top = M <= 32;  // one warp: every run ends inside it
+        const uint32_t blocks = (M + 127) / 128;
+        if (level0)
+            msm_merge_level_kernel<true><<<blocks, 128, 0, st>>>(ik, ip, M, top ? nullptr : ok, top ? nullptr : op,
+                                                                 buckets);
+        else
+            msm_merge_level_kernel<false><<<blocks, 128, 0, st>>>(ik, ip, M, top ? nullptr : ok,
+                                                                  top ? nullptr : op, buckets);
+        ZK_CHECK(cudaGetLastError());
+        if (top) break;
+        const uint32_t M2 = 2 * ((M + 31) / 32);
+        ik = ok;
+        ip = op;
+        ok += M2;
+        op += M2;
+        M = M2;
+    }
+    return cudaSuccess;
 }
 
 __global__ void __launch_bounds__(128) msm_reduce_kernel(const Xyzz* __restrict__ buckets,
@@ -253,11 +359,13 @@ size_t msm_u32_words(const MsmPlan& p) {
     w += align_up(p.NB + 1, 64);
     w += align_up(scan_tmp_words(p.NB), 64);
     w += align_up((size_t)p.n * p.W, 64);
-    w += align_up((size_t)2 * p.nacc, 64);
+    w += align_up((size_t)2 * p.nacc + msm_merge_extra(p.nacc), 64);
     return w;
 }
 
-size_t msm_point_count(const MsmPlan& p) { return (size_t)2 * p.nacc + p.NB + (size_t)p.W * p.G + p.W; }
+size_t msm_point_count(const MsmPlan& p) {
+    return (size_t)2 * p.nacc + msm_merge_extra(p.nacc) + p.NB + (size_t)p.W * p.G + p.W;
+}
 
 size_t msm_scratch_bytes(const MsmPlan& p) {
     return align_up(msm_u32_words(p) * 4, 256) + msm_point_count(p) * sizeof(Xyzz);
@@ -276,7 +384,7 @@ void msm_layout_split(const MsmPlan& p, uint32_t* words, Xyzz* points, MsmScratc
     s->part_key = w;
     Xyzz* q = points;
     s->part_pt = q;
-    q += (size_t)2 * p.nacc;
+    q += (size_t)2 * p.nacc + msm_merge_extra(p.nacc);
     s->buckets = q;
     q += p.NB;
     s->segsum = q;
@@ -297,8 +405,7 @@ cudaError_t msm_accumulate_merge(const uint32_t* entries, const uint32_t* offset
     msm_accumulate_kernel<<<(nacc + 127) / 128, 128, 0, st>>>(entries, offset, NB, bases, L, nacc, buckets, part_key,
                                                               part_pt);
     ZK_CHECK(cudaGetLastError());
-    msm_merge_kernel<<<(nacc + 127) / 128, 128, 0, st>>>(part_key, part_pt, nacc, buckets);
-    return cudaGetLastError();
+    return msm_merge(part_key, part_pt, nacc, buckets, st);
 }
 
 cudaError_t msm_run(Jac* out, const Aff* bases, const Fr* scalars, const MsmPlan& p, const MsmScratch& s,
@@ -319,8 +426,7 @@ cudaError_t msm_run(Jac* out, const Aff* bases, const Fr* scalars, const MsmPlan
     msm_accumulate_kernel<<<(p.nacc + 127) / 128, 128, 0, st>>>(s.entries, s.offset, p.NB, bases, p.L, p.nacc,
                                                                 s.buckets, s.part_key, s.part_pt);
     ZK_CHECK(cudaGetLastError());
-    msm_merge_kernel<<<(p.nacc + 127) / 128, 128, 0, st>>>(s.part_key, s.part_pt, p.nacc, s.buckets);
-    ZK_CHECK(cudaGetLastError());
+    ZK_CHECK(msm_merge(s.part_key, s.part_pt, p.nacc, s.buckets, st));
     const uint32_t nred = (uint32_t)p.W * p.G;
     msm_reduce_kernel<<<(nred + 127) / 128, 128, 0, st>>>(s.buckets, s.offset, p.W, p.B, p.seg, p.G, s.segsum);
     ZK_CHECK(cudaGetLastError());

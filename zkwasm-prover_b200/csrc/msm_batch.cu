@@ -191,9 +191,9 @@ static bool batch_plan(const uint32_t* n, const int* c, uint32_t count, BatchLay
     L.off_entries = o;
     o = al(o + ent * 4);
     L.off_pkey = o;
-    o = al(o + (size_t)2 * L.nacc * 4);
+    o = al(o + ((size_t)2 * L.nacc + msm_merge_extra(L.nacc)) * 4);
     L.off_ppt = o;
-    o = al(o + (size_t)2 * L.nacc * sizeof(Xyzz));
+    o = al(o + ((size_t)2 * L.nacc + msm_merge_extra(L.nacc)) * sizeof(Xyzz));
     L.off_buckets = o;
     o = al(o + (size_t)L.NB * sizeof(Xyzz));
     L.off_segsum = o;

@@ -5,11 +5,12 @@ The reference picks the MSM window width with a fixed formula
 
 * ``default``  - the library's cost formula (``zkp_msm_default_window``);
 * ``autotune`` - ``zkp_msm_autotune``: time every candidate window on the
-  actual bases and scalars and keep the fastest (the judge of the others);
+  actual bases and scalars and keep the fastest (the yardstick for the others);
 * ``learned``  - an MLP cost model (``zkp_mlp_*`` kernels) trained on the
-  autotuner's own measurements, predicting log(ms) from the shape features
-  [log2 n / 24, log2 batch / 8, scalar bit-length histogram (7 bins),
-  (c - 12) / 8]; the window with the smallest prediction wins.
+  autotuner's own measurements, predicting log(ms per MSM) from the shape
+  features [log2 n / 24, log2 batch / 8, scalar bit-length histogram
+  (7 bins), (c - 12) / 8], where batch is the number of MSMs sharing one
+  zkp_msm_batch pipeline; the window with the smallest prediction wins.
 
 A schedule only chooses the window width, so every picker gives the same
 MSM result; regret (ms) is measured against the autotuner's best.
@@ -179,28 +180,72 @@ class Model:
 # ------------------------------------------------------------------ dataset / evaluation
 
 
-def collect(sizes, mixes=MIXES, reps=2, seed=100, c_min=C_MIN, c_max=C_MAX):
-    """Autotune every (size, mix) shape; one record per shape."""
+def autotune_batch(bases, cols, n: int, c_min=C_MIN, c_max=C_MAX, reps=2):
+    """Exhaustive search for len(cols) same-shape MSMs run as one zkp_msm_batch
+    pipeline with one window for all; returns (best c, {c: ms per batch}).
+    Windows whose pipeline does not fit (2^32 or more sorted entries) are left
+    out."""
+    L = lib()
+    count = len(cols)
+    ns = [n] * count
+    n_arr = (ctypes.c_uint32 * count)(*ns)
+    need, ok = 0, []
+    for c in range(c_min, c_max + 1):
+        c_arr = (ctypes.c_int * count)(*([c] * count))
+        b = L.zkp_msm_batch_scratch_bytes(ctypes.addressof(n_arr), ctypes.addressof(c_arr), count)
+        if b:
+            ok.append(c)
+            need = max(need, b)
+    scratch = torch.empty(max(1, need), dtype=torch.uint8, device="cuda")
+    out = torch.empty((count, 12), dtype=torch.int64, device="cuda")
+    times = {}
+    for c in ok:
+        ws = [c] * count
+        H.msm_batch(bases, cols, ns, ws, scratch=scratch, out=out)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(reps):
+            H.msm_batch(bases, cols, ns, ws, scratch=scratch, out=out)
+        b.record()
+        b.synchronize()
+        times[c] = a.elapsed_time(b) / reps
+    del scratch
+    return min(times, key=times.get), times
+
+
+def collect(sizes, mixes=MIXES, batches=(1,), reps=2, seed=100, c_min=C_MIN, c_max=C_MAX, max_points=1 << 26):
+    """Autotune every (size, batch, mix) shape; one record per shape.  A batch
+    of b is b same-shape MSMs (independent scalars) through one zkp_msm_batch
+    pipeline; batch 1 uses zkp_msm.  "times_ms" is the time of the whole
+    batch.  Shapes above max_points scalars in total are skipped."""
     records = []
     nmax = max(sizes)
     bases, _ = bases_with_known_logs(nmax, seed)
     for n in sizes:
-        for mi, mix in enumerate(mixes):
-            s = scalars(n, mix, seed + 17 * n.bit_length() + mi)
-            hist = histogram(s)
-            best, times = autotune(bases, s, n, c_min, c_max, reps)
-            records.append({"n": n, "batch": 1, "mix": mix, "hist": hist, "best": best, "times_ms": times})
-            del s
+        for batch in batches:
+            if n * batch > max_points:
+                continue
+            for mi, mix in enumerate(mixes):
+                cols = [scalars(n, mix, seed + 17 * n.bit_length() + 1000 * j + mi) for j in range(batch)]
+                hist = histogram(cols[0])
+                if batch == 1:
+                    best, times = autotune(bases, cols[0], n, c_min, c_max, reps)
+                else:
+                    best, times = autotune_batch(bases, cols, n, c_min, c_max, reps)
+                records.append({"n": n, "batch": batch, "mix": mix, "hist": hist, "best": best,
+                                "times_ms": times})
+                del cols
     return records
 
 
 def training_set(records):
+    """Model inputs and targets: log(ms per MSM) of every measured window."""
     X, y = [], []
     for r in records:
         f = shape_features(r["n"], r["batch"], r["hist"])
         for c, ms in r["times_ms"].items():
             X.append(model_input(f, int(c)))
-            y.append(math.log(ms))
+            y.append(math.log(ms / r["batch"]))
     return np.array(X, np.float32), np.array(y, np.float32)
 
 
@@ -213,7 +258,8 @@ def regret(records, picker):
         c = picker(r)
         if c not in times:  # outside the measured range: charge the nearest measured window
             c = min(times, key=lambda k: abs(k - c))
-        rows.append({"n": r["n"], "mix": r["mix"], "picked": c, "regret_ms": times[c] - best})
+        rows.append({"n": r["n"], "batch": r["batch"], "mix": r["mix"], "picked": c,
+                     "regret_ms": times[c] - best})
         total += times[c] - best
     return total, rows
 

@@ -2,8 +2,10 @@
 
     python zkwasm-prover_b200/train_schedule.py OUT_DIR
 
-1. autotunes every (size, scalar mix) shape for sizes 2^12..2^22 and four
-   scalar distributions (uniform, small < 2^20, 90%-sparse, mixed);
+1. autotunes every (size, batch, scalar mix) shape for sizes 2^12..2^22,
+   batches of 1, 4, 16 and 32 same-size MSMs in one zkp_msm_batch pipeline
+   (at most 2^26 scalars per batch) and four scalar distributions (uniform,
+   small < 2^20, 90%-sparse, mixed);
 2. trains the MLP with the library's kernels on the even sizes;
 3. evaluates the window picked by the model, by the library's default
    formula and by the reference's formula (src/cuda/msm.rs:105) on the
@@ -25,7 +27,7 @@ def main(out_dir):
     S = zkp.schedule
     os.makedirs(out_dir, exist_ok=True)
     sizes = [1 << k for k in range(12, 23)]
-    records = S.collect(sizes)
+    records = S.collect(sizes, batches=(1, 4, 16, 32), max_points=1 << 26)
     train = [r for r in records if (r["n"].bit_length() - 1) % 2 == 0]
     test = [r for r in records if (r["n"].bit_length() - 1) % 2 == 1]
     X, y = S.training_set(train)
@@ -40,12 +42,13 @@ def main(out_dir):
     for name, recs in (("train", train), ("test", test)):
         res = {}
         for pname, picker in (("learned", learned), ("default", lambda r: S.default_window(r["n"])),
-                              ("reference_formula", lambda r: S.reference_window(r["n"]))):
+                              ("reference_formula", lambda r: S.reference_window(r["n"], r["batch"]))):
             tot, rows = S.regret(recs, picker)
             res[pname] = {"total_regret_ms": tot, "rows": rows}
         res["best_total_ms"] = sum(min(r["times_ms"].values()) for r in recs)
         out[name] = res
-    model.save(os.path.join(out_dir, "msm_schedule_model.npz"), meta={"trained_on": "even log2 sizes 12..22"})
+    model.save(os.path.join(out_dir, "msm_schedule_model.npz"),
+               meta={"trained_on": "even log2 sizes 12..22, batches 1/4/16/32"})
     with open(os.path.join(out_dir, "msm_schedule_data.json"), "w") as f:
         json.dump(records, f)
     with open(os.path.join(out_dir, "msm_schedule_eval.json"), "w") as f:
