@@ -323,12 +323,15 @@ size_t zkp_mlp_param_count(void);
 size_t zkp_mlp_scratch_floats(uint32_t B);
 cudaError_t zkp_mlp_init(float *params, uint64_t seed, cudaStream_t stream);
 cudaError_t zkp_mlp_forward(const float *params, const float *X, uint32_t B, float *y, cudaStream_t stream);
-/* mean squared error over the batch and its gradient (loss: device float) */
-cudaError_t zkp_mlp_grad(const float *params, const float *X, const float *t, uint32_t B, float *grads, float *loss,
-                         float *scratch, cudaStream_t stream);
+/* mean squared error over the batch, each sample's squared error scaled by
+ * weights[b] (device floats; null = all 1), and its gradient (loss: device
+ * float) */
+cudaError_t zkp_mlp_grad(const float *params, const float *X, const float *t, const float *weights, uint32_t B,
+                         float *grads, float *loss, float *scratch, cudaStream_t stream);
 /* one Adam step, step >= 1 */
 cudaError_t zkp_mlp_train_step(float *params, float *grads, float *m, float *v, const float *X, const float *t,
-                               uint32_t B, float lr, int step, float *loss, float *scratch, cudaStream_t stream);
+                               const float *weights, uint32_t B, float lr, int step, float *loss, float *scratch,
+                               cudaStream_t stream);
 /* window with the smallest predicted time for the nine shape features
  * (host array); scratch: 256 device floats; synchronises the stream */
 int zkp_msm_schedule_predict(const float *params, const float *features, int c_min, int c_max, float *scratch,

@@ -10,8 +10,10 @@ import torch
 pytestmark = pytest.mark.gpu
 
 
-def _np_grad(params, X, t):
-    """Analytic gradient of the batch MSE for the kernel's parameter layout."""
+def _np_grad(params, X, t, w=None):
+    """Analytic gradient of the (weighted) batch MSE for the kernel's parameter
+    layout."""
+    w = np.ones(X.shape[0]) if w is None else w
     D, H1, H2 = X.shape[1], 64, 64
     sizes = [D * H1, H1, H1 * H2, H2, H2, 1]
     offs = np.cumsum([0] + sizes)
@@ -27,7 +29,7 @@ def _np_grad(params, X, t):
     h2 = np.maximum(z2, 0)
     y = h2 @ W3 + b3
     B = X.shape[0]
-    g = 2 * (y - t) / B
+    g = 2 * w * (y - t) / B
     dW3 = h2.T @ g
     db3 = g.sum()
     d2 = np.outer(g, W3) * (z2 > 0)
@@ -36,7 +38,7 @@ def _np_grad(params, X, t):
     d1 = (d2 @ W2.T) * (z1 > 0)
     dW1 = X.T @ d1
     db1 = d1.sum(0)
-    loss = np.mean((y - t) ** 2)
+    loss = np.mean(w * (y - t) ** 2)
     return np.concatenate([dW1.ravel(), db1, dW2.ravel(), db2, dW3, [db3]]), loss, y
 
 
@@ -50,19 +52,23 @@ def test_mlp_forward_and_gradient(gpu):
     X = rng.normal(size=(B, D)).astype(np.float32)
     t = rng.normal(size=B).astype(np.float32)
     p = m.params.cpu().numpy().astype(np.float64)
-    g_np, loss_np, y_np = _np_grad(p, X.astype(np.float64), t.astype(np.float64))
-    assert np.allclose(m.predict(X), y_np, rtol=1e-4, atol=1e-4)
-    assert np.allclose(S.mlp_forward_numpy(p, X.astype(np.float64)), y_np)
-    xd, td = torch.from_numpy(X).cuda(), torch.from_numpy(t).cuda()
-    grads = torch.empty_like(m.params)
-    loss = torch.zeros(1, dtype=torch.float32, device="cuda")
-    scratch = torch.empty(L.zkp_mlp_scratch_floats(B), dtype=torch.float32, device="cuda")
-    gpu.abi.check(L.zkp_mlp_grad(m.params.data_ptr(), xd.data_ptr(), td.data_ptr(), B, grads.data_ptr(),
-                                 loss.data_ptr(), scratch.data_ptr(), gpu.host.stream_handle()))
-    g = grads.cpu().numpy()
-    assert abs(float(loss.item()) - loss_np) <= 1e-4 * max(1.0, loss_np)
-    # FP32 kernel vs float64 NumPy: tolerance 1e-4 relative to the gradient norm
-    assert np.max(np.abs(g - g_np)) <= 1e-4 * max(1.0, np.max(np.abs(g_np)))
+    wts = rng.uniform(0.2, 3.0, size=B).astype(np.float32)
+    xd, td, wd = torch.from_numpy(X).cuda(), torch.from_numpy(t).cuda(), torch.from_numpy(wts).cuda()
+    for w in (None, wts):
+        g_np, loss_np, y_np = _np_grad(p, X.astype(np.float64), t.astype(np.float64),
+                                       None if w is None else w.astype(np.float64))
+        assert np.allclose(m.predict(X), y_np, rtol=1e-4, atol=1e-4)
+        assert np.allclose(S.mlp_forward_numpy(p, X.astype(np.float64)), y_np)
+        grads = torch.empty_like(m.params)
+        loss = torch.zeros(1, dtype=torch.float32, device="cuda")
+        scratch = torch.empty(L.zkp_mlp_scratch_floats(B), dtype=torch.float32, device="cuda")
+        gpu.abi.check(L.zkp_mlp_grad(m.params.data_ptr(), xd.data_ptr(), td.data_ptr(),
+                                     None if w is None else wd.data_ptr(), B, grads.data_ptr(), loss.data_ptr(),
+                                     scratch.data_ptr(), gpu.host.stream_handle()))
+        g = grads.cpu().numpy()
+        assert abs(float(loss.item()) - loss_np) <= 1e-4 * max(1.0, loss_np)
+        # FP32 kernel vs float64 NumPy: tolerance 1e-4 relative to the gradient norm
+        assert np.max(np.abs(g - g_np)) <= 1e-4 * max(1.0, np.max(np.abs(g_np)))
 
 
 def test_mlp_training_fits(gpu):

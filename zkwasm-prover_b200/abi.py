@@ -75,8 +75,8 @@ SIGNATURES = {
     "zkp_mlp_scratch_floats": ([U], SZ),
     "zkp_mlp_init": [P, ctypes.c_uint64, S],
     "zkp_mlp_forward": [P, P, U, P, S],
-    "zkp_mlp_grad": [P, P, P, U, P, P, P, S],
-    "zkp_mlp_train_step": [P, P, P, P, P, P, U, ctypes.c_float, I, P, P, S],
+    "zkp_mlp_grad": [P, P, P, P, U, P, P, P, S],
+    "zkp_mlp_train_step": [P, P, P, P, P, P, P, U, ctypes.c_float, I, P, P, S],
     "zkp_msm_schedule_predict": ([P, P, I, I, P, S], I),
     "zkp_calib_mont_rate": [P, U, U, S],
 }

@@ -84,12 +84,16 @@ __global__ void mlp_forward_kernel(const float* P, const float* X, uint32_t B, f
 }
 
 // per-sample output error g_b = 2 (y_b - t_b) / B and the loss sum
-__global__ void mlp_dloss_kernel(const float* y, const float* t, uint32_t B, float* g, float* loss) {
+// weighted mean squared error: loss = sum_b w_b (y_b - t_b)^2 / B (w_b = 1
+// when w is null); g_b = dloss / dy_b
+__global__ void mlp_dloss_kernel(const float* y, const float* t, const float* w, uint32_t B, float* g,
+                                 float* loss) {
     const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= B) return;
     const float e = y[b] - t[b];
-    g[b] = 2.f * e / (float)B;
-    atomicAdd(loss, e * e / (float)B);
+    const float wb = w ? w[b] : 1.f;
+    g[b] = 2.f * wb * e / (float)B;
+    atomicAdd(loss, wb * e * e / (float)B);
 }
 
 // per-sample backward to the hidden layers: d2[b][k] = g_b W3[k] 1(h2>0),
@@ -193,10 +197,11 @@ cudaError_t zkp_mlp_forward(const float* params, const float* X, uint32_t B, flo
     return cudaGetLastError();
 }
 
-// gradient of the mean squared error over the batch; loss (device float) is
-// overwritten; scratch: zkp_mlp_scratch_floats(B) floats
-cudaError_t zkp_mlp_grad(const float* params, const float* X, const float* t, uint32_t B, float* grads, float* loss,
-                         float* scratch, cudaStream_t stream) {
+// gradient of the (optionally per-sample weighted) mean squared error over the
+// batch; weights may be null; loss (device float) is overwritten; scratch:
+// zkp_mlp_scratch_floats(B) floats
+cudaError_t zkp_mlp_grad(const float* params, const float* X, const float* t, const float* weights, uint32_t B,
+                         float* grads, float* loss, float* scratch, cudaStream_t stream) {
     if (!params || !X || !t || !grads || !loss || !scratch || B == 0) return cudaErrorInvalidValue;
     float* y = scratch;
     float* g = y + B;
@@ -205,7 +210,7 @@ cudaError_t zkp_mlp_grad(const float* params, const float* X, const float* t, ui
     ZK_CHECK(cudaMemsetAsync(loss, 0, sizeof(float), stream));
     const unsigned gb = (B + 127) / 128;
     mlp_forward_kernel<<<gb, 128, 0, stream>>>(params, X, B, y, act);
-    mlp_dloss_kernel<<<gb, 128, 0, stream>>>(y, t, B, g, loss);
+    mlp_dloss_kernel<<<gb, 128, 0, stream>>>(y, t, weights, B, g, loss);
     mlp_backward_hidden_kernel<<<gb, 128, 0, stream>>>(params, act, g, B, d);
     mlp_param_grad_kernel<<<(P_COUNT + 127) / 128, 128, 0, stream>>>(X, act, g, d, B, grads);
     return cudaGetLastError();
@@ -213,9 +218,10 @@ cudaError_t zkp_mlp_grad(const float* params, const float* X, const float* t, ui
 
 // one Adam step (step counts from 1); m and v hold the moments
 cudaError_t zkp_mlp_train_step(float* params, float* grads, float* m, float* v, const float* X, const float* t,
-                               uint32_t B, float lr, int step, float* loss, float* scratch, cudaStream_t stream) {
+                               const float* weights, uint32_t B, float lr, int step, float* loss, float* scratch,
+                               cudaStream_t stream) {
     if (step < 1) return cudaErrorInvalidValue;
-    ZK_CHECK(zkp_mlp_grad(params, X, t, B, grads, loss, scratch, stream));
+    ZK_CHECK(zkp_mlp_grad(params, X, t, weights, B, grads, loss, scratch, stream));
     const float b1c = 1.f - powf(0.9f, (float)step), b2c = 1.f - powf(0.999f, (float)step);
     adam_kernel<<<(P_COUNT + 255) / 256, 256, 0, stream>>>(params, grads, m, v, lr, b1c, b2c);
     return cudaGetLastError();

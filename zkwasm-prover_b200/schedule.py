@@ -7,10 +7,11 @@ The reference picks the MSM window width with a fixed formula
 * ``autotune`` - ``zkp_msm_autotune``: time every candidate window on the
   actual bases and scalars and keep the fastest (the yardstick for the others);
 * ``learned``  - an MLP cost model (``zkp_mlp_*`` kernels) trained on the
-  autotuner's own measurements, predicting log(ms per MSM) from the shape
-  features [log2 n / 24, log2 batch / 8, scalar bit-length histogram
-  (7 bins), (c - 12) / 8], where batch is the number of MSMs sharing one
-  zkp_msm_batch pipeline; the window with the smallest prediction wins.
+  autotuner's own measurements, predicting log(ms) relative to the shape's
+  mean over windows from the shape features [log2 n / 24, log2 batch / 8,
+  scalar bit-length histogram (7 bins), (c - 12) / 8], where batch is the
+  number of MSMs sharing one zkp_msm_batch pipeline; the window with the
+  smallest prediction wins.
 
 A schedule only chooses the window width, so every picker gives the same
 MSM result; regret (ms) is measured against the autotuner's best.
@@ -147,10 +148,13 @@ class Model:
                                         H.stream_handle()), "zkp_mlp_forward")
         return y.cpu().numpy()
 
-    def train(self, X: np.ndarray, y: np.ndarray, steps=4000, lr=3e-3):
+    def train(self, X: np.ndarray, y: np.ndarray, steps=4000, lr=3e-3, weights=None):
+        """Full-batch Adam on the (weighted) mean squared error; returns the
+        loss history [(step, loss)]."""
         L = lib()
         x = torch.from_numpy(np.ascontiguousarray(X, np.float32)).cuda()
         t = torch.from_numpy(np.ascontiguousarray(y, np.float32)).cuda()
+        w = None if weights is None else torch.from_numpy(np.ascontiguousarray(weights, np.float32)).cuda()
         B = x.shape[0]
         g = torch.zeros_like(self.params)
         m = torch.zeros_like(self.params)
@@ -161,7 +165,8 @@ class Model:
         hist = []
         for step in range(1, steps + 1):
             abi.check(L.zkp_mlp_train_step(self.params.data_ptr(), g.data_ptr(), m.data_ptr(), v.data_ptr(),
-                                           x.data_ptr(), t.data_ptr(), B, lr, step, loss.data_ptr(),
+                                           x.data_ptr(), t.data_ptr(), None if w is None else w.data_ptr(),
+                                           B, lr, step, loss.data_ptr(),
                                            scratch.data_ptr(), st), "zkp_mlp_train_step")
             if step == 1 or step % 500 == 0:
                 hist.append((step, float(loss.item())))
@@ -239,14 +244,24 @@ def collect(sizes, mixes=MIXES, batches=(1,), reps=2, seed=100, c_min=C_MIN, c_m
 
 
 def training_set(records):
-    """Model inputs and targets: log(ms per MSM) of every measured window."""
-    X, y = [], []
+    """Model inputs, targets and sample weights.  The target of window c is
+    log(ms) minus its mean over the shape's measured windows: the pick is an
+    argmin over the windows of one shape, so a per-shape offset carries no
+    information and the model's capacity goes to how time depends on c.  The
+    weight sqrt(fastest ms of the shape), normalised to mean 1, makes the
+    shapes where a wrong pick costs the most milliseconds count the most."""
+    X, y, w = [], [], []
     for r in records:
         f = shape_features(r["n"], r["batch"], r["hist"])
-        for c, ms in r["times_ms"].items():
-            X.append(model_input(f, int(c)))
-            y.append(math.log(ms / r["batch"]))
-    return np.array(X, np.float32), np.array(y, np.float32)
+        logs = {int(c): math.log(ms) for c, ms in r["times_ms"].items()}
+        mean = sum(logs.values()) / len(logs)
+        wt = math.sqrt(min(r["times_ms"].values()))
+        for c, lt in logs.items():
+            X.append(model_input(f, c))
+            y.append(lt - mean)
+            w.append(wt)
+    w = np.array(w, np.float32)
+    return np.array(X, np.float32), np.array(y, np.float32), w / w.mean()
 
 
 def regret(records, picker):

@@ -1,12 +1,16 @@
 """Train the MSM schedule model on this GPU.
 
-    python zkwasm-prover_b200/train_schedule.py OUT_DIR
+    python zkwasm-prover_b200/train_schedule.py OUT_DIR [RECORDS.json]
+
+With RECORDS.json (a msm_schedule_data.json written earlier) the timings are
+read from it instead of measured again.
 
 1. autotunes every (size, batch, scalar mix) shape for sizes 2^12..2^22,
    batches of 1, 4, 16 and 32 same-size MSMs in one zkp_msm_batch pipeline
    (at most 2^26 scalars per batch) and four scalar distributions (uniform,
    small < 2^20, 90%-sparse, mixed);
-2. trains the MLP with the library's kernels on the even sizes;
+2. trains the MLP with the library's kernels on the even sizes (weighted
+   mean squared error of per-shape centred log times);
 3. evaluates the window picked by the model, by the library's default
    formula and by the reference's formula (src/cuda/msm.rs:105) on the
    held-out odd sizes, as regret in ms against the autotuner's best;
@@ -22,17 +26,21 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(HERE))
 
 
-def main(out_dir):
+def main(out_dir, records_path=None):
     zkp = importlib.import_module("zkwasm-prover_b200")
     S = zkp.schedule
     os.makedirs(out_dir, exist_ok=True)
     sizes = [1 << k for k in range(12, 23)]
-    records = S.collect(sizes, batches=(1, 4, 16, 32), max_points=1 << 26)
+    if records_path:
+        with open(records_path) as f:
+            records = json.load(f)
+    else:
+        records = S.collect(sizes, batches=(1, 4, 16, 32), max_points=1 << 26)
     train = [r for r in records if (r["n"].bit_length() - 1) % 2 == 0]
     test = [r for r in records if (r["n"].bit_length() - 1) % 2 == 1]
-    X, y = S.training_set(train)
+    X, y, w = S.training_set(train)
     model = S.Model.fresh(seed=7)
-    loss_hist = model.train(X, y, steps=6000, lr=3e-3)
+    loss_hist = model.train(X, y, steps=10000, lr=3e-3, weights=w)
 
     def learned(r):
         return model.pick(S.shape_features(r["n"], r["batch"], r["hist"]))
@@ -58,4 +66,4 @@ def main(out_dir):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "gpurun_out")
+    main(sys.argv[1] if len(sys.argv) > 1 else "schedule_out", sys.argv[2] if len(sys.argv) > 2 else None)
