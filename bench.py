@@ -424,6 +424,17 @@ def max_over_ranks(x, ws):
     return float(t.item())
 
 
+def run_msm_only(args):
+    """Single MSMs through zkp_msm (device-resident inputs) at the given sizes;
+    one JSON line.  Used for profiling the MSM kernels on their own."""
+    torch.cuda.set_device(0)
+    zkp = importlib.import_module("zkwasm-prover_b200")
+    zkp.load_library()
+    sizes = tuple(1 << int(x) for x in args.msm_log_sizes.split(","))
+    print(json.dumps({"metric": "MSM Mpts/s", "msm": run_msm(zkp, torch.device("cuda", 0), sizes=sizes,
+                                                            reps=max(1, args.steps))}))
+
+
 def run_ours(args):
     ws, rank, local = dist_setup()
     device = torch.device("cuda", local)
@@ -687,9 +698,13 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-msm", action="store_true")
     ap.add_argument("--no-reference-gpu", action="store_true")
+    ap.add_argument("--msm-only", action="store_true", help="time only single MSMs (sizes from --msm-log-sizes)")
+    ap.add_argument("--msm-log-sizes", default="18,22")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
+    elif args.msm_only:
+        run_msm_only(args)
     else:
         run_ours(args)
 

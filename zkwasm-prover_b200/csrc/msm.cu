@@ -95,46 +95,51 @@ __global__ void __launch_bounds__(128) msm_accumulate_kernel(const uint32_t* __r
     if (s < total) {
         const uint32_t e = min(s + L, total);
         uint32_t key = find_bucket(offset, 0, NB, s);
-        uint32_t pos = s;
-        // the base of the next entry is prefetched into L1 while the current
-        // one is added (a register copy would cost occupancy)
-        uint32_t ent_next = entries[pos];
+        uint32_t kbeg = offset[key], kend = offset[key + 1];
+        // One flat loop over the slice: every lane adds one entry per
+        // iteration, so the lanes of a warp stay in step across bucket
+        // boundaries (a loop per bucket run would idle the lanes whose runs
+        // end first).  The base of the next entry is prefetched into L1 while
+        // the current one is added (a register copy would cost occupancy).
+        Xyzz acc = xyzz_identity();
+        uint32_t ent_next = entries[s];
         prefetch_l1(bases + (ent_next & 0x7fffffffu));
-        while (pos < e) {
-            const uint32_t kbeg = offset[key], kend = offset[key + 1];
-            const uint32_t rend = min(kend, e);
-            Xyzz acc = xyzz_identity();
-            for (uint32_t p = pos; p < rend; p++) {
-                const uint32_t ent = ent_next;
-                if (p + 1 < e) {
-                    ent_next = entries[p + 1];
-                    prefetch_l1(bases + (ent_next & 0x7fffffffu));
-                }
-                Aff a = ld_aff(bases + (ent & 0x7fffffffu));
-                if (aff_is_id(a)) continue;
+        for (uint32_t p = s; p < e; p++) {
+            const uint32_t ent = ent_next;
+            if (p + 1 < e) {
+                ent_next = entries[p + 1];
+                prefetch_l1(bases + (ent_next & 0x7fffffffu));
+            }
+            Aff a = ld_aff(bases + (ent & 0x7fffffffu));
+            if (!aff_is_id(a)) {
                 if (ent >> 31) a.y = fe_neg<FqCfg>(a.y);
                 acc = xyzz_add_aff(acc, a.x, a.y);
             }
-            const bool before = kbeg < s;
-            const bool after = kend > e;
-            if (!before && !after) {
-                st_xyzz(buckets + key, acc);
-            } else if (before) {
-                head_key = key;
-                st_xyzz(part_pt + 2 * t, acc);
-            } else {
-                tail_key = key;
-                st_xyzz(part_pt + 2 * t + 1, acc);
-            }
-            pos = rend;
-            if (pos < e) {
-                // the next non-empty bucket is usually within a few keys
-                uint32_t k = key + 1, tries = 0;
-                while (tries < 8 && offset[k + 1] <= pos) {
-                    k++;
-                    tries++;
+            if (p + 1 == kend || p + 1 == e) {  // the run of this bucket ends here
+                const bool before = kbeg < s;
+                const bool after = kend > e;
+                if (!before && !after) {
+                    st_xyzz(buckets + key, acc);
+                } else if (before) {
+                    head_key = key;
+                    st_xyzz(part_pt + 2 * t, acc);
+                } else {
+                    tail_key = key;
+                    st_xyzz(part_pt + 2 * t + 1, acc);
                 }
-                key = (offset[k + 1] > pos) ? k : find_bucket(offset, k, NB, pos);
+                acc = xyzz_identity();
+                if (p + 1 < e) {
+                    // the next non-empty bucket is usually within a few keys
+                    const uint32_t pos = p + 1;
+                    uint32_t k = key + 1, tries = 0;
+                    while (tries < 8 && offset[k + 1] <= pos) {
+                        k++;
+                        tries++;
+                    }
+                    key = (offset[k + 1] > pos) ? k : find_bucket(offset, k, NB, pos);
+                    kbeg = offset[key];
+                    kend = offset[key + 1];
+                }
             }
         }
     }
