@@ -171,10 +171,11 @@ class ExtendPhase:
         return ["intt_pass1", "intt_pass2", "coset_pass1", "coset_pass2"]
 
     def stage_bytes(self):
-        """unique bytes each stage launch must read + write (one chunk)."""
+        """algorithmic bytes each stage launch must read + write (one chunk):
+        its input and output columns, no twiddle or twist tables."""
         c, n, E = self.chunk, self.n, self.E
         if self.fused():
-            return [2 * c * n * 32, 0, (2 + 2 * E) * c * n * 32, 2 * E * c * n * 32]
+            return [2 * c * n * 32, 0, (2 + E) * c * n * 32, 2 * E * c * n * 32]
         return [2 * c * n * 32, 2 * c * n * 32, (2 + E) * c * n * 32, 2 * E * c * n * 32]
 
     def stage_mults(self):
