@@ -144,21 +144,28 @@ cudaError_t eval_logup_z_compose(void *z, void *input, void *table, void *multip
 cudaError_t eval_logup_z_pure(void *z, void *input, void *table, void *last_z, int last_z_index, int n,
                               cudaStream_t stream);
 
-/* src/cuda/bn254_c.rs:248-259, cuda/msm.cu:434-467.  The whole MSM already ran
- * inside msm(); this leaves each result where the reference does (element 0
- * of each per-MSM region) and only reports pending errors. */
+/* src/cuda/bn254_c.rs:248-259, cuda/msm.cu:434-467.  buckets is the device
+ * array of batch_size pointers to the per-MSM regions msm() ran in
+ * (src/cuda/msm.rs:387-420); one launch runs the final window combination of
+ * every MSM side by side and writes each Jacobian result where the reference
+ * does, element 0 of its region.  Must follow the msm() calls in stream order
+ * (the reference host synchronises their streams first).  Returns pending
+ * errors of earlier launches, as the reference does.  The other arguments are
+ * accepted and unused. */
 cudaError_t batch_msm_collect(void *remain_indices, void *remain_acc, void *next_remain_indices,
                               void *next_remain_acc, void *buckets, uint32_t workers, uint32_t windows,
                               uint32_t window_bits, uint32_t batch_size, cudaStream_t stream);
 
 /* src/cuda/bn254_c.rs:261-279, cuda/msm.cu:350-432.  Computes
  * sum_i [s_i] p_i for array_len affine bases p and Montgomery-form scalars s
- * and writes the Jacobian sum to res[0] (96 bytes).  res must span the
- * reference's per-MSM region of (windows << window_bits) + 2 * workers
- * Jacobian points and sort_buf 3 * array_len * windows u32 (the sizes
- * src/cuda/msm.rs:297-317 allocates); both are used as scratch.  The other
- * index buffers, threads, workers, the sort-storage size and skip_zero are
- * accepted and unused.  Never blocks the host. */
+ * up to the per-window sums, which stay in the region with a note of where
+ * they are; batch_msm_collect then writes the Jacobian sum to res[0] (96
+ * bytes), as in the reference.  res must span the reference's per-MSM region
+ * of (windows << window_bits) + 2 * workers Jacobian points and sort_buf
+ * 3 * array_len * windows u32 (the sizes src/cuda/msm.rs:297-317 allocates);
+ * both are used as scratch.  The other index buffers, threads, workers, the
+ * sort-storage size and skip_zero are accepted and unused.  Never blocks the
+ * host. */
 cudaError_t msm(void *res, void *p, void *s, void *indices_buf0, void *indices_buf1, void *indices_buf2,
                 void *indices_buf3, void *sort_buf, void *indices_buf, int array_len, int windows, int window_bits,
                 int threads, int workers, int prepared_sort_indices_temp_storage_bytes, int skip_zero,

@@ -231,6 +231,10 @@ cudaError_t eval_logup_z_pure(void* z, void* input, void* table, void* last_z, i
     return zk::logup_z_scan(F(z), F(last_z), last_z_index, (uint32_t)n, F(table), stream);
 }
 
+// byte offset, inside the 256-byte head of each MSM region, of the note msm()
+// leaves for batch_msm_collect (the Jacobian result takes bytes 0..95)
+static constexpr uint32_t MSM_NOTE_OFF = 128;
+
 cudaError_t batch_msm_collect(void* remain_indices, void* remain_acc, void* next_remain_indices,
                               void* next_remain_acc, void* buckets, uint32_t workers, uint32_t windows,
                               uint32_t window_bits, uint32_t batch_size, cudaStream_t stream) {
@@ -238,13 +242,14 @@ cudaError_t batch_msm_collect(void* remain_indices, void* remain_acc, void* next
     (void)remain_acc;
     (void)next_remain_indices;
     (void)next_remain_acc;
-    (void)buckets;
     (void)workers;
     (void)windows;
     (void)window_bits;
-    (void)batch_size;
-    (void)stream;
-    return cudaGetLastError();
+    ZK_CHECK(cudaGetLastError());  // errors of earlier msm() launches surface here, as in the reference
+    if (batch_size == 0) return cudaSuccess;
+    if (!buckets) return cudaErrorInvalidValue;
+    // buckets: device array of the per-MSM regions msm() parked its window sums in
+    return msm_collect(reinterpret_cast<char* const*>(buckets), batch_size, MSM_NOTE_OFF, stream);
 }
 
 cudaError_t msm(void* res, void* p, void* s, void* indices_buf0, void* indices_buf1, void* indices_buf2,
@@ -265,7 +270,7 @@ cudaError_t msm(void* res, void* p, void* s, void* indices_buf0, void* indices_b
     // scratch the reference host allocates for this call (src/cuda/msm.rs:297-317)
     const size_t words_avail = (size_t)3 * n * (size_t)windows;
     const size_t region_bytes = (((size_t)windows << window_bits) + 2 * (size_t)workers) * sizeof(Jac);
-    const size_t head = 256;  // res[0] (the result) stays clear of the scratch points
+    const size_t head = 256;  // res[0] (the result) and the parked note stay clear of the scratch points
     if (region_bytes <= head) return cudaErrorInvalidValue;
     const size_t pts_avail = (region_bytes - head) / sizeof(Xyzz);
     // preferred window first, then wider and narrower ones until the plan fits
@@ -283,7 +288,9 @@ cudaError_t msm(void* res, void* p, void* s, void* indices_buf0, void* indices_b
             MsmScratch sc;
             Xyzz* pts = reinterpret_cast<Xyzz*>(reinterpret_cast<char*>(res) + head);
             msm_layout_split(pl, reinterpret_cast<uint32_t*>(sort_buf), pts, &sc);
-            return msm_run(reinterpret_cast<Jac*>(res), reinterpret_cast<const Aff*>(p), CF(s), pl, sc, stream);
+            // the final combination runs in batch_msm_collect, for all MSMs at once
+            return msm_run(reinterpret_cast<Jac*>(res), reinterpret_cast<const Aff*>(p), CF(s), pl, sc, stream,
+                           reinterpret_cast<char*>(res) + MSM_NOTE_OFF);
         }
     }
     return cudaErrorInvalidValue;
@@ -368,10 +375,26 @@ cudaError_t zkp_powers(void* out, const void* base, const void* w, uint32_t n, c
     return zk::geometric(F(out), CF(base), CF(w), n, stream);
 }
 
+#ifndef ZK_EXTEND_SECOND_RADIX
+#define ZK_EXTEND_SECOND_RADIX 0  // 0: the general NTT plan's split
+#endif
+
+// passes of the extend phase: the NTT plan, or with ZK_EXTEND_SECOND_RADIX a
+// two-pass split whose second (fused) radix is that value
+static int extend_plan(int log_n, int* rad) {
+    const int np = ntt_plan(log_n, rad);
+    if (ZK_EXTEND_SECOND_RADIX > 0 && np == 2 && log_n - ZK_EXTEND_SECOND_RADIX >= 3 &&
+        log_n - ZK_EXTEND_SECOND_RADIX <= 12) {
+        rad[1] = ZK_EXTEND_SECOND_RADIX;
+        rad[0] = log_n - ZK_EXTEND_SECOND_RADIX;
+    }
+    return np;
+}
+
 // the fused stage applies when the transform takes two passes whose second
 // radix is 2^9..2^11 (two tiles of that radix fit in shared memory)
 static bool extend_fused(int log_n, int* rad) {
-    const int np = ntt_plan(log_n, rad);
+    const int np = extend_plan(log_n, rad);
     return np == 2 && rad[1] >= 9 && rad[1] <= 11;
 }
 
@@ -413,7 +436,7 @@ cudaError_t zkp_extend_batch(void* ext_out, void* coeff_out, const void* lagrang
     const size_t n = (size_t)1 << log_n;
     const uint32_t E = 1u << ext_bits;
     int rad[4];
-    const int np = ntt_plan(log_n, rad);
+    const int np = extend_plan(log_n, rad);
     if (np > 2) return cudaErrorInvalidValue;
     if (coeff_out && extend_fused(log_n, rad)) {
         // 1. first inverse pass: lagrange -> coeff_out (intermediate, transformed in place next)

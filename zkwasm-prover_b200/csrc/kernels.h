@@ -83,8 +83,14 @@ void msm_layout(const MsmPlan& p, void* base, MsmScratch* s);
 void msm_layout_split(const MsmPlan& p, uint32_t* words, Xyzz* points, MsmScratch* s);
 // sum_i [scalars_i] bases_i written as a Jacobian point at out; scalars in
 // Montgomery form; no allocation, no host synchronisation.
+// With park_note set, the final combination is left out: the window sums
+// stay in scratch and a 16-byte note at park_note (which must lie below
+// s.winsum, within 4 GiB) records where; msm_collect finishes such MSMs.
 cudaError_t msm_run(Jac* out, const Aff* bases, const Fr* scalars, const MsmPlan& p, const MsmScratch& s,
-                    cudaStream_t st);
+                    cudaStream_t st, void* park_note = nullptr);
+// final combinations of count parked MSMs: regions[i] + note_off holds the
+// note, the Jacobian result goes to regions[i] (device array of pointers)
+cudaError_t msm_collect(char* const* regions, uint32_t count, uint32_t note_off, cudaStream_t st);
 
 size_t msm_merge_extra(uint32_t nacc);  // merge-level items after the 2 * nacc partials
 // part_key / part_pt hold 2 * nacc + msm_merge_extra(nacc) items

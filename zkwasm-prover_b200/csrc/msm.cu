@@ -56,14 +56,31 @@ __global__ void msm_scatter_kernel(const Fr* __restrict__ scalars, uint32_t n, i
     Fr k = fe_from_mont<FrCfg>(ldg_elem<FrCfg>(scalars + i));
     const uint32_t B = 1u << (c - 1);
     uint32_t carry = 0;
-    for (int w = 0; w < W; w++) {
-        int d = msm_signed_digit(k.v, w, c, carry);
-        if (d != 0) {
-            uint32_t mag = d > 0 ? (uint32_t)d : (uint32_t)(-d);
-            uint32_t key = (uint32_t)w * B + mag - 1;
-            uint32_t slot = atomicSub(&count[key], 1u) - 1u;
-            entries[offset[key] + slot] = i | (d < 0 ? 0x80000000u : 0u);
+    // windows in groups of eight: the digits, then eight independent slot
+    // claims (atomics with a return value) in flight together, then the stores
+    for (int w0 = 0; w0 < W; w0 += 8) {
+        uint32_t key[8], base[8], slot[8];
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+            key[u] = KEY_NONE;
+            if (w0 + u < W) {
+                const int d = msm_signed_digit(k.v, w0 + u, c, carry);
+                if (d != 0) {
+                    const uint32_t mag = d > 0 ? (uint32_t)d : (uint32_t)(-d);
+                    key[u] = ((uint32_t)(w0 + u) * B + mag - 1) | (d < 0 ? 0x80000000u : 0u);
+                }
+            }
         }
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+            if (key[u] != KEY_NONE) {
+                slot[u] = atomicSub(&count[key[u] & 0x7fffffffu], 1u) - 1u;
+                base[u] = offset[key[u] & 0x7fffffffu];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < 8; u++)
+            if (key[u] != KEY_NONE) entries[base[u] + slot[u]] = i | (key[u] & 0x80000000u);
     }
 }
 
@@ -413,10 +430,55 @@ cudaError_t msm_accumulate_merge(const uint32_t* entries, const uint32_t* offset
     return msm_merge(part_key, part_pt, nacc, buckets, st);
 }
 
+// ------------------------------------------------------------ parked finals
+// The reference host runs msm() once per column and then batch_msm_collect
+// over all of them.  msm() can stop after the window sums and leave a note
+// of where they are; batch_msm_collect then runs every MSM's final Horner
+// chain at once, one CTA each, instead of one latency-bound chain per call.
+
+struct MsmParked {
+    uint32_t magic, W, c, winsum_off;  // winsum_off: bytes from the note itself to the window sums
+};
+static constexpr uint32_t PARK_MAGIC = 0x4d534d50u;
+
+__global__ void msm_park_kernel(MsmParked* note, uint32_t W, uint32_t c, uint32_t winsum_off) {
+    note->magic = PARK_MAGIC;
+    note->W = W;
+    note->c = c;
+    note->winsum_off = winsum_off;
+}
+
+// one CTA per region: regions[i] + note_off holds the note, the Jacobian
+// result goes to regions[i][0]
+__global__ void __launch_bounds__(COOP_THREADS) msm_collect_kernel(char* const* regions, uint32_t note_off) {
+    __shared__ Fq buf[8];
+    char* base = regions[blockIdx.x];
+    const MsmParked note = *reinterpret_cast<const MsmParked*>(base + note_off);
+    if (note.magic != PARK_MAGIC) return;  // uniform: no msm() result parked here
+    const Xyzz* win = reinterpret_cast<const Xyzz*>(base + note_off + note.winsum_off);
+    const Jac j = coop_horner(buf, win, (int)note.W, (int)note.c);
+    if (threadIdx.x == 0) {
+        Jac* out = reinterpret_cast<Jac*>(base);
+        st_elem<FqCfg>(&out->x, j.x);
+        st_elem<FqCfg>(&out->y, j.y);
+        st_elem<FqCfg>(&out->z, j.z);
+    }
+}
+
+cudaError_t msm_collect(char* const* regions, uint32_t count, uint32_t note_off, cudaStream_t st) {
+    if (count == 0) return cudaSuccess;
+    msm_collect_kernel<<<count, COOP_THREADS, 0, st>>>(regions, note_off);
+    return cudaGetLastError();
+}
+
 cudaError_t msm_run(Jac* out, const Aff* bases, const Fr* scalars, const MsmPlan& p, const MsmScratch& s,
-                    cudaStream_t st) {
+                    cudaStream_t st, void* park_note) {
     if (p.n == 0) {
         // empty sum: the identity
+        if (park_note) {
+            msm_park_kernel<<<1, 1, 0, st>>>(reinterpret_cast<MsmParked*>(park_note), 0, (uint32_t)p.c, 0);
+            return cudaGetLastError();
+        }
         msm_final_kernel<<<1, COOP_THREADS, 0, st>>>(nullptr, 0, p.c, out);
         return cudaGetLastError();
     }
@@ -443,6 +505,13 @@ cudaError_t msm_run(Jac* out, const Aff* bases, const Fr* scalars, const MsmPlan
     }
     msm_window_kernel<<<p.W, p.G < 256 ? p.G : 256, wsm, st>>>(s.segsum, p.G, s.winsum);
     ZK_CHECK(cudaGetLastError());
+    if (park_note) {
+        const ptrdiff_t off = reinterpret_cast<const char*>(s.winsum) - reinterpret_cast<const char*>(park_note);
+        if (off <= 0 || off > 0xffffffffll) return cudaErrorInvalidValue;
+        msm_park_kernel<<<1, 1, 0, st>>>(reinterpret_cast<MsmParked*>(park_note), (uint32_t)p.W, (uint32_t)p.c,
+                                          (uint32_t)off);
+        return cudaGetLastError();
+    }
     msm_final_kernel<<<1, COOP_THREADS, 0, st>>>(s.winsum, p.W, p.c, out);
     return cudaGetLastError();
 }

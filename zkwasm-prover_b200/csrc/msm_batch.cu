@@ -65,14 +65,32 @@ __global__ void batch_scatter_kernel(const BatchDesc* d, uint32_t count, const F
         const uint32_t j = s - q.sc_off;
         Fr k = fe_from_mont<FrCfg>(ldg_elem<FrCfg>(scalars[i] + j));
         uint32_t carry = 0;
-        for (uint32_t w = 0; w < q.W; w++) {
-            const int dg = msm_signed_digit(k.v, (int)w, (int)q.c, carry);
-            if (dg != 0) {
-                const uint32_t mag = dg > 0 ? (uint32_t)dg : (uint32_t)(-dg);
-                const uint32_t key = q.key_off + w * q.B + mag - 1;
-                const uint32_t slot = atomicSub(&cnt[key], 1u) - 1u;
-                entries[offset[key] + slot] = j | (dg < 0 ? 0x80000000u : 0u);
+        // as msm_scatter_kernel: eight slot claims in flight together
+        for (uint32_t w0 = 0; w0 < q.W; w0 += 8) {
+            uint32_t key[8], neg[8], base[8], slot[8];
+#pragma unroll
+            for (uint32_t u = 0; u < 8; u++) {
+                key[u] = 0xffffffffu;
+                neg[u] = 0;
+                if (w0 + u < q.W) {
+                    const int dg = msm_signed_digit(k.v, (int)(w0 + u), (int)q.c, carry);
+                    if (dg != 0) {
+                        const uint32_t mag = dg > 0 ? (uint32_t)dg : (uint32_t)(-dg);
+                        key[u] = q.key_off + (w0 + u) * q.B + mag - 1;
+                        neg[u] = dg < 0 ? 0x80000000u : 0u;
+                    }
+                }
             }
+#pragma unroll
+            for (uint32_t u = 0; u < 8; u++) {
+                if (key[u] != 0xffffffffu) {
+                    slot[u] = atomicSub(&cnt[key[u]], 1u) - 1u;
+                    base[u] = offset[key[u]];
+                }
+            }
+#pragma unroll
+            for (uint32_t u = 0; u < 8; u++)
+                if (key[u] != 0xffffffffu) entries[base[u] + slot[u]] = j | neg[u];
         }
     }
 }

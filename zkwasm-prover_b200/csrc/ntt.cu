@@ -189,26 +189,33 @@ __device__ __forceinline__ void stage2_last(Fr* x, int lt, const PassOut& po) {
     constexpr int R = 1 << LOGR;
     constexpr int S = R / 2;
     constexpr int TH = R / 8;
-    Fr v[8];
-#pragma unroll
+    // each thread reads and rewrites only its own slots u and u + S, so a
+    // pair is finished before the next is loaded (two elements live at a time)
+#pragma unroll 1
     for (int k = 0; k < 4; k++) {
-        int u = lt + k * TH;
-        v[2 * k] = sm_ld(x, u);
-        v[2 * k + 1] = sm_ld(x, u + S);
-    }
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < 4; k++) {
-        int u = lt + k * TH;
-        dft2(v[2 * k], v[2 * k + 1]);
-        sm_st(x, u, finish_out(po, v[2 * k], (uint32_t)u));
-        sm_st(x, u + S, finish_out(po, v[2 * k + 1], (uint32_t)(u + S)));
+        const int u = lt + k * TH;
+        Fr v0 = sm_ld(x, u), v1 = sm_ld(x, u + S);
+        dft2(v0, v1);
+        sm_st(x, u, finish_out(po, v0, (uint32_t)u));
+        sm_st(x, u + S, finish_out(po, v1, (uint32_t)(u + S)));
     }
     __syncthreads();
 }
 
+#ifndef ZK_PASS10_MIN_BLOCKS
+#define ZK_PASS10_MIN_BLOCKS 4
+#endif
+
+// resident CTAs per SM the register budget of a pass kernel is sized for:
+// 16 warps per SM (128 registers a thread) for most shapes
+__host__ __device__ constexpr int pass_min_blocks(int logr, int g) {
+    return ((g << logr) / 8) >= 512 ? 1
+           : (logr == 10 && g == 1) ? ZK_PASS10_MIN_BLOCKS
+           : ((g << logr) / 8 >= 32 ? 512 / ((g << logr) / 8) : 16);
+}
+
 template <int LOGR, int G>
-__global__ void __launch_bounds__((G << LOGR) / 8, ((G << LOGR) / 8) >= 512 ? 1 : ((G << LOGR) / 8 >= 32 ? 512 / ((G << LOGR) / 8) : 16))
+__global__ void __launch_bounds__((G << LOGR) / 8, pass_min_blocks(LOGR, G))
 ntt_pass_kernel(NttPassArgs a) {
     constexpr int R = 1 << LOGR;
     constexpr int TR = R / 8;  // threads per DFT
@@ -302,8 +309,12 @@ __device__ __forceinline__ void dft_tile(Fr* x, int lt, const Fr* tw, int log_n,
 //       sub[z n + y + R q].
 // The coefficients stay in shared memory across the 2^e cosets, so they are
 // read once instead of 2^e times with a strided pattern.
+// resident CTAs per SM the register budget is sized for: two tiles of 2^LOGR
+// elements in shared memory allow 7 CTAs of 2^9, 3 of 2^10 and 1 of 2^11
+__host__ __device__ constexpr int fused_min_blocks(int logr) { return logr <= 9 ? 7 : logr == 10 ? 3 : 1; }
+
 template <int LOGR>
-__global__ void __launch_bounds__((1 << LOGR) / 8, ((1 << LOGR) / 8) >= 512 ? 1 : 3)
+__global__ void __launch_bounds__((1 << LOGR) / 8, fused_min_blocks(LOGR))
 ntt_fused_extend_kernel(FusedExtendArgs a) {
     constexpr int R = 1 << LOGR;
     constexpr int T = R / 8;

@@ -147,7 +147,10 @@ def batch_msm(points_buf, scalar_bufs, length: int, stream=None):
                         ptr(idx[1]), ptr(idx[2]), ptr(idx[3]), ptr(sort_buf), ptr(acc_idx[i]), length, windows, c,
                         threads, worker, sort_buf.numel() * 4, 1, st)
         abi.check(err, "msm")
-    abi.check(lib().batch_msm_collect(None, None, None, None, None, worker, windows, c, count, st),
+    # device array of the per-MSM region pointers (src/cuda/msm.rs:387-420)
+    regions = torch.tensor([curve_buf.data_ptr() + i * curve_buf_size * 96 for i in range(count)],
+                           dtype=torch.int64, device="cuda")
+    abi.check(lib().batch_msm_collect(None, None, None, None, ptr(regions), worker, windows, c, count, st),
               "batch_msm_collect")
     torch.cuda.synchronize()
     rows = [curve_buf[i * curve_buf_size] for i in range(count)]
