@@ -285,6 +285,38 @@ def run_msm(zkp, device, sizes=(1 << 18, 1 << 22), reps=5):
     return res
 
 
+def run_msm_columns(zkp, device, count=16, log_n=18, reps=3):
+    """count MSMs of 2^log_n points over one base array (columns committed
+    together): the drop-in reference ABI (msm per column, then one
+    batch_msm_collect, with the reference host's window and scratch sizing,
+    src/cuda/msm.rs:239-455) against a loop of zkp_msm calls."""
+    H = zkp.host
+    n = 1 << log_n
+    bases, _ = msm_inputs(zkp, n, 91, device)
+    cols = [random_fr(n, 300 + i, device) for i in range(count)]
+    ref = H.ReferenceMsmBatch(bases, cols, n)
+    scratch = H.msm_scratch(n)
+    out = torch.empty((count, 12), dtype=torch.int64, device=device)
+
+    def loop():
+        for i, c in enumerate(cols):
+            H.msm(bases, c, n=n, scratch=scratch, out=out[i])
+
+    res = {"count": count, "n": n}
+    for name, fn in (("reference_abi", ref.enqueue), ("zkp_msm_loop", loop)):
+        fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(reps):
+            fn()
+        b.record()
+        b.synchronize()
+        res[f"{name}_ms"] = round(a.elapsed_time(b) / reps, 3)
+    res["reference_abi_window_bits"] = ref.c
+    return res
+
+
 def run_msm_batch(zkp, device, count=32, lo=14, hi=20, seed=2024, reps=3):
     """Batched uneven MSMs over one SRS (sizes 2^U, U uniform in [lo, hi];
     per MSM the scalars are uniform (50%), small < 2^20 (35%) or 90%-sparse
@@ -492,6 +524,7 @@ def run_ours(args):
         cpu = cpu_baseline_port(args.log_n, args.ext_bits) if not args.no_cpu_baseline else None
         msm = run_msm(zkp, device) if not args.no_msm else None
         msm_batch = run_msm_batch(zkp, device) if not args.no_msm else None
+        msm_columns = run_msm_columns(zkp, device) if not args.no_msm else None
         out = {
             "metric": f"NTT HBM GB/s: batched iNTT 2^{args.log_n} -> coset NTT 2^{args.log_n + args.ext_bits}, "
                       f"{args.columns} columns",
@@ -532,6 +565,7 @@ def run_ours(args):
             "cpu_baseline": cpu,
             "msm": msm,
             "msm_batch": msm_batch,
+            "msm_columns": msm_columns,
         }
         if clk:
             out["clocks"] = clk
@@ -651,6 +685,44 @@ def reference_gpu_timings(args):
         ok = bool((O.g1_jac_to_aff(curve[0:1].cpu().numpy().view(np.uint64)) == O.msm_known_dlog(d, O.rand_fr(nn, 902))).all())
         res.append({"n": nn, "ms": round(ms, 3), "mpts_per_s": round(nn / ms / 1e3, 2), "window_bits": c,
                     "matches_oracle": ok})
+        if nn == 1 << 18:
+            # 16 columns committed together, as src/cuda/msm.rs:239-455 issues them:
+            # msm per column into its own region, then one batch_msm_collect
+            B = 16
+            c16 = min(4, 3) + 10 + max((nn - 1).bit_length(), 22) - 22  # msm.rs:105 for 16 MSMs
+            w16 = (254 + c16 - 1) // c16
+            bucket16 = w16 << c16
+            region = bucket16 + 2 * worker
+            curves = torch.empty((B * region, 12), dtype=torch.int64, device=dev)
+            single16 = nn * w16
+            idx16 = [torch.empty(single16, dtype=torch.int32, device=dev) for _ in range(4)]
+            sort16 = torch.empty(3 * single16, dtype=torch.int32, device=dev)
+            accs = [torch.empty(2 * worker, dtype=torch.int32, device=dev) for _ in range(B)]
+            cols = [torch.from_numpy(O.rand_fr(nn, 1000 + i).view(np.int64)).to(dev) for i in range(B)]
+            cb = curves.data_ptr()
+            ri16 = ptrs([a.data_ptr() for a in accs])
+            nri16 = ptrs([a.data_ptr() + worker * 4 for a in accs])
+            bk16 = ptrs([cb + i * region * 96 for i in range(B)])
+            ra16 = ptrs([cb + (i * region + bucket16) * 96 for i in range(B)])
+            nra16 = ptrs([cb + (i * region + bucket16 + worker) * 96 for i in range(B)])
+
+            def columns():
+                for i in range(B):
+                    assert L.msm(VP(cb + i * region * 96), p(bases), p(cols[i]), p(idx16[0]), p(idx16[1]),
+                                 p(idx16[2]), p(idx16[3]), p(sort16), p(accs[i]), nn, w16, c16, 64, worker,
+                                 3 * single16 * 4, 1, VP(st)) == 0
+                assert L.batch_msm_collect(p(ri16), p(ra16), p(nri16), p(nra16), p(bk16), worker, w16, c16, B,
+                                           VP(st)) == 0
+
+            columns()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for _ in range(reps):
+                columns()
+            torch.cuda.synchronize()
+            out["msm_columns"] = {"count": B, "n": nn, "window_bits": c16,
+                                  "reference_abi_ms": round((time.perf_counter() - t0) / reps * 1e3, 3)}
+            del curves, idx16, sort16, accs, cols
         del bases, sc, curve, idx, sort, acc
     out["msm"] = res
     return out

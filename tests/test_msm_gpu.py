@@ -173,10 +173,11 @@ def test_msm_batch_many_buckets(O, gpu):
         assert (_jac_to_aff(O, got[i]) == O.msm_known_dlog(d, cols[i])).all(), i
 
 
-def test_reference_abi_batch_msm(O, gpu):
-    # msm() per column + batch_msm_collect, buffers sized like src/cuda/msm.rs
+@pytest.mark.parametrize("n", [1 << 12, 1 << 16])
+def test_reference_abi_batch_msm(O, gpu, n):
+    # msm() per column + batch_msm_collect, buffers sized like src/cuda/msm.rs;
+    # msm() places its scratch in the sort buffer and the region as fits
     H = gpu.host
-    n = 1 << 12
     d = O.rand_fr(n, 81)
     bases = H.to_device(O.g1_gen_bases(d))
     cols = [O.rand_fr(n, 82 + i) for i in range(3)]

@@ -272,7 +272,6 @@ cudaError_t msm(void* res, void* p, void* s, void* indices_buf0, void* indices_b
     const size_t region_bytes = (((size_t)windows << window_bits) + 2 * (size_t)workers) * sizeof(Jac);
     const size_t head = 256;  // res[0] (the result) and the parked note stay clear of the scratch points
     if (region_bytes <= head) return cudaErrorInvalidValue;
-    const size_t pts_avail = (region_bytes - head) / sizeof(Xyzz);
     // preferred window first, then wider and narrower ones until the plan fits
     const int c0 = msm_make_plan(n, 0).c;
     int order[40];
@@ -282,16 +281,18 @@ cudaError_t msm(void* res, void* p, void* s, void* indices_buf0, void* indices_b
         if (c0 + d <= 22) order[no++] = c0 + d;
         if (c0 - d >= 4) order[no++] = c0 - d;
     }
+    // both caller buffers are scratch arenas: the sort buffer (shared by every
+    // msm() call of a batch) and the region after its 256-byte head, which
+    // must hold the window sums that batch_msm_collect reads later
+    void* arena[2] = {sort_buf, reinterpret_cast<char*>(res) + head};
+    const size_t arena_bytes[2] = {words_avail * 4, region_bytes - head};
     for (int i = 0; i < no; i++) {
         MsmPlan pl = msm_make_plan(n, order[i]);
-        if (msm_u32_words(pl) <= words_avail && msm_point_count(pl) <= pts_avail) {
-            MsmScratch sc;
-            Xyzz* pts = reinterpret_cast<Xyzz*>(reinterpret_cast<char*>(res) + head);
-            msm_layout_split(pl, reinterpret_cast<uint32_t*>(sort_buf), pts, &sc);
+        MsmScratch sc = {};
+        if (msm_layout_arenas(pl, arena, arena_bytes, 2, &sc, 1))
             // the final combination runs in batch_msm_collect, for all MSMs at once
             return msm_run(reinterpret_cast<Jac*>(res), reinterpret_cast<const Aff*>(p), CF(s), pl, sc, stream,
                            reinterpret_cast<char*>(res) + MSM_NOTE_OFF);
-        }
     }
     return cudaErrorInvalidValue;
 }

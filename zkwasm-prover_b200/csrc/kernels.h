@@ -81,11 +81,16 @@ size_t msm_point_count(const MsmPlan& p);   // partial points + buckets + segmen
 size_t msm_scratch_bytes(const MsmPlan& p); // one contiguous scratch area (both of the above)
 void msm_layout(const MsmPlan& p, void* base, MsmScratch* s);
 void msm_layout_split(const MsmPlan& p, uint32_t* words, Xyzz* points, MsmScratch* s);
+// places the plan's buffers (largest first, 256-byte aligned) into the first
+// of up to 8 caller arenas with room, the window sums only into arena
+// winsum_arena when that is not negative; false when they do not fit
+bool msm_layout_arenas(const MsmPlan& p, void* const* arena, const size_t* arena_bytes, int n_arenas,
+                       MsmScratch* s, int winsum_arena = -1);
 // sum_i [scalars_i] bases_i written as a Jacobian point at out; scalars in
 // Montgomery form; no allocation, no host synchronisation.
-// With park_note set, the final combination is left out: the window sums
-// stay in scratch and a 16-byte note at park_note (which must lie below
-// s.winsum, within 4 GiB) records where; msm_collect finishes such MSMs.
+// With park_note set (8-byte aligned), the final combination is left out: the
+// window sums stay in scratch and a 24-byte note at park_note records where;
+// msm_collect finishes such MSMs.
 cudaError_t msm_run(Jac* out, const Aff* bases, const Fr* scalars, const MsmPlan& p, const MsmScratch& s,
                     cudaStream_t st, void* park_note = nullptr);
 // final combinations of count parked MSMs: regions[i] + note_off holds the

@@ -414,6 +414,52 @@ void msm_layout_split(const MsmPlan& p, uint32_t* words, Xyzz* points, MsmScratc
     s->winsum = q;
 }
 
+bool msm_layout_arenas(const MsmPlan& p, void* const* arena, const size_t* arena_bytes, int n_arenas,
+                       MsmScratch* s, int winsum_arena) {
+    // the plan's buffers, largest first, each into the first arena with room
+    const size_t parts = (size_t)2 * p.nacc + msm_merge_extra(p.nacc);
+    void** slot[9] = {reinterpret_cast<void**>(&s->count),    reinterpret_cast<void**>(&s->offset),
+                      reinterpret_cast<void**>(&s->scan_tmp), reinterpret_cast<void**>(&s->entries),
+                      reinterpret_cast<void**>(&s->part_key), reinterpret_cast<void**>(&s->part_pt),
+                      reinterpret_cast<void**>(&s->buckets),  reinterpret_cast<void**>(&s->segsum),
+                      reinterpret_cast<void**>(&s->winsum)};
+    size_t bytes[9] = {(size_t)p.NB * 4,
+                       ((size_t)p.NB + 1) * 4,
+                       scan_tmp_words(p.NB) * 4,
+                       (size_t)p.n * p.W * 4,
+                       parts * 4,
+                       parts * sizeof(Xyzz),
+                       (size_t)p.NB * sizeof(Xyzz),
+                       (size_t)p.W * p.G * sizeof(Xyzz),
+                       (size_t)p.W * sizeof(Xyzz)};
+    int order[9];
+    for (int i = 0; i < 9; i++) order[i] = i;
+    for (int i = 1; i < 9; i++)
+        for (int j = i; j > 0 && bytes[order[j]] > bytes[order[j - 1]]; j--) {
+            const int t = order[j];
+            order[j] = order[j - 1];
+            order[j - 1] = t;
+        }
+    size_t used[8] = {};
+    if (n_arenas > 8) n_arenas = 8;
+    for (int k = 0; k < 9; k++) {
+        const int b = order[k];
+        int a = 0;
+        for (; a < n_arenas; a++) {
+            if (b == 8 && winsum_arena >= 0 && a != winsum_arena) continue;
+            const uintptr_t base = reinterpret_cast<uintptr_t>(arena[a]);
+            const size_t start = align_up(base + used[a], 256) - base;
+            if (start + bytes[b] <= arena_bytes[a]) {
+                *slot[b] = reinterpret_cast<char*>(arena[a]) + start;
+                used[a] = start + bytes[b];
+                break;
+            }
+        }
+        if (a == n_arenas) return false;
+    }
+    return true;
+}
+
 void msm_layout(const MsmPlan& p, void* base, MsmScratch* s) {
     uint32_t* words = reinterpret_cast<uint32_t*>(base);
     Xyzz* pts = reinterpret_cast<Xyzz*>(reinterpret_cast<char*>(base) + align_up(msm_u32_words(p) * 4, 256));
@@ -437,15 +483,17 @@ cudaError_t msm_accumulate_merge(const uint32_t* entries, const uint32_t* offset
 // chain at once, one CTA each, instead of one latency-bound chain per call.
 
 struct MsmParked {
-    uint32_t magic, W, c, winsum_off;  // winsum_off: bytes from the note itself to the window sums
+    uint32_t magic, W, c, pad;
+    const Xyzz* winsum;  // device address of the window sums
 };
 static constexpr uint32_t PARK_MAGIC = 0x4d534d50u;
 
-__global__ void msm_park_kernel(MsmParked* note, uint32_t W, uint32_t c, uint32_t winsum_off) {
+__global__ void msm_park_kernel(MsmParked* note, uint32_t W, uint32_t c, const Xyzz* winsum) {
     note->magic = PARK_MAGIC;
     note->W = W;
     note->c = c;
-    note->winsum_off = winsum_off;
+    note->pad = 0;
+    note->winsum = winsum;
 }
 
 // one CTA per region: regions[i] + note_off holds the note, the Jacobian
@@ -455,8 +503,7 @@ __global__ void __launch_bounds__(COOP_THREADS) msm_collect_kernel(char* const* 
     char* base = regions[blockIdx.x];
     const MsmParked note = *reinterpret_cast<const MsmParked*>(base + note_off);
     if (note.magic != PARK_MAGIC) return;  // uniform: no msm() result parked here
-    const Xyzz* win = reinterpret_cast<const Xyzz*>(base + note_off + note.winsum_off);
-    const Jac j = coop_horner(buf, win, (int)note.W, (int)note.c);
+    const Jac j = coop_horner(buf, note.winsum, (int)note.W, (int)note.c);
     if (threadIdx.x == 0) {
         Jac* out = reinterpret_cast<Jac*>(base);
         st_elem<FqCfg>(&out->x, j.x);
@@ -476,7 +523,7 @@ cudaError_t msm_run(Jac* out, const Aff* bases, const Fr* scalars, const MsmPlan
     if (p.n == 0) {
         // empty sum: the identity
         if (park_note) {
-            msm_park_kernel<<<1, 1, 0, st>>>(reinterpret_cast<MsmParked*>(park_note), 0, (uint32_t)p.c, 0);
+            msm_park_kernel<<<1, 1, 0, st>>>(reinterpret_cast<MsmParked*>(park_note), 0, (uint32_t)p.c, nullptr);
             return cudaGetLastError();
         }
         msm_final_kernel<<<1, COOP_THREADS, 0, st>>>(nullptr, 0, p.c, out);
@@ -506,10 +553,8 @@ cudaError_t msm_run(Jac* out, const Aff* bases, const Fr* scalars, const MsmPlan
     msm_window_kernel<<<p.W, p.G < 256 ? p.G : 256, wsm, st>>>(s.segsum, p.G, s.winsum);
     ZK_CHECK(cudaGetLastError());
     if (park_note) {
-        const ptrdiff_t off = reinterpret_cast<const char*>(s.winsum) - reinterpret_cast<const char*>(park_note);
-        if (off <= 0 || off > 0xffffffffll) return cudaErrorInvalidValue;
         msm_park_kernel<<<1, 1, 0, st>>>(reinterpret_cast<MsmParked*>(park_note), (uint32_t)p.W, (uint32_t)p.c,
-                                          (uint32_t)off);
+                                          s.winsum);
         return cudaGetLastError();
     }
     msm_final_kernel<<<1, COOP_THREADS, 0, st>>>(s.winsum, p.W, p.c, out);

@@ -124,37 +124,59 @@ def msm_window_bits(msm_count: int, length: int) -> int:
     return min(log2_ceil(msm_count), 3) + 10 + max(log2_ceil(length), 22) - 22
 
 
+class ReferenceMsmBatch:
+    """The buffers and calls of src/cuda/msm.rs:239-455 through the drop-in
+    msm + batch_msm_collect symbols, with the reference's scratch sizing:
+    one region of (windows << c) + 2 * workers Jacobian points per MSM, a
+    shared sort buffer of 3 * length * windows u32, and the device array of
+    region pointers batch_msm_collect takes."""
+
+    def __init__(self, points_buf, scalar_bufs, length: int, stream=None):
+        threads, bits = 64, 254
+        self.points, self.scalars, self.length = points_buf, list(scalar_bufs), length
+        self.count = count = len(self.scalars)
+        self.c = c = msm_window_bits(count, length)
+        self.windows = windows = (bits + c - 1) // c
+        bucket_size = windows << c
+        max_worker = 128 * 512
+        self.worker = (length + threads - 1) // threads * threads if length < max_worker else max_worker
+        self.threads = threads
+        self.region = bucket_size + self.worker * 2
+        self.curve_buf = torch.empty((count * self.region, 12), dtype=torch.int64, device="cuda")
+        single = length * windows
+        self.sort_buf = torch.empty(max(1, single * 3), dtype=torch.int32, device="cuda")
+        self.idx = [torch.empty(max(1, single), dtype=torch.int32, device="cuda") for _ in range(4)]
+        self.acc_idx = [torch.empty(max(1, self.worker * 2), dtype=torch.int32, device="cuda") for _ in range(count)]
+        # device array of the per-MSM region pointers (src/cuda/msm.rs:387-420)
+        self.regions = torch.tensor([self.curve_buf.data_ptr() + i * self.region * 96 for i in range(count)],
+                                    dtype=torch.int64, device="cuda")
+        self.stream = stream
+
+    def enqueue(self):
+        """msm per column, then batch_msm_collect; no host synchronisation."""
+        st = stream_handle(self.stream)
+        for i, s in enumerate(self.scalars):
+            err = lib().msm(self.curve_buf.data_ptr() + i * self.region * 96, ptr(self.points), ptr(s),
+                            ptr(self.idx[0]), ptr(self.idx[1]), ptr(self.idx[2]), ptr(self.idx[3]),
+                            ptr(self.sort_buf), ptr(self.acc_idx[i]), self.length, self.windows, self.c,
+                            self.threads, self.worker, self.sort_buf.numel() * 4, 1, st)
+            abi.check(err, "msm")
+        abi.check(lib().batch_msm_collect(None, None, None, None, ptr(self.regions), self.worker, self.windows,
+                                          self.c, self.count, st), "batch_msm_collect")
+
+    def results(self):
+        """Jacobian results as a numpy (count, 12) uint64 array (synchronises)."""
+        torch.cuda.synchronize()
+        return to_host(torch.stack([self.curve_buf[i * self.region] for i in range(self.count)]))
+
+
 def batch_msm(points_buf, scalar_bufs, length: int, stream=None):
     """src/cuda/msm.rs:239-455 through the drop-in msm + batch_msm_collect
     symbols, with the reference's scratch sizing.  Returns Jacobian points as a
     numpy (B, 12) uint64 array."""
-    threads, bits = 64, 254
-    count = len(scalar_bufs)
-    c = msm_window_bits(count, length)
-    windows = (bits + c - 1) // c
-    bucket_size = windows << c
-    max_worker = 128 * 512
-    worker = (length + threads - 1) // threads * threads if length < max_worker else max_worker
-    curve_buf_size = bucket_size + worker * 2
-    curve_buf = torch.empty((count * curve_buf_size, 12), dtype=torch.int64, device="cuda")
-    single = length * windows
-    sort_buf = torch.empty(max(1, single * 3), dtype=torch.int32, device="cuda")
-    idx = [torch.empty(max(1, single), dtype=torch.int32, device="cuda") for _ in range(4)]
-    acc_idx = [torch.empty(max(1, worker * 2), dtype=torch.int32, device="cuda") for _ in range(count)]
-    st = stream_handle(stream)
-    for i, s in enumerate(scalar_bufs):
-        err = lib().msm(curve_buf.data_ptr() + i * curve_buf_size * 96, ptr(points_buf), ptr(s), ptr(idx[0]),
-                        ptr(idx[1]), ptr(idx[2]), ptr(idx[3]), ptr(sort_buf), ptr(acc_idx[i]), length, windows, c,
-                        threads, worker, sort_buf.numel() * 4, 1, st)
-        abi.check(err, "msm")
-    # device array of the per-MSM region pointers (src/cuda/msm.rs:387-420)
-    regions = torch.tensor([curve_buf.data_ptr() + i * curve_buf_size * 96 for i in range(count)],
-                           dtype=torch.int64, device="cuda")
-    abi.check(lib().batch_msm_collect(None, None, None, None, ptr(regions), worker, windows, c, count, st),
-              "batch_msm_collect")
-    torch.cuda.synchronize()
-    rows = [curve_buf[i * curve_buf_size] for i in range(count)]
-    return to_host(torch.stack(rows))
+    b = ReferenceMsmBatch(points_buf, scalar_bufs, length, stream)
+    b.enqueue()
+    return b.results()
 
 
 def msm_scratch(n: int, window_bits: int = 0) -> torch.Tensor:
