@@ -93,8 +93,9 @@ def test_ntt_batch_columns(O, gpu, log_n, ncols):
         assert (got[c * n:(c + 1) * n] == O.ntt(a[c * n:(c + 1) * n], log_n)).all()
 
 
+# fused stage radices: 2^18 -> 2^9, 2^19 -> 2^9, 2^20 and 2^21 -> 2^10, 2^22 -> 2^11
 @pytest.mark.parametrize("log_n,ext_bits,ncols", [(4, 3, 2), (10, 3, 3), (13, 3, 2), (16, 2, 2),
-                                                  (18, 3, 2), (19, 2, 1), (20, 3, 1)])
+                                                  (18, 3, 2), (19, 2, 1), (20, 3, 1), (22, 1, 1)])
 def test_extend_batch_matches_coset_ntt(O, gpu, log_n, ext_bits, ncols):
     H = gpu.host
     n = 1 << log_n

@@ -309,9 +309,16 @@ __device__ __forceinline__ void dft_tile(Fr* x, int lt, const Fr* tw, int log_n,
 //       sub[z n + y + R q].
 // The coefficients stay in shared memory across the 2^e cosets, so they are
 // read once instead of 2^e times with a strided pattern.
+#ifndef ZK_FUSED_ONE_TILE
+#define ZK_FUSED_ONE_TILE 1
+#endif
+
 // resident CTAs per SM the register budget is sized for: two tiles of 2^LOGR
-// elements in shared memory allow 7 CTAs of 2^9, 3 of 2^10 and 1 of 2^11
-__host__ __device__ constexpr int fused_min_blocks(int logr) { return logr <= 9 ? 7 : logr == 10 ? 3 : 1; }
+// elements in shared memory allow 7 CTAs of 2^9, 3 of 2^10 and 1 of 2^11; one
+// tile (the coefficients re-read from L2 for each coset) allows 4 of 2^10
+__host__ __device__ constexpr int fused_min_blocks(int logr) {
+    return logr <= 9 ? 7 : logr == 10 ? (ZK_FUSED_ONE_TILE ? 4 : 3) : 1;
+}
 
 template <int LOGR>
 __global__ void __launch_bounds__((1 << LOGR) / 8, fused_min_blocks(LOGR))
@@ -320,7 +327,7 @@ ntt_fused_extend_kernel(FusedExtendArgs a) {
     constexpr int T = R / 8;
     extern __shared__ uint4 smem_u4[];
     Fr* A = reinterpret_cast<Fr*>(smem_u4);
-    Fr* B = A + R;
+    Fr* B = ZK_FUSED_ONE_TILE ? A : A + R;
     const int tid = threadIdx.x;
     const int log_items = a.log_n - LOGR;
     const uint32_t q = blockIdx.x;
@@ -347,7 +354,17 @@ ntt_fused_extend_kernel(FusedExtendArgs a) {
     }
     for (int z = 0; z < a.E; z++) {
         const Fr* S = a.stab + (size_t)z * R;
-        for (int i = tid; i < R; i += T) sm_st(B, i, nt_mul(sm_ld(A, i), ldg_elem<FrCfg>(S + i)));
+        if (ZK_FUSED_ONE_TILE) {
+            // the tile is the workspace: coset 0 twists it in place, later
+            // cosets re-read the coefficients this CTA wrote (L2-resident)
+            __syncthreads();
+            for (int i = tid; i < R; i += T) {
+                const Fr cf = z == 0 ? sm_ld(A, i) : ld_elem<FrCfg>(coeff + q + ((size_t)i << log_items));
+                sm_st(B, i, nt_mul(cf, ldg_elem<FrCfg>(S + i)));
+            }
+        } else {
+            for (int i = tid; i < R; i += T) sm_st(B, i, nt_mul(sm_ld(A, i), ldg_elem<FrCfg>(S + i)));
+        }
         __syncthreads();
         PassOut pf;
         pf.tw = a.tw;
@@ -368,7 +385,7 @@ ntt_fused_extend_kernel(FusedExtendArgs a) {
 template <int LOGR>
 static cudaError_t launch_fused(const FusedExtendArgs& a, unsigned ncols, cudaStream_t s) {
     constexpr int R = 1 << LOGR;
-    const size_t smem = (size_t)2 * R * sizeof(Fr);
+    const size_t smem = (size_t)(ZK_FUSED_ONE_TILE ? 1 : 2) * R * sizeof(Fr);
     static bool attr_set = false;
     if (!attr_set) {
         ZK_CHECK(cudaFuncSetAttribute(ntt_fused_extend_kernel<LOGR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
