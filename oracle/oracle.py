@@ -153,6 +153,45 @@ def omega(log_n: int) -> int:
     return w
 
 
+# GLV endomorphism of G1 (Gallant, Lambert, Vanstone, CRYPTO 2001), used by
+# the library's MSM; the reference has no counterpart (its MSM runs on the
+# full 254-bit scalars), so this restates the published method: beta and
+# lambda are the cube roots of unity mod p and mod r with
+# (beta x, y) = [lambda] (x, y), the short lattice basis comes from the
+# extended Euclidean algorithm on (r, lambda) stopped at sqrt(r), and
+# c_i = floor(k g_i / 2^256) with g1 = round(b2 2^256 / r), g2 = round(-b1 2^256 / r).
+GLV_LAMBDA = 0x30644E72E131A029048B6E193FD84104CC37A73FEC2BC5E9B8CA0B2D36636F23
+GLV_BETA = 0x30644E72E131A0295E6DD9E7E0ACCCB0C28F069FBB966E3DE4BD44E5607CFD48
+
+
+def _glv_basis():
+    import math
+
+    r0, t0, r1, t1 = R_MOD, 0, GLV_LAMBDA, 1
+    seq = [(r0, t0), (r1, t1)]
+    while r1:
+        q = r0 // r1
+        r0, r1 = r1, r0 - q * r1
+        t0, t1 = t1, t0 - q * t1
+        seq.append((r1, t1))
+    i = max(j for j, (rj, _) in enumerate(seq) if rj >= math.isqrt(R_MOD))
+    v1 = (seq[i + 1][0], -seq[i + 1][1])
+    v2 = min([(seq[i][0], -seq[i][1]), (seq[i + 2][0], -seq[i + 2][1])], key=lambda v: v[0] ** 2 + v[1] ** 2)
+    return v1 + v2
+
+
+GLV_A1, GLV_B1, GLV_A2, GLV_B2 = _glv_basis()
+GLV_G1 = ((GLV_B2 << 256) + R_MOD // 2) // R_MOD
+GLV_G2 = ((-GLV_B1 << 256) + R_MOD // 2) // R_MOD
+
+
+def glv_split(k: int):
+    """(k1, k2) with k = k1 + k2 lambda (mod r), |k1|, |k2| < 2^127."""
+    c1 = (k * GLV_G1) >> 256
+    c2 = (k * GLV_G2) >> 256
+    return k - c1 * GLV_A1 - c2 * GLV_A2, -c1 * GLV_B1 - c2 * GLV_B2
+
+
 def delta() -> int:
     """GENERATOR^(2^S), the permutation column-coset generator halo2 uses
     (src/permutation.rs:51, 94)."""

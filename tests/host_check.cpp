@@ -110,3 +110,31 @@ extern "C" int hc_signed_digit(const uint64_t* k, int w, int c, uint32_t* carry)
     memcpy(v, k, 32);
     return msm_signed_digit(v, w, c, *carry);
 }
+
+#include "../zkwasm-prover_b200/csrc/glv.cuh"
+
+// k: canonical scalars (4 x u64); m1, m2: magnitudes; neg: two flags per scalar
+extern "C" void hc_glv_split(const uint64_t* k, uint64_t* m1, uint64_t* m2, int* neg, long n) {
+    for (long i = 0; i < n; i++) {
+        uint32_t kv[8], a[8], b[8];
+        memcpy(kv, k + 4 * i, 32);
+        bool n1, n2;
+        glv_split(kv, a, b, n1, n2);
+        memcpy(m1 + 4 * i, a, 32);
+        memcpy(m2 + 4 * i, b, 32);
+        neg[2 * i] = n1;
+        neg[2 * i + 1] = n2;
+    }
+}
+
+// affine points (8 x u64 each, Montgomery) -> phi(points)
+extern "C" void hc_glv_phi(uint64_t* out, const uint64_t* pts, long n) {
+    for (long i = 0; i < n; i++) {
+        Aff a;
+        memcpy(a.x.v, pts + 8 * i, 32);
+        memcpy(a.y.v, pts + 8 * i + 4, 32);
+        const Aff r = glv_phi(a);
+        memcpy(out + 8 * i, r.x.v, 32);
+        memcpy(out + 8 * i + 4, r.y.v, 32);
+    }
+}

@@ -33,6 +33,8 @@ def hc():
         "hc_xyzz_dbl": [P, P],
         "hc_xyzz_mul_u32": [P, P, ctypes.c_uint32],
         "hc_xyzz_to_jac": [P, P],
+        "hc_glv_split": [P, P, P, P, ctypes.c_long],
+        "hc_glv_phi": [P, P, ctypes.c_long],
     }.items():
         getattr(L, name).argtypes = args
     L.hc_bits_at.argtypes = [P, ctypes.c_uint32, ctypes.c_uint32]
@@ -169,3 +171,28 @@ def test_xyzz_formulas(O, hc):
     j = np.empty(12, np.uint64)
     hc.hc_xyzz_to_jac(_p(j), _p(zero))
     assert O.fq_ints(j[8:])[0] == 0 and O.fq_ints(j[4:8])[0] == 1
+
+
+def test_glv_split_matches_restatement(O, hc):
+    rng = random.Random(17)
+    ks = [0, 1, 2, O.R_MOD - 1, O.R_MOD // 2, O.GLV_LAMBDA, (O.R_MOD - 1) // 3, (1 << 253) - 1]
+    ks += [rng.randrange(O.R_MOD) for _ in range(3000)]
+    k = np.array([[(x >> (64 * j)) & (2 ** 64 - 1) for j in range(4)] for x in ks], np.uint64)
+    m1, m2 = np.zeros_like(k), np.zeros_like(k)
+    neg = np.zeros(2 * len(ks), np.int32)
+    hc.hc_glv_split(_p(k), _p(m1), _p(m2), _p(neg), len(ks))
+    for i, x in enumerate(ks):
+        a = sum(int(m1[i, j]) << (64 * j) for j in range(4)) * (-1 if neg[2 * i] else 1)
+        b = sum(int(m2[i, j]) << (64 * j) for j in range(4)) * (-1 if neg[2 * i + 1] else 1)
+        assert (a, b) == O.glv_split(x)
+        assert (a + b * O.GLV_LAMBDA - x) % O.R_MOD == 0
+        assert abs(a) < 2 ** 127 and abs(b) < 2 ** 127
+
+
+def test_glv_phi_is_lambda_multiple(O, hc):
+    d = O.rand_fr(64, 18)
+    pts = O.g1_gen_bases(d)
+    out = np.zeros_like(pts)
+    hc.hc_glv_phi(_p(out), _p(pts), pts.shape[0])
+    lam = O.fr_vec([x * O.GLV_LAMBDA % O.R_MOD for x in O.fr_ints(d)])
+    assert (out == O.g1_gen_bases(lam)).all()

@@ -61,6 +61,7 @@ struct MsmPlan {
     uint32_t seg;   // buckets per reduction segment
     uint32_t G;     // reduction segments per window
     uint32_t n;
+    int glv;        // 1: scalars split k = k1 + k2 lambda over the bases and their endomorphism images
 };
 
 struct MsmScratch {
@@ -73,9 +74,12 @@ struct MsmScratch {
     Xyzz* buckets;       // NB
     Xyzz* segsum;        // W * G
     Xyzz* winsum;        // W
+    Aff* phi;            // n endomorphism images of the bases (GLV plans), else null
 };
 
-MsmPlan msm_make_plan(uint32_t n, int c);
+MsmPlan msm_make_plan(uint32_t n, int c, bool glv = true);
+// sorted entries (nonzero digits at most) of a plan: n W, or 2 n W with GLV
+inline size_t msm_entry_count(const MsmPlan& p) { return (size_t)p.n * p.W * (p.glv ? 2 : 1); }
 size_t msm_u32_words(const MsmPlan& p);     // count + offset + scan tmp + entries + part keys
 size_t msm_point_count(const MsmPlan& p);   // partial points + buckets + segment and window sums
 size_t msm_scratch_bytes(const MsmPlan& p); // one contiguous scratch area (both of the above)

@@ -22,6 +22,7 @@
 // points msm / batch_msm_collect.
 #include "common.cuh"
 #include "kernels.h"
+#include "glv.cuh"
 #include "msm_common.cuh"
 
 namespace zk {
@@ -32,56 +33,121 @@ static constexpr uint32_t KEY_NONE = 0xffffffffu;
 #define ZK_MSM_REDUCE_THREADS 32768
 #endif
 
-__global__ void msm_count_kernel(const Fr* __restrict__ scalars, uint32_t n, int c, int W,
-                                 uint32_t* __restrict__ count) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    Fr k = fe_from_mont<FrCfg>(ldg_elem<FrCfg>(scalars + i));
+// Lanes of a warp that hit the same bucket key share one atomic: the lowest
+// lane of each group of equal keys adds the group's size.  Skewed digits
+// (narrow top windows, repeated or small scalars) would otherwise serialise
+// thousands of atomics on a handful of addresses.  Whole warps only.
+__device__ __forceinline__ uint32_t key_group(uint32_t key, int& leader, uint32_t& rank) {
+    const uint32_t peers = __match_any_sync(0xffffffffu, key);
+    const uint32_t lane = threadIdx.x & 31;
+    leader = __ffs(peers) - 1;
+    rank = __popc(peers & ((1u << lane) - 1u));
+    return peers;
+}
+
+// histogram of the nonzero signed digits of one scalar magnitude v (whole
+// warps: lanes without a scalar pass zero)
+__device__ __forceinline__ void count_digits(const uint32_t v[8], int c, int W, uint32_t* __restrict__ count) {
     const uint32_t B = 1u << (c - 1);
     uint32_t carry = 0;
     for (int w = 0; w < W; w++) {
-        int d = msm_signed_digit(k.v, w, c, carry);
-        if (d != 0) {
-            uint32_t mag = d > 0 ? (uint32_t)d : (uint32_t)(-d);
-            atomicAdd(&count[(uint32_t)w * B + mag - 1], 1u);
-        }
+        const int d = msm_signed_digit(v, w, c, carry);
+        const uint32_t key = d != 0 ? (uint32_t)w * B + (uint32_t)(d > 0 ? d : -d) - 1 : KEY_NONE;
+        int leader;
+        uint32_t rank;
+        const uint32_t peers = key_group(key, leader, rank);
+        if (key != KEY_NONE && rank == 0) atomicAdd(&count[key], (uint32_t)__popc(peers));
     }
 }
 
-__global__ void msm_scatter_kernel(const Fr* __restrict__ scalars, uint32_t n, int c, int W,
-                                   const uint32_t* __restrict__ offset, uint32_t* __restrict__ count,
-                                   uint32_t* __restrict__ entries) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    Fr k = fe_from_mont<FrCfg>(ldg_elem<FrCfg>(scalars + i));
+// entries (point | sign << 31) of the nonzero digits of one scalar magnitude v
+// whose point is `point`, negated when `neg`.  Windows go in groups of eight:
+// the digits, then eight independent slot claims (atomics with a return
+// value) in flight together, then the stores.
+__device__ __forceinline__ void scatter_digits(const uint32_t v[8], int c, int W, uint32_t point, bool neg,
+                                               const uint32_t* __restrict__ offset, uint32_t* __restrict__ count,
+                                               uint32_t* __restrict__ entries) {
     const uint32_t B = 1u << (c - 1);
+    const uint32_t nbit = neg ? 0x80000000u : 0u;
     uint32_t carry = 0;
-    // windows in groups of eight: the digits, then eight independent slot
-    // claims (atomics with a return value) in flight together, then the stores
     for (int w0 = 0; w0 < W; w0 += 8) {
         uint32_t key[8], base[8], slot[8];
 #pragma unroll
         for (int u = 0; u < 8; u++) {
             key[u] = KEY_NONE;
             if (w0 + u < W) {
-                const int d = msm_signed_digit(k.v, w0 + u, c, carry);
+                const int d = msm_signed_digit(v, w0 + u, c, carry);
                 if (d != 0) {
                     const uint32_t mag = d > 0 ? (uint32_t)d : (uint32_t)(-d);
-                    key[u] = ((uint32_t)(w0 + u) * B + mag - 1) | (d < 0 ? 0x80000000u : 0u);
+                    key[u] = ((uint32_t)(w0 + u) * B + mag - 1) | ((d < 0 ? 0x80000000u : 0u) ^ nbit);
                 }
             }
         }
 #pragma unroll
         for (int u = 0; u < 8; u++) {
-            if (key[u] != KEY_NONE) {
-                slot[u] = atomicSub(&count[key[u] & 0x7fffffffu], 1u) - 1u;
-                base[u] = offset[key[u] & 0x7fffffffu];
+            const uint32_t kk = key[u] == KEY_NONE ? KEY_NONE : key[u] & 0x7fffffffu;
+            int leader;
+            uint32_t rank;
+            const uint32_t peers = key_group(kk, leader, rank);
+            if (kk != KEY_NONE) {
+                uint32_t top = 0;
+                if (rank == 0) top = atomicSub(&count[kk], (uint32_t)__popc(peers));
+                top = __shfl_sync(peers, top, leader);
+                slot[u] = top - 1u - rank;
+                base[u] = offset[kk];
             }
         }
 #pragma unroll
         for (int u = 0; u < 8; u++)
-            if (key[u] != KEY_NONE) entries[base[u] + slot[u]] = i | (key[u] & 0x80000000u);
+            if (key[u] != KEY_NONE) entries[base[u] + slot[u]] = point | (key[u] & 0x80000000u);
     }
+}
+
+// one thread per scalar: Montgomery -> canonical, then the digits of the
+// scalar (GLV = false) or of its two GLV halves |k1| (point i) and |k2|
+// (point n + i, the image of base i under the endomorphism)
+template <bool GLV>
+__global__ void msm_count_kernel(const Fr* __restrict__ scalars, uint32_t n, int c, int W,
+                                 uint32_t* __restrict__ count) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i - (threadIdx.x & 31) >= n) return;  // whole warps past the end
+    const Fr k = i < n ? fe_from_mont<FrCfg>(ldg_elem<FrCfg>(scalars + i)) : fe_zero<FrCfg>();
+    if (GLV) {
+        uint32_t m1[8], m2[8];
+        bool n1, n2;
+        glv_split(k.v, m1, m2, n1, n2);
+        count_digits(m1, c, W, count);
+        count_digits(m2, c, W, count);
+    } else {
+        count_digits(k.v, c, W, count);
+    }
+}
+
+template <bool GLV>
+__global__ void msm_scatter_kernel(const Fr* __restrict__ scalars, uint32_t n, int c, int W,
+                                   const uint32_t* __restrict__ offset, uint32_t* __restrict__ count,
+                                   uint32_t* __restrict__ entries) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i - (threadIdx.x & 31) >= n) return;  // whole warps past the end
+    const Fr k = i < n ? fe_from_mont<FrCfg>(ldg_elem<FrCfg>(scalars + i)) : fe_zero<FrCfg>();
+    if (GLV) {
+        uint32_t m1[8], m2[8];
+        bool n1, n2;
+        glv_split(k.v, m1, m2, n1, n2);
+        scatter_digits(m1, c, W, i, n1, offset, count, entries);
+        scatter_digits(m2, c, W, n + i, n2, offset, count, entries);
+    } else {
+        scatter_digits(k.v, c, W, i, false, offset, count, entries);
+    }
+}
+
+// phi[i] = (beta x_i, y_i), the endomorphism images of the bases
+__global__ void msm_phi_kernel(const Aff* __restrict__ bases, uint32_t n, Aff* __restrict__ phi) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const Aff r = glv_phi(ld_aff(bases + i));
+    st_elem<FqCfg>(&phi[i].x, r.x);
+    st_elem<FqCfg>(&phi[i].y, r.y);
 }
 
 __device__ __forceinline__ void prefetch_l1(const void* p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
@@ -98,9 +164,16 @@ __device__ __forceinline__ uint32_t find_bucket(const uint32_t* off, uint32_t lo
     return lo;
 }
 
+// point idx of the sorted entries: bases[idx] below nbase, else the
+// endomorphism image phi[idx - nbase] (GLV halves)
+__device__ __forceinline__ const Aff* entry_point(const Aff* bases, const Aff* phi, uint32_t nbase, uint32_t idx) {
+    return idx < nbase ? bases + idx : phi + (idx - nbase);
+}
+
 __global__ void __launch_bounds__(128) msm_accumulate_kernel(const uint32_t* __restrict__ entries,
                                                              const uint32_t* __restrict__ offset, uint32_t NB,
-                                                             const Aff* __restrict__ bases, uint32_t L,
+                                                             const Aff* __restrict__ bases,
+                                                             const Aff* __restrict__ phi, uint32_t nbase, uint32_t L,
                                                              uint32_t nacc, Xyzz* __restrict__ buckets,
                                                              uint32_t* __restrict__ part_key,
                                                              Xyzz* __restrict__ part_pt) {
@@ -120,14 +193,14 @@ __global__ void __launch_bounds__(128) msm_accumulate_kernel(const uint32_t* __r
         // the current one is added (a register copy would cost occupancy).
         Xyzz acc = xyzz_identity();
         uint32_t ent_next = entries[s];
-        prefetch_l1(bases + (ent_next & 0x7fffffffu));
+        prefetch_l1(entry_point(bases, phi, nbase, ent_next & 0x7fffffffu));
         for (uint32_t p = s; p < e; p++) {
             const uint32_t ent = ent_next;
             if (p + 1 < e) {
                 ent_next = entries[p + 1];
-                prefetch_l1(bases + (ent_next & 0x7fffffffu));
+                prefetch_l1(entry_point(bases, phi, nbase, ent_next & 0x7fffffffu));
             }
-            Aff a = ld_aff(bases + (ent & 0x7fffffffu));
+            Aff a = ld_aff(entry_point(bases, phi, nbase, ent & 0x7fffffffu));
             if (!aff_is_id(a)) {
                 if (ent >> 31) a.y = fe_neg<FqCfg>(a.y);
                 acc = xyzz_add_aff(acc, a.x, a.y);
@@ -333,14 +406,18 @@ __global__ void __launch_bounds__(COOP_THREADS) msm_final_kernel(const Xyzz* __r
 
 // ------------------------------------------------------------------ planning
 
-static int windows_for(int c) { return (254 + c - 1) / c; }
+// windows of c bits for 254-bit scalars, or for the < 2^127 GLV halves
+static int windows_for(int c, bool glv) { return glv ? (128 + c - 1) / c : (254 + c - 1) / c; }
 
-static int pick_c(uint32_t n) {
+static size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+static int pick_c(uint32_t n, bool glv) {
     int best = 4;
     double best_cost = 1e300;
     for (int c = 4; c <= 20; c++) {
-        const double W = windows_for(c);
-        const double cost = 10.0 * n * W + 28.0 * W * (double)(1u << (c - 1)) + 9.0 * 300.0 * (W - 1) * c;
+        const double W = windows_for(c, glv);
+        const double pts = glv ? 2.0 * n : (double)n;
+        const double cost = 10.0 * pts * W + 28.0 * W * (double)(1u << (c - 1)) + 9.0 * 150.0 * (W - 1) * c;
         if (cost < best_cost) {
             best_cost = cost;
             best = c;
@@ -349,14 +426,15 @@ static int pick_c(uint32_t n) {
     return best;
 }
 
-MsmPlan msm_make_plan(uint32_t n, int c) {
+MsmPlan msm_make_plan(uint32_t n, int c, bool glv) {
     MsmPlan p;
     p.n = n;
-    p.c = (c >= 4 && c <= 22) ? c : pick_c(n);
-    p.W = windows_for(p.c);
+    p.glv = glv ? 1 : 0;
+    p.c = (c >= 4 && c <= 22) ? c : pick_c(n, glv);
+    p.W = windows_for(p.c, glv);
     p.B = 1u << (p.c - 1);
     p.NB = (uint32_t)p.W * p.B;
-    const uint64_t max_entries = (uint64_t)n * p.W;
+    const uint64_t max_entries = msm_entry_count(p);
     const uint64_t target_threads = 148ull * 4 * 128;
     uint64_t L = (max_entries + target_threads - 1) / target_threads;
     if (L < 8) L = 8;
@@ -373,14 +451,12 @@ MsmPlan msm_make_plan(uint32_t n, int c) {
     return p;
 }
 
-static size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
-
 size_t msm_u32_words(const MsmPlan& p) {
     size_t w = 0;
     w += align_up(p.NB, 64);
     w += align_up(p.NB + 1, 64);
     w += align_up(scan_tmp_words(p.NB), 64);
-    w += align_up((size_t)p.n * p.W, 64);
+    w += align_up(msm_entry_count(p), 64);
     w += align_up((size_t)2 * p.nacc + msm_merge_extra(p.nacc), 64);
     return w;
 }
@@ -390,7 +466,8 @@ size_t msm_point_count(const MsmPlan& p) {
 }
 
 size_t msm_scratch_bytes(const MsmPlan& p) {
-    return align_up(msm_u32_words(p) * 4, 256) + msm_point_count(p) * sizeof(Xyzz);
+    return align_up(msm_u32_words(p) * 4, 256) + msm_point_count(p) * sizeof(Xyzz) +
+           (p.glv ? (size_t)p.n * sizeof(Aff) : 0);
 }
 
 void msm_layout_split(const MsmPlan& p, uint32_t* words, Xyzz* points, MsmScratch* s) {
@@ -402,7 +479,7 @@ void msm_layout_split(const MsmPlan& p, uint32_t* words, Xyzz* points, MsmScratc
     s->scan_tmp = w;
     w += align_up(scan_tmp_words(p.NB), 64);
     s->entries = w;
-    w += align_up((size_t)p.n * p.W, 64);
+    w += align_up(msm_entry_count(p), 64);
     s->part_key = w;
     Xyzz* q = points;
     s->part_pt = q;
@@ -412,29 +489,32 @@ void msm_layout_split(const MsmPlan& p, uint32_t* words, Xyzz* points, MsmScratc
     s->segsum = q;
     q += (size_t)p.W * p.G;
     s->winsum = q;
+    q += p.W;
+    s->phi = p.glv ? reinterpret_cast<Aff*>(q) : nullptr;
 }
 
 bool msm_layout_arenas(const MsmPlan& p, void* const* arena, const size_t* arena_bytes, int n_arenas,
                        MsmScratch* s, int winsum_arena) {
     // the plan's buffers, largest first, each into the first arena with room
     const size_t parts = (size_t)2 * p.nacc + msm_merge_extra(p.nacc);
-    void** slot[9] = {reinterpret_cast<void**>(&s->count),    reinterpret_cast<void**>(&s->offset),
-                      reinterpret_cast<void**>(&s->scan_tmp), reinterpret_cast<void**>(&s->entries),
-                      reinterpret_cast<void**>(&s->part_key), reinterpret_cast<void**>(&s->part_pt),
-                      reinterpret_cast<void**>(&s->buckets),  reinterpret_cast<void**>(&s->segsum),
-                      reinterpret_cast<void**>(&s->winsum)};
-    size_t bytes[9] = {(size_t)p.NB * 4,
-                       ((size_t)p.NB + 1) * 4,
-                       scan_tmp_words(p.NB) * 4,
-                       (size_t)p.n * p.W * 4,
-                       parts * 4,
-                       parts * sizeof(Xyzz),
-                       (size_t)p.NB * sizeof(Xyzz),
-                       (size_t)p.W * p.G * sizeof(Xyzz),
-                       (size_t)p.W * sizeof(Xyzz)};
-    int order[9];
-    for (int i = 0; i < 9; i++) order[i] = i;
-    for (int i = 1; i < 9; i++)
+    void** slot[10] = {reinterpret_cast<void**>(&s->count),    reinterpret_cast<void**>(&s->offset),
+                       reinterpret_cast<void**>(&s->scan_tmp), reinterpret_cast<void**>(&s->entries),
+                       reinterpret_cast<void**>(&s->part_key), reinterpret_cast<void**>(&s->part_pt),
+                       reinterpret_cast<void**>(&s->buckets),  reinterpret_cast<void**>(&s->segsum),
+                       reinterpret_cast<void**>(&s->winsum),   reinterpret_cast<void**>(&s->phi)};
+    size_t bytes[10] = {(size_t)p.NB * 4,
+                        ((size_t)p.NB + 1) * 4,
+                        scan_tmp_words(p.NB) * 4,
+                        msm_entry_count(p) * 4,
+                        parts * 4,
+                        parts * sizeof(Xyzz),
+                        (size_t)p.NB * sizeof(Xyzz),
+                        (size_t)p.W * p.G * sizeof(Xyzz),
+                        (size_t)p.W * sizeof(Xyzz),
+                        p.glv ? (size_t)p.n * sizeof(Aff) : 0};
+    int order[10];
+    for (int i = 0; i < 10; i++) order[i] = i;
+    for (int i = 1; i < 10; i++)
         for (int j = i; j > 0 && bytes[order[j]] > bytes[order[j - 1]]; j--) {
             const int t = order[j];
             order[j] = order[j - 1];
@@ -442,7 +522,7 @@ bool msm_layout_arenas(const MsmPlan& p, void* const* arena, const size_t* arena
         }
     size_t used[8] = {};
     if (n_arenas > 8) n_arenas = 8;
-    for (int k = 0; k < 9; k++) {
+    for (int k = 0; k < 10; k++) {
         const int b = order[k];
         int a = 0;
         for (; a < n_arenas; a++) {
@@ -457,6 +537,7 @@ bool msm_layout_arenas(const MsmPlan& p, void* const* arena, const size_t* arena
         }
         if (a == n_arenas) return false;
     }
+    if (!p.glv) s->phi = nullptr;
     return true;
 }
 
@@ -470,7 +551,8 @@ void msm_layout(const MsmPlan& p, void* base, MsmScratch* s) {
 cudaError_t msm_accumulate_merge(const uint32_t* entries, const uint32_t* offset, uint32_t NB, const Aff* bases,
                                  uint32_t L, uint32_t nacc, Xyzz* buckets, uint32_t* part_key, Xyzz* part_pt,
                                  cudaStream_t st) {
-    msm_accumulate_kernel<<<(nacc + 127) / 128, 128, 0, st>>>(entries, offset, NB, bases, L, nacc, buckets, part_key,
+    msm_accumulate_kernel<<<(nacc + 127) / 128, 128, 0, st>>>(entries, offset, NB, bases, nullptr, 0xffffffffu, L,
+                                                              nacc, buckets, part_key,
                                                               part_pt);
     ZK_CHECK(cudaGetLastError());
     return msm_merge(part_key, part_pt, nacc, buckets, st);
@@ -532,12 +614,22 @@ cudaError_t msm_run(Jac* out, const Aff* bases, const Fr* scalars, const MsmPlan
     const uint32_t tb = 256;
     const uint32_t nblk = (p.n + tb - 1) / tb;
     ZK_CHECK(cudaMemsetAsync(s.count, 0, sizeof(uint32_t) * p.NB, st));
-    msm_count_kernel<<<nblk, tb, 0, st>>>(scalars, p.n, p.c, p.W, s.count);
+    if (p.glv)
+        msm_count_kernel<true><<<nblk, tb, 0, st>>>(scalars, p.n, p.c, p.W, s.count);
+    else
+        msm_count_kernel<false><<<nblk, tb, 0, st>>>(scalars, p.n, p.c, p.W, s.count);
     ZK_CHECK(cudaGetLastError());
     ZK_CHECK(scan_u32(s.count, s.offset, p.NB, s.scan_tmp, st));
-    msm_scatter_kernel<<<nblk, tb, 0, st>>>(scalars, p.n, p.c, p.W, s.offset, s.count, s.entries);
+    if (p.glv) {
+        msm_scatter_kernel<true><<<nblk, tb, 0, st>>>(scalars, p.n, p.c, p.W, s.offset, s.count, s.entries);
+        ZK_CHECK(cudaGetLastError());
+        msm_phi_kernel<<<nblk, tb, 0, st>>>(bases, p.n, s.phi);
+    } else {
+        msm_scatter_kernel<false><<<nblk, tb, 0, st>>>(scalars, p.n, p.c, p.W, s.offset, s.count, s.entries);
+    }
     ZK_CHECK(cudaGetLastError());
-    msm_accumulate_kernel<<<(p.nacc + 127) / 128, 128, 0, st>>>(s.entries, s.offset, p.NB, bases, p.L, p.nacc,
+    msm_accumulate_kernel<<<(p.nacc + 127) / 128, 128, 0, st>>>(s.entries, s.offset, p.NB, bases, s.phi,
+                                                                p.glv ? p.n : 0xffffffffu, p.L, p.nacc,
                                                                 s.buckets, s.part_key, s.part_pt);
     ZK_CHECK(cudaGetLastError());
     ZK_CHECK(msm_merge(s.part_key, s.part_pt, p.nacc, s.buckets, st));

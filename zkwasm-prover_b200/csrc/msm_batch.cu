@@ -166,7 +166,7 @@ static bool batch_plan(const uint32_t* n, const int* c, uint32_t count, BatchLay
     L.desc.resize(count);
     uint64_t key = 0, sc = 0, red = 0, win = 0, ent = 0;
     for (uint32_t i = 0; i < count; i++) {
-        const MsmPlan p = msm_make_plan(n[i], c ? c[i] : 0);
+        const MsmPlan p = msm_make_plan(n[i], c ? c[i] : 0, false);  // the batched kernels take whole scalars
         BatchDesc& q = L.desc[i];
         q.n = n[i];
         q.c = (uint32_t)p.c;

@@ -39,7 +39,7 @@ static std::mutex g_static_mu;
 // fixed window and at least 32 sorted entries per accumulation thread, so the
 // scratch of every n <= ZKP_MSM_STATIC_MAX_N fits the array
 static zk::MsmPlan static_plan(uint32_t n) {
-    zk::MsmPlan p = zk::msm_make_plan(n, ZKP_MSM_STATIC_WINDOW);
+    zk::MsmPlan p = zk::msm_make_plan(n, ZKP_MSM_STATIC_WINDOW, false);
     const uint64_t entries = (uint64_t)n * p.W;
     if (p.L < 32) {
         p.L = 32;
