@@ -158,14 +158,15 @@ def test_msm_batch_uneven(O, gpu):
 
 
 def test_msm_batch_many_buckets(O, gpu):
-    # 40 MSMs with 16-bit windows: 40 * 16 * 2^15 = 21M buckets, more than one
-    # pass of the top-level bucket-offset scan (4096 * 4096) covers
+    # 40 MSMs with 17-bit windows over the 127-bit GLV halves: 40 * 8 * 2^16 =
+    # 21M buckets, more than one pass of the top-level bucket-offset scan
+    # (4096 * 4096) covers
     H = gpu.host
     n = 512
     d = O.rand_fr(n, 95)
     bases = H.to_device(O.g1_gen_bases(d))
     cols = [O.rand_fr(n, 200 + i) for i in range(40)]
-    ns, ws = [n] * 40, [16] * 40
+    ns, ws = [n] * 40, [17] * 40
     out = H.msm_batch(bases, [H.to_device(c) for c in cols], ns, ws)
     torch.cuda.synchronize()
     got = H.to_host(out)

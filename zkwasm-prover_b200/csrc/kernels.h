@@ -103,9 +103,12 @@ cudaError_t msm_collect(char* const* regions, uint32_t count, uint32_t note_off,
 
 size_t msm_merge_extra(uint32_t nacc);  // merge-level items after the 2 * nacc partials
 // part_key / part_pt hold 2 * nacc + msm_merge_extra(nacc) items
+// entry points below nbase index bases, the others phi (GLV images)
 cudaError_t msm_accumulate_merge(const uint32_t* entries, const uint32_t* offset, uint32_t NB, const Aff* bases,
-                                 uint32_t L, uint32_t nacc, Xyzz* buckets, uint32_t* part_key, Xyzz* part_pt,
-                                 cudaStream_t st);
+                                 const Aff* phi, uint32_t nbase, uint32_t L, uint32_t nacc, Xyzz* buckets,
+                                 uint32_t* part_key, Xyzz* part_pt, cudaStream_t st);
+// phi[i] = (beta x_i, y_i) for i < n
+cudaError_t msm_phi(const Aff* bases, uint32_t n, Aff* phi, cudaStream_t st);
 
 size_t msm_batch_scratch_bytes(const uint32_t* n, const int* c, uint32_t count);
 cudaError_t msm_batch_run(Jac* out, const Aff* bases, const Fr* const* scalars, const uint32_t* n, const int* c,

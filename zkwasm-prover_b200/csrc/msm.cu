@@ -548,10 +548,16 @@ void msm_layout(const MsmPlan& p, void* base, MsmScratch* s) {
 }
 
 // stages 4 and 5 over any sorted key space (shared by the batched MSM)
+cudaError_t msm_phi(const Aff* bases, uint32_t n, Aff* phi, cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    msm_phi_kernel<<<(n + 255) / 256, 256, 0, st>>>(bases, n, phi);
+    return cudaGetLastError();
+}
+
 cudaError_t msm_accumulate_merge(const uint32_t* entries, const uint32_t* offset, uint32_t NB, const Aff* bases,
-                                 uint32_t L, uint32_t nacc, Xyzz* buckets, uint32_t* part_key, Xyzz* part_pt,
-                                 cudaStream_t st) {
-    msm_accumulate_kernel<<<(nacc + 127) / 128, 128, 0, st>>>(entries, offset, NB, bases, nullptr, 0xffffffffu, L,
+                                 const Aff* phi, uint32_t nbase, uint32_t L, uint32_t nacc, Xyzz* buckets,
+                                 uint32_t* part_key, Xyzz* part_pt, cudaStream_t st) {
+    msm_accumulate_kernel<<<(nacc + 127) / 128, 128, 0, st>>>(entries, offset, NB, bases, phi, nbase, L,
                                                               nacc, buckets, part_key,
                                                               part_pt);
     ZK_CHECK(cudaGetLastError());

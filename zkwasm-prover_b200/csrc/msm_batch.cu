@@ -13,6 +13,7 @@
 
 #include "common.cuh"
 #include "kernels.h"
+#include "glv.cuh"
 #include "msm_common.cuh"
 
 namespace zk {
@@ -40,61 +41,83 @@ __device__ __forceinline__ uint32_t find_desc(const BatchDesc* d, uint32_t count
     return lo;
 }
 
+// Every MSM of the batch runs on GLV halves: scalar j of an MSM becomes
+// |k1| on base j and |k2| on phi(base j), stored at point nmax + j (nmax: the
+// longest MSM's base prefix, whose images are computed once).
+
+__device__ __forceinline__ void batch_count_half(const uint32_t v[8], const BatchDesc& q, uint32_t* cnt) {
+    uint32_t carry = 0;
+    for (uint32_t w = 0; w < q.W; w++) {
+        const int dg = msm_signed_digit(v, (int)w, (int)q.c, carry);
+        if (dg != 0) {
+            const uint32_t mag = dg > 0 ? (uint32_t)dg : (uint32_t)(-dg);
+            atomicAdd(&cnt[q.key_off + w * q.B + mag - 1], 1u);
+        }
+    }
+}
+
 __global__ void batch_count_kernel(const BatchDesc* d, uint32_t count, const Fr* const* scalars, uint32_t total,
                                    uint32_t* cnt) {
     for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < total; s += gridDim.x * blockDim.x) {
         const uint32_t i = find_desc<&BatchDesc::sc_off>(d, count, s);
         const BatchDesc q = d[i];
-        Fr k = fe_from_mont<FrCfg>(ldg_elem<FrCfg>(scalars[i] + (s - q.sc_off)));
-        uint32_t carry = 0;
-        for (uint32_t w = 0; w < q.W; w++) {
-            const int dg = msm_signed_digit(k.v, (int)w, (int)q.c, carry);
-            if (dg != 0) {
-                const uint32_t mag = dg > 0 ? (uint32_t)dg : (uint32_t)(-dg);
-                atomicAdd(&cnt[q.key_off + w * q.B + mag - 1], 1u);
+        const Fr k = fe_from_mont<FrCfg>(ldg_elem<FrCfg>(scalars[i] + (s - q.sc_off)));
+        uint32_t m1[8], m2[8];
+        bool n1, n2;
+        glv_split(k.v, m1, m2, n1, n2);
+        batch_count_half(m1, q, cnt);
+        batch_count_half(m2, q, cnt);
+    }
+}
+
+// as scatter_digits of the single MSM: eight slot claims in flight together
+__device__ __forceinline__ void batch_scatter_half(const uint32_t v[8], const BatchDesc& q, uint32_t point,
+                                                   bool negate, const uint32_t* offset, uint32_t* cnt,
+                                                   uint32_t* entries) {
+    const uint32_t nbit = negate ? 0x80000000u : 0u;
+    uint32_t carry = 0;
+    for (uint32_t w0 = 0; w0 < q.W; w0 += 8) {
+        uint32_t key[8], neg[8], base[8], slot[8];
+#pragma unroll
+        for (uint32_t u = 0; u < 8; u++) {
+            key[u] = 0xffffffffu;
+            neg[u] = 0;
+            if (w0 + u < q.W) {
+                const int dg = msm_signed_digit(v, (int)(w0 + u), (int)q.c, carry);
+                if (dg != 0) {
+                    const uint32_t mag = dg > 0 ? (uint32_t)dg : (uint32_t)(-dg);
+                    key[u] = q.key_off + (w0 + u) * q.B + mag - 1;
+                    neg[u] = (dg < 0 ? 0x80000000u : 0u) ^ nbit;
+                }
             }
         }
+#pragma unroll
+        for (uint32_t u = 0; u < 8; u++) {
+            if (key[u] != 0xffffffffu) {
+                slot[u] = atomicSub(&cnt[key[u]], 1u) - 1u;
+                base[u] = offset[key[u]];
+            }
+        }
+#pragma unroll
+        for (uint32_t u = 0; u < 8; u++)
+            if (key[u] != 0xffffffffu) entries[base[u] + slot[u]] = point | neg[u];
     }
 }
 
 __global__ void batch_scatter_kernel(const BatchDesc* d, uint32_t count, const Fr* const* scalars, uint32_t total,
-                                     const uint32_t* offset, uint32_t* cnt, uint32_t* entries) {
+                                     uint32_t nmax, const uint32_t* offset, uint32_t* cnt, uint32_t* entries) {
     for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < total; s += gridDim.x * blockDim.x) {
         const uint32_t i = find_desc<&BatchDesc::sc_off>(d, count, s);
         const BatchDesc q = d[i];
         const uint32_t j = s - q.sc_off;
-        Fr k = fe_from_mont<FrCfg>(ldg_elem<FrCfg>(scalars[i] + j));
-        uint32_t carry = 0;
-        // as msm_scatter_kernel: eight slot claims in flight together
-        for (uint32_t w0 = 0; w0 < q.W; w0 += 8) {
-            uint32_t key[8], neg[8], base[8], slot[8];
-#pragma unroll
-            for (uint32_t u = 0; u < 8; u++) {
-                key[u] = 0xffffffffu;
-                neg[u] = 0;
-                if (w0 + u < q.W) {
-                    const int dg = msm_signed_digit(k.v, (int)(w0 + u), (int)q.c, carry);
-                    if (dg != 0) {
-                        const uint32_t mag = dg > 0 ? (uint32_t)dg : (uint32_t)(-dg);
-                        key[u] = q.key_off + (w0 + u) * q.B + mag - 1;
-                        neg[u] = dg < 0 ? 0x80000000u : 0u;
-                    }
-                }
-            }
-#pragma unroll
-            for (uint32_t u = 0; u < 8; u++) {
-                if (key[u] != 0xffffffffu) {
-                    slot[u] = atomicSub(&cnt[key[u]], 1u) - 1u;
-                    base[u] = offset[key[u]];
-                }
-            }
-#pragma unroll
-            for (uint32_t u = 0; u < 8; u++)
-                if (key[u] != 0xffffffffu) entries[base[u] + slot[u]] = j | neg[u];
-        }
+        const Fr k = fe_from_mont<FrCfg>(ldg_elem<FrCfg>(scalars[i] + j));
+        uint32_t m1[8], m2[8];
+        bool n1, n2;
+        glv_split(k.v, m1, m2, n1, n2);
+        batch_scatter_half(m1, q, j, n1, offset, cnt, entries);
+        batch_scatter_half(m2, q, nmax + j, n2, offset, cnt, entries);
     }
 }
-
 
 __global__ void __launch_bounds__(128) batch_reduce_kernel(const BatchDesc* d, uint32_t count, uint32_t total,
                                                            const Xyzz* buckets, const uint32_t* offset,
@@ -154,10 +177,10 @@ __global__ void __launch_bounds__(COOP_THREADS) batch_final_kernel(const BatchDe
 
 struct BatchLayout {
     std::vector<BatchDesc> desc;
-    uint32_t NB = 0, total = 0, red_total = 0, win_total = 0, L = 8, nacc = 1, maxG = 1;
+    uint32_t NB = 0, total = 0, red_total = 0, win_total = 0, L = 8, nacc = 1, maxG = 1, nmax = 0;
     uint64_t entries = 0;
     size_t off_desc = 0, off_cnt = 0, off_offset = 0, off_scan = 0, off_entries = 0, off_pkey = 0, off_ppt = 0,
-           off_buckets = 0, off_segsum = 0, off_winsum = 0, bytes = 0;
+           off_buckets = 0, off_segsum = 0, off_winsum = 0, off_phi = 0, bytes = 0;
 };
 
 static size_t al(size_t x) { return (x + 255) / 256 * 256; }
@@ -166,7 +189,7 @@ static bool batch_plan(const uint32_t* n, const int* c, uint32_t count, BatchLay
     L.desc.resize(count);
     uint64_t key = 0, sc = 0, red = 0, win = 0, ent = 0;
     for (uint32_t i = 0; i < count; i++) {
-        const MsmPlan p = msm_make_plan(n[i], c ? c[i] : 0, false);  // the batched kernels take whole scalars
+        const MsmPlan p = msm_make_plan(n[i], c ? c[i] : 0, true);
         BatchDesc& q = L.desc[i];
         q.n = n[i];
         q.c = (uint32_t)p.c;
@@ -182,10 +205,13 @@ static bool batch_plan(const uint32_t* n, const int* c, uint32_t count, BatchLay
         sc += n[i];
         red += (uint64_t)p.W * p.G;
         win += p.W;
-        ent += (uint64_t)n[i] * p.W;
+        ent += msm_entry_count(p);
         if (p.G > L.maxG) L.maxG = p.G;
+        if (n[i] > L.nmax) L.nmax = n[i];
     }
-    if (key >= 0xffffffffull || sc >= 0x7fffffffull || ent >= 0xffffffffull || red >= 0xffffffffull) return false;
+    if (key >= 0xffffffffull || sc >= 0x7fffffffull || ent >= 0xffffffffull || red >= 0xffffffffull ||
+        L.nmax >= 0x40000000u)
+        return false;
     L.NB = (uint32_t)key;
     L.total = (uint32_t)sc;
     L.red_total = (uint32_t)red;
@@ -218,6 +244,8 @@ static bool batch_plan(const uint32_t* n, const int* c, uint32_t count, BatchLay
     o = al(o + (size_t)L.red_total * sizeof(Xyzz));
     L.off_winsum = o;
     o = al(o + (size_t)L.win_total * sizeof(Xyzz));
+    L.off_phi = o;
+    o = al(o + (size_t)L.nmax * sizeof(Aff));
     L.bytes = o;
     return true;
 }
@@ -245,6 +273,7 @@ cudaError_t msm_batch_run(Jac* out, const Aff* bases, const Fr* const* scalars, 
     Xyzz* buckets = reinterpret_cast<Xyzz*>(base + L.off_buckets);
     Xyzz* segsum = reinterpret_cast<Xyzz*>(base + L.off_segsum);
     Xyzz* winsum = reinterpret_cast<Xyzz*>(base + L.off_winsum);
+    Aff* phi = reinterpret_cast<Aff*>(base + L.off_phi);
     // the descriptor table goes up from pageable host memory; the copy is
     // staged before cudaMemcpyAsync returns, so the vector may go away after
     ZK_CHECK(cudaMemcpyAsync(d, L.desc.data(), count * sizeof(BatchDesc), cudaMemcpyHostToDevice, st));
@@ -255,9 +284,10 @@ cudaError_t msm_batch_run(Jac* out, const Aff* bases, const Fr* const* scalars, 
     batch_count_kernel<<<g1, 256, 0, st>>>(d, count, scalars, L.total, cnt);
     ZK_CHECK(cudaGetLastError());
     ZK_CHECK(scan_u32(cnt, offset, L.NB, scan, st));
-    batch_scatter_kernel<<<g1, 256, 0, st>>>(d, count, scalars, L.total, offset, cnt, entries);
+    batch_scatter_kernel<<<g1, 256, 0, st>>>(d, count, scalars, L.total, L.nmax, offset, cnt, entries);
     ZK_CHECK(cudaGetLastError());
-    ZK_CHECK(msm_accumulate_merge(entries, offset, L.NB, bases, L.L, L.nacc, buckets, pkey, ppt, st));
+    ZK_CHECK(msm_phi(bases, L.nmax, phi, st));
+    ZK_CHECK(msm_accumulate_merge(entries, offset, L.NB, bases, phi, L.nmax, L.L, L.nacc, buckets, pkey, ppt, st));
     batch_reduce_kernel<<<(L.red_total + 127) / 128, 128, 0, st>>>(d, count, L.red_total, buckets, offset, segsum);
     ZK_CHECK(cudaGetLastError());
     uint32_t bd = 1;
