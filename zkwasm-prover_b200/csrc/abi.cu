@@ -272,8 +272,11 @@ cudaError_t msm(void* res, void* p, void* s, void* indices_buf0, void* indices_b
     const size_t region_bytes = (((size_t)windows << window_bits) + 2 * (size_t)workers) * sizeof(Jac);
     const size_t head = 256;  // res[0] (the result) and the parked note stay clear of the scratch points
     if (region_bytes <= head) return cudaErrorInvalidValue;
-    // preferred window first, then wider and narrower ones until the plan fits
-    const int c0 = msm_make_plan(n, 0).c;
+    // Whole 254-bit scalars, no GLV split: with the final combinations of all
+    // columns running side by side in batch_msm_collect, halving the final's
+    // doublings gains nothing and the split and the endomorphism images cost.
+    // Preferred window first, then wider and narrower ones until the plan fits.
+    const int c0 = msm_make_plan(n, 0, false).c;
     int order[40];
     int no = 0;
     order[no++] = c0;
@@ -287,7 +290,7 @@ cudaError_t msm(void* res, void* p, void* s, void* indices_buf0, void* indices_b
     void* arena[2] = {sort_buf, reinterpret_cast<char*>(res) + head};
     const size_t arena_bytes[2] = {words_avail * 4, region_bytes - head};
     for (int i = 0; i < no; i++) {
-        MsmPlan pl = msm_make_plan(n, order[i]);
+        MsmPlan pl = msm_make_plan(n, order[i], false);
         MsmScratch sc = {};
         if (msm_layout_arenas(pl, arena, arena_bytes, 2, &sc, 1))
             // the final combination runs in batch_msm_collect, for all MSMs at once
