@@ -357,22 +357,37 @@ static cudaError_t msm_merge(uint32_t* part_key, Xyzz* part_pt, uint32_t nacc, X
     return cudaSuccess;
 }
 
+// Thread t = w G + g sums segment g of window w by running sums; then each
+// group of GS = min(G, 128) consecutive threads (one window) adds its results
+// as a tree, and the group's sum goes to segsum[t / GS], so the window
+// kernel is left with G / GS partial sums per window.
 __global__ void __launch_bounds__(128) msm_reduce_kernel(const Xyzz* __restrict__ buckets,
                                                          const uint32_t* __restrict__ offset, int W, uint32_t B,
                                                          uint32_t seg, uint32_t G, Xyzz* __restrict__ segsum) {
+    __shared__ Xyzz sm[128];
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (uint32_t)W * G) return;
-    const uint32_t w = t / G, g = t % G;
-    const uint32_t lo = g * seg;
-    Xyzz T = xyzz_identity(), S = xyzz_identity();
-    for (uint32_t j = 0; j < seg; j++) {
-        const uint32_t b = lo + seg - 1 - j;
-        const uint32_t key = w * B + b;
-        if (offset[key + 1] != offset[key]) T = xyzz_add(T, ld_xyzz(buckets + key));
-        S = xyzz_add(S, T);
+    Xyzz S = xyzz_identity();
+    if (t < (uint32_t)W * G) {
+        const uint32_t w = t / G, g = t % G;
+        const uint32_t lo = g * seg;
+        Xyzz T = xyzz_identity();
+        for (uint32_t j = 0; j < seg; j++) {
+            const uint32_t b = lo + seg - 1 - j;
+            const uint32_t key = w * B + b;
+            if (offset[key + 1] != offset[key]) T = xyzz_add(T, ld_xyzz(buckets + key));
+            S = xyzz_add(S, T);
+        }
+        if (lo) S = xyzz_add(S, xyzz_mul_u32(T, lo));
     }
-    if (lo) S = xyzz_add(S, xyzz_mul_u32(T, lo));
-    st_xyzz(segsum + t, S);
+    const uint32_t GS = G < 128 ? G : 128;
+    const uint32_t k = threadIdx.x;
+    sm[k] = S;
+    __syncthreads();
+    for (uint32_t h = GS >> 1; h > 0; h >>= 1) {
+        if ((k & (GS - 1)) < h) sm[k] = xyzz_add(sm[k], sm[k + h]);
+        __syncthreads();
+    }
+    if ((k & (GS - 1)) == 0 && t < (uint32_t)W * G) st_xyzz(segsum + t / GS, sm[k]);
 }
 
 // one CTA per window; blockDim (a power of two, <= G) threads first add
@@ -642,13 +657,10 @@ cudaError_t msm_run(Jac* out, const Aff* bases, const Fr* scalars, const MsmPlan
     const uint32_t nred = (uint32_t)p.W * p.G;
     msm_reduce_kernel<<<(nred + 127) / 128, 128, 0, st>>>(s.buckets, s.offset, p.W, p.B, p.seg, p.G, s.segsum);
     ZK_CHECK(cudaGetLastError());
-    const size_t wsm = (size_t)(p.G < 256 ? p.G : 256) * sizeof(Xyzz);
-    static bool attr = false;
-    if (!attr) {
-        ZK_CHECK(cudaFuncSetAttribute(msm_window_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 256 * (int)sizeof(Xyzz)));
-        attr = true;
-    }
-    msm_window_kernel<<<p.W, p.G < 256 ? p.G : 256, wsm, st>>>(s.segsum, p.G, s.winsum);
+    // partial sums per window left by the reduce kernel's group trees
+    const uint32_t parts = p.G < 128 ? 1u : p.G / 128u;
+    const uint32_t wt = parts < 256 ? parts : 256;
+    msm_window_kernel<<<p.W, wt, (size_t)wt * sizeof(Xyzz), st>>>(s.segsum, parts, s.winsum);
     ZK_CHECK(cudaGetLastError());
     if (park_note) {
         msm_park_kernel<<<1, 1, 0, st>>>(reinterpret_cast<MsmParked*>(park_note), (uint32_t)p.W, (uint32_t)p.c,

@@ -119,28 +119,42 @@ __global__ void batch_scatter_kernel(const BatchDesc* d, uint32_t count, const F
     }
 }
 
+// as msm_reduce_kernel, over every MSM's (window, segment) threads; each
+// MSM's threads start on a 128-thread boundary, so a CTA serves one MSM and
+// its group trees (GS = min(G, 128) threads, one window) stay inside the CTA
 __global__ void __launch_bounds__(128) batch_reduce_kernel(const BatchDesc* d, uint32_t count, uint32_t total,
                                                            const Xyzz* buckets, const uint32_t* offset,
                                                            Xyzz* segsum) {
+    __shared__ Xyzz sm[128];
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= total) return;
-    const uint32_t i = find_desc<&BatchDesc::red_off>(d, count, t);
+    const uint32_t i = find_desc<&BatchDesc::red_off>(d, count, blockIdx.x * blockDim.x);
     const BatchDesc q = d[i];
     const uint32_t lt = t - q.red_off;
-    const uint32_t w = lt / q.G, g = lt % q.G;
-    const uint32_t lo = g * q.seg;
-    Xyzz T = xyzz_identity(), S = xyzz_identity();
-    for (uint32_t j = 0; j < q.seg; j++) {
-        const uint32_t key = q.key_off + w * q.B + lo + q.seg - 1 - j;
-        if (offset[key + 1] != offset[key]) T = xyzz_add(T, ld_xyzz(buckets + key));
-        S = xyzz_add(S, T);
+    Xyzz S = xyzz_identity();
+    if (t < total && lt < q.W * q.G) {
+        const uint32_t w = lt / q.G, g = lt % q.G;
+        const uint32_t lo = g * q.seg;
+        Xyzz T = xyzz_identity();
+        for (uint32_t j = 0; j < q.seg; j++) {
+            const uint32_t key = q.key_off + w * q.B + lo + q.seg - 1 - j;
+            if (offset[key + 1] != offset[key]) T = xyzz_add(T, ld_xyzz(buckets + key));
+            S = xyzz_add(S, T);
+        }
+        if (lo) S = xyzz_add(S, xyzz_mul_u32(T, lo));
     }
-    if (lo) S = xyzz_add(S, xyzz_mul_u32(T, lo));
-    st_xyzz(segsum + t, S);
+    const uint32_t GS = q.G < 128 ? q.G : 128;
+    const uint32_t k = threadIdx.x;
+    sm[k] = S;
+    __syncthreads();
+    for (uint32_t h = GS >> 1; h > 0; h >>= 1) {
+        if ((k & (GS - 1)) < h) sm[k] = xyzz_add(sm[k], sm[k + h]);
+        __syncthreads();
+    }
+    if ((k & (GS - 1)) == 0 && t < total && lt < q.W * q.G) st_xyzz(segsum + q.red_off + lt / GS, sm[k]);
 }
 
-// one CTA per (MSM, window); blockDim a power of two: each thread first adds
-// the segment results k, k + blockDim, ... of its window, then a tree
+// one CTA per (MSM, window): adds the window's G / min(G, 128) group sums,
+// each thread a strided subset first, then a tree (blockDim a power of two)
 __global__ void __launch_bounds__(256) batch_window_kernel(const BatchDesc* d, uint32_t count, const Xyzz* segsum, Xyzz* winsum) {
     extern __shared__ uint4 smem_u4[];
     Xyzz* sm = reinterpret_cast<Xyzz*>(smem_u4);
@@ -148,8 +162,9 @@ __global__ void __launch_bounds__(256) batch_window_kernel(const BatchDesc* d, u
     const uint32_t i = find_desc<&BatchDesc::win_off>(d, count, b);
     const BatchDesc q = d[i];
     const uint32_t w = b - q.win_off;
+    const uint32_t parts = q.G < 128 ? 1u : q.G / 128u;
     Xyzz acc = xyzz_identity();
-    for (uint32_t g = k; g < q.G; g += blockDim.x) acc = xyzz_add(acc, ld_xyzz(segsum + q.red_off + w * q.G + g));
+    for (uint32_t g = k; g < parts; g += blockDim.x) acc = xyzz_add(acc, ld_xyzz(segsum + q.red_off + w * parts + g));
     sm[k] = acc;
     __syncthreads();
     for (uint32_t h = blockDim.x >> 1; h > 0; h >>= 1) {
@@ -199,11 +214,13 @@ static bool batch_plan(const uint32_t* n, const int* c, uint32_t count, BatchLay
         q.sc_off = (uint32_t)sc;
         q.G = p.G;
         q.seg = p.seg;
+        red = (red + 127) / 128 * 128;  // each MSM's reduction threads start a CTA
         q.red_off = (uint32_t)red;
         q.win_off = (uint32_t)win;
         key += (uint64_t)p.W * p.B;
         sc += n[i];
         red += (uint64_t)p.W * p.G;
+        red = (red + 127) / 128 * 128;
         win += p.W;
         ent += msm_entry_count(p);
         if (p.G > L.maxG) L.maxG = p.G;
@@ -290,8 +307,9 @@ cudaError_t msm_batch_run(Jac* out, const Aff* bases, const Fr* const* scalars, 
     ZK_CHECK(msm_accumulate_merge(entries, offset, L.NB, bases, phi, L.nmax, L.L, L.nacc, buckets, pkey, ppt, st));
     batch_reduce_kernel<<<(L.red_total + 127) / 128, 128, 0, st>>>(d, count, L.red_total, buckets, offset, segsum);
     ZK_CHECK(cudaGetLastError());
+    const uint32_t max_parts = L.maxG < 128 ? 1u : L.maxG / 128u;
     uint32_t bd = 1;
-    while (bd < L.maxG && bd < 256) bd <<= 1;
+    while (bd < max_parts && bd < 256) bd <<= 1;
     static bool attr = false;
     if (!attr) {
         ZK_CHECK(cudaFuncSetAttribute(batch_window_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
