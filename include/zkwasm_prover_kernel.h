@@ -254,8 +254,10 @@ cudaError_t zkp_extend_batch(void *ext_out, void *coeff_out, const void *lagrang
                              void *scratch, void *stage_events, cudaStream_t stream);
 
 /* out[i] = (accumulate ? out[i] : 0) + 1 / (in[i] + c[0]) (c may be NULL);
- * zero maps to zero. out may alias in. */
-cudaError_t zkp_batch_inverse(void *out, const void *in, const void *c, uint32_t n, int accumulate,
+ * zero maps to zero. out may alias in.  scratch: NULL or
+ * zkp_scan_scratch_elems(n) device elements (not aliasing out or in); with it
+ * the whole array takes one field inversion instead of one per 2048 elements. */
+cudaError_t zkp_batch_inverse(void *out, const void *in, const void *c, uint32_t n, int accumulate, void *scratch,
                               cudaStream_t stream);
 
 /* out[i] = [k64[i]] G as affine points (identity (0, 0) for k = 0), with

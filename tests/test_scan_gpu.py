@@ -12,21 +12,25 @@ import torch
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("n", [1, 5, 2048, 2049, 100000, 1 << 20])
-def test_batch_inverse(O, gpu, n):
+# (1 << 22) + 5: 2049 block products, so the three-phase form recurses twice
+@pytest.mark.parametrize("n", [1, 5, 2048, 2049, 100000, 1 << 20, (1 << 22) + 5])
+@pytest.mark.parametrize("with_scratch", [False, True])
+def test_batch_inverse(O, gpu, n, with_scratch):
     H = gpu.host
     a = O.rand_fr(n, 100 + n)
     if n > 10:
         a[7] = 0
+        a[n - 1] = 0
     c = O.rand_fr(1, 3)
     out = H.empty_fr(n)
-    H.batch_inverse(out, H.to_device(a), H.to_device(c))
+    scratch = H.scan_scratch(n) if with_scratch else None
+    H.batch_inverse(out, H.to_device(a), H.to_device(c), scratch=scratch)
     torch.cuda.synchronize()
     exp = O.inv(O.add(a, c))
     assert (H.to_host(out) == exp).all()
     # plain inverse with zero -> zero, in place
     d = H.to_device(a)
-    H.batch_inverse(d, d)
+    H.batch_inverse(d, d, scratch=scratch)
     torch.cuda.synchronize()
     assert (H.to_host(d) == O.batch_inv(a)).all()
 

@@ -59,7 +59,7 @@ SIGNATURES = {
     "zkp_coset_table_elems": ([I, I], SZ),
     "zkp_coset_twist_tables": [P, P, P, I, I, P, S],
     "zkp_extend_batch": [P, P, P, U, I, I, P, P, P, P, P, P, S],
-    "zkp_batch_inverse": [P, P, P, U, I, S],
+    "zkp_batch_inverse": [P, P, P, U, I, P, S],
     "zkp_scan_scratch_elems": ([U], SZ),
     "zkp_g1_multiples": [P, P, U, S],
     "zkp_fr_to_mont": [P, P, U, S],

@@ -162,9 +162,11 @@ cudaError_t logup_eval_h_z_set(void* res, void* set, void* l0, void* l_last, voi
 
 cudaError_t logup_sum_input_inv(void* sum, void* input, void* temp, void* beta, int init, int n,
                                 cudaStream_t stream) {
-    (void)temp;
     if (n < 0) return cudaErrorInvalidValue;
-    return zk::batch_inverse(F(sum), CF(input), CF(beta), (uint32_t)n, init != 0, stream);
+    // temp: the host's n-element buffer (src/lib.rs:596), scratch of the
+    // three-phase inversion
+    return zk::batch_inverse(F(sum), CF(input), CF(beta), (uint32_t)n, init != 0, F(temp), temp ? (size_t)n : 0,
+                             stream);
 }
 
 cudaError_t logup_eval_h_inputs_product_sum(void* product, void* product_sum, void* sets, int n_set, int n,
@@ -214,7 +216,7 @@ cudaError_t shplonk_h_x_merge(void* res, void* v, void* values, void* omegas, vo
 
 cudaError_t shplonk_h_x_div_points(void* values, void* omegas, void* points, int points_n, int n) {
     if (n < 0) return cudaErrorInvalidValue;
-    return zk::div_by_point_diffs(F(values), CF(omegas), CF(points), points_n, (uint32_t)n, 0);
+    return zk::div_by_point_diffs(F(values), CF(omegas), CF(points), points_n, (uint32_t)n, nullptr, 0, 0);
 }
 
 cudaError_t eval_logup_z_compose(void* z, void* input, void* table, void* multiplicity, void* beta, void* last_z,
@@ -568,10 +570,11 @@ cudaError_t zkp_extend_batch(void* ext_out, void* coeff_out, const void* lagrang
     return cudaGetLastError();
 }
 
-cudaError_t zkp_batch_inverse(void* out, const void* in, const void* c, uint32_t n, int accumulate,
+cudaError_t zkp_batch_inverse(void* out, const void* in, const void* c, uint32_t n, int accumulate, void* scratch,
                               cudaStream_t stream) {
     if (n && (!out || !in)) return cudaErrorInvalidValue;
-    return zk::batch_inverse(F(out), CF(in), CF(c), n, accumulate, stream);
+    return zk::batch_inverse(F(out), CF(in), CF(c), n, accumulate, F(scratch), scratch ? fr_scan_tmp_elems(n) : 0,
+                             stream);
 }
 
 size_t zkp_scan_scratch_elems(uint32_t n) { return fr_scan_tmp_elems(n); }

@@ -156,8 +156,13 @@ cudaError_t shplonk_h_x_merge(Fr* res, const Fr* v, const Fr* values, const Fr* 
 
 
 // ------------------------------------------------------------------ Fr scans
-cudaError_t batch_inverse(Fr* out, const Fr* in, const Fr* c, uint32_t n, int accumulate, cudaStream_t s);
-cudaError_t div_by_point_diffs(Fr* values, const Fr* omegas, const Fr* points, int np, uint32_t n, cudaStream_t s);
+// scratch (may be null) of at least batch_inv_scratch_elems(n) elements
+// selects the three-phase form with a single field inversion
+size_t batch_inv_scratch_elems(uint32_t n);
+cudaError_t batch_inverse(Fr* out, const Fr* in, const Fr* c, uint32_t n, int accumulate, Fr* scratch,
+                          size_t scratch_elems, cudaStream_t s);
+cudaError_t div_by_point_diffs(Fr* values, const Fr* omegas, const Fr* points, int np, uint32_t n, Fr* scratch,
+                               size_t scratch_elems, cudaStream_t s);
 size_t fr_scan_tmp_elems(uint32_t n);
 cudaError_t fr_scan_excl(Fr* out, const Fr* in, uint32_t n, const Fr* init, int op, Fr* tmp, cudaStream_t s);
 cudaError_t logup_z_scan(Fr* z, Fr* last_z, int last_index, uint32_t n, Fr* tmp, cudaStream_t s);

@@ -107,8 +107,32 @@ struct DstScale {  // out[i] *= inv
     }
 };
 
+// product of each block's SBLK elements (zeros count as one), for the
+// three-phase form below
+template <class Src>
+__global__ void __launch_bounds__(ST) batch_prod_kernel(Src src, uint32_t n, Fr* tot) {
+    __shared__ Fr wsm[32];
+    const size_t base = (size_t)blockIdx.x * SBLK;
+    const int t = threadIdx.x;
+    const Fr one = fe_one<FrCfg>();
+    Fr run = one;
+#pragma unroll
+    for (int k = 0; k < SK; k++) {
+        const size_t i = base + t + (size_t)ST * k;
+        if (i < n) {
+            Fr a = src((uint32_t)i);
+            if (!fe_is_zero<FrCfg>(a)) run = fe_mul<FrCfg>(run, a);
+        }
+    }
+    Fr total;
+    block_excl_scan_fr(OP_MUL, run, wsm, total);
+    if (t == 0) st_elem<FrCfg>(tot + blockIdx.x, total);
+}
+
+// inv_tots: the inverses of the block products (three-phase form), or null
+// to invert each block's product in the block (one Fermat inversion per block)
 template <class Src, class Dst>
-__global__ void __launch_bounds__(ST) batch_inv_kernel(Src src, Dst dst, uint32_t n) {
+__global__ void __launch_bounds__(ST) batch_inv_kernel(Src src, Dst dst, uint32_t n, const Fr* inv_tots) {
     __shared__ Fr wsm[32];
     __shared__ Fr rev[ST];
     __shared__ Fr inv_tot;
@@ -139,7 +163,7 @@ __global__ void __launch_bounds__(ST) batch_inv_kernel(Src src, Dst dst, uint32_
     rev[ST - 1 - t] = Srev;
     __syncthreads();
     Fr S = rev[t];
-    if (t == 0) inv_tot = fe_inv<FrCfg>(tot);
+    if (t == 0) inv_tot = inv_tots ? ld_elem<FrCfg>(inv_tots + blockIdx.x) : fe_inv<FrCfg>(tot);
     __syncthreads();
     Fr cur = fe_mul<FrCfg>(fe_mul<FrCfg>(inv_tot, S), E);
 #pragma unroll
@@ -158,22 +182,47 @@ __global__ void __launch_bounds__(ST) batch_inv_kernel(Src src, Dst dst, uint32_
     }
 }
 
+// Scratch elements of the three-phase form for n elements: the block
+// products and their inverses, then the same for the blocks of those.
+size_t batch_inv_scratch_elems(uint32_t n) {
+    const uint32_t nb = (n + SBLK - 1) / SBLK;
+    return nb <= 1 ? 0 : 2 * (size_t)nb + batch_inv_scratch_elems(nb);
+}
+
+// With scratch of batch_inv_scratch_elems(n): (1) block products, (2) their
+// inverses by the same routine (recursively, one field inversion at the top),
+// (3) every block unwound with its product's inverse.  A single field
+// inversion is a long dependent chain on one thread, so one per 2048 elements
+// stalls every block on it; three phases leave one (or a few) in all.
+// Without scratch, each block inverts its own product.
 template <class Src, class Dst>
-static cudaError_t launch_batch_inv(Src src, Dst dst, uint32_t n, cudaStream_t s) {
+static cudaError_t launch_batch_inv(Src src, Dst dst, uint32_t n, Fr* scratch, size_t scratch_elems, cudaStream_t s) {
     if (n == 0) return cudaSuccess;
     const uint32_t nb = (n + SBLK - 1) / SBLK;
-    batch_inv_kernel<Src, Dst><<<nb, ST, 0, s>>>(src, dst, n);
+    if (nb > 1 && scratch && scratch_elems >= batch_inv_scratch_elems(n)) {
+        Fr* tot = scratch;
+        Fr* inv = scratch + nb;
+        batch_prod_kernel<Src><<<nb, ST, 0, s>>>(src, n, tot);
+        ZK_CHECK(cudaGetLastError());
+        ZK_CHECK(launch_batch_inv(SrcPlus{tot, nullptr}, DstStore{inv, 0}, nb, scratch + 2 * (size_t)nb,
+                                  scratch_elems - 2 * (size_t)nb, s));
+        batch_inv_kernel<Src, Dst><<<nb, ST, 0, s>>>(src, dst, n, inv);
+        return cudaGetLastError();
+    }
+    batch_inv_kernel<Src, Dst><<<nb, ST, 0, s>>>(src, dst, n, nullptr);
     return cudaGetLastError();
 }
 
-cudaError_t batch_inverse(Fr* out, const Fr* in, const Fr* c, uint32_t n, int accumulate, cudaStream_t s) {
-    return launch_batch_inv(SrcPlus{in, c}, DstStore{out, accumulate}, n, s);
+cudaError_t batch_inverse(Fr* out, const Fr* in, const Fr* c, uint32_t n, int accumulate, Fr* scratch,
+                          size_t scratch_elems, cudaStream_t s) {
+    return launch_batch_inv(SrcPlus{in, c}, DstStore{out, accumulate}, n, scratch, scratch_elems, s);
 }
 
 // values[i] /= prod_j (omegas[i] - points[j])
-cudaError_t div_by_point_diffs(Fr* values, const Fr* omegas, const Fr* points, int np, uint32_t n, cudaStream_t s) {
+cudaError_t div_by_point_diffs(Fr* values, const Fr* omegas, const Fr* points, int np, uint32_t n, Fr* scratch,
+                               size_t scratch_elems, cudaStream_t s) {
     if (np <= 0) return cudaSuccess;
-    return launch_batch_inv(SrcPointDiff{omegas, points, np}, DstScale{values}, n, s);
+    return launch_batch_inv(SrcPointDiff{omegas, points, np}, DstScale{values}, n, scratch, scratch_elems, s);
 }
 
 // ------------------------------------------------------------ exclusive scan
@@ -230,6 +279,8 @@ __global__ void __launch_bounds__(ST) scan_small_kernel(Fr* x, uint32_t m, int o
         if (base + k < m) st_elem<FrCfg>(x + base + k, op_apply(op, e, v[k]));
 }
 
+// scratch of the scans, also enough for the three-phase batch inversion
+// (the callers below use it for both, one after the other)
 size_t fr_scan_tmp_elems(uint32_t n) {
     size_t t = 0;
     uint32_t m = n;
@@ -237,7 +288,8 @@ size_t fr_scan_tmp_elems(uint32_t n) {
         m = (m + SBLK - 1) / SBLK;
         t += m;
     }
-    return t + 1;
+    const size_t inv = batch_inv_scratch_elems(n);
+    return (t + 1 > inv ? t + 1 : inv);
 }
 
 // out[i] = init op x_0 op ... op x_{i-1}; out may alias in
@@ -280,7 +332,10 @@ cudaError_t logup_z_scan(Fr* z, Fr* last_z, int last_index, uint32_t n, Fr* tmp,
 
 cudaError_t logup_z_compose(Fr* z, const Fr* sum, const Fr* table, const Fr* m, const Fr* beta, Fr* last_z,
                             int last_index, uint32_t n, Fr* tmp, cudaStream_t s) {
-    ZK_CHECK(batch_inverse(z, table, beta, n, 0, s));
+    // tmp may be the table itself (the reference-ABI entry reuses it once the
+    // inverses are taken); then the inversion runs without scratch
+    Fr* inv_scratch = tmp == table ? nullptr : tmp;
+    ZK_CHECK(batch_inverse(z, table, beta, n, 0, inv_scratch, fr_scan_tmp_elems(n), s));
     unsigned nb = (n + 255) / 256;
     if (nb > 148 * 32) nb = 148 * 32;
     logup_step2_kernel<<<nb, 256, 0, s>>>(z, sum, m, n);
@@ -336,7 +391,7 @@ cudaError_t permutation_chunk_z(Fr* z, const Fr* const* cols, const Fr* const* s
                                 Fr* tmp, cudaStream_t s) {
     perm_den_kernel<<<grid_n(n), 256, 0, s>>>(z, cols, sig, ncols, beta, gamma, n);
     ZK_CHECK(cudaGetLastError());
-    ZK_CHECK(batch_inverse(z, z, nullptr, n, 0, s));
+    ZK_CHECK(batch_inverse(z, z, nullptr, n, 0, tmp, fr_scan_tmp_elems(n), s));
     perm_num_kernel<<<grid_n(n), 256, 0, s>>>(z, cols, dbeta, ncols, gamma, omegas, n);
     ZK_CHECK(cudaGetLastError());
     return fr_scan_excl(z, z, n, init, OP_MUL, tmp, s);
@@ -366,7 +421,7 @@ cudaError_t shuffle_z(Fr* z, const Fr* const* inputs, const Fr* const* tables, c
                       uint32_t n, Fr* num_tmp, Fr* tmp, cudaStream_t s) {
     shuffle_terms_kernel<<<grid_n(n), 256, 0, s>>>(z, num_tmp, inputs, tables, betas, groups, n);
     ZK_CHECK(cudaGetLastError());
-    ZK_CHECK(batch_inverse(z, z, nullptr, n, 0, s));
+    ZK_CHECK(batch_inverse(z, z, nullptr, n, 0, tmp, fr_scan_tmp_elems(n), s));
     mul_inplace_kernel<<<grid_n(n), 256, 0, s>>>(z, num_tmp, n);
     ZK_CHECK(cudaGetLastError());
     return fr_scan_excl(z, z, n, nullptr, OP_MUL, tmp, s);

@@ -255,8 +255,10 @@ def scan_scratch(n: int) -> torch.Tensor:
     return empty_fr(max(1, lib().zkp_scan_scratch_elems(n)))
 
 
-def batch_inverse(out, inp, c=None, accumulate=False, stream=None):
-    abi.check(lib().zkp_batch_inverse(ptr(out), ptr(inp), ptr(c), inp.shape[0], int(accumulate),
+def batch_inverse(out, inp, c=None, accumulate=False, scratch=None, stream=None):
+    """out = (accumulate ? out : 0) + 1 / (inp + c); scratch from scan_scratch(n)
+    (or None for one field inversion per 2048 elements)."""
+    abi.check(lib().zkp_batch_inverse(ptr(out), ptr(inp), ptr(c), inp.shape[0], int(accumulate), ptr(scratch),
                                       stream_handle(stream)), "zkp_batch_inverse")
 
 
