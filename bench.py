@@ -285,97 +285,122 @@ def run_msm(zkp, device, sizes=(1 << 18, 1 << 22), reps=5):
     return res
 
 
-def run_rows(zkp, device, mont_rate, peak_hbm, log_n=22, log_ext=24, reps=3):
+def run_rows(lib, device, mont_rate, peak_hbm, ours=True, log_n=22, log_ext=24, reps=3):
     """One timed kernel for each remaining hot-path row at the k = 22 column
     size (scans, inversions, grand products: n = 2^22) and its extended domain
     (quotient kernels: N = 2^24), device-resident inputs, CUDA events.  Each
     line gives the algorithmic bytes (the kernel's input and output columns)
     and Fr products (its formula, per row), the two resulting time bounds
     (bytes / measured HBM copy rate, products / measured Montgomery-product
-    rate), which one binds, and the fraction of that bound reached."""
-    L = zkp.load_library()
-    H = zkp.host
+    rate), which one binds, and the fraction of that bound reached.
+
+    The rows named by a reference C symbol run through that symbol, so the
+    same call times this library (ours=True, lib = its ctypes handle) or the
+    reference's kernels rebuilt for sm_100a (ours=False, lib = the oracle/_ref
+    handle, only the reference-symbol rows); the zkp_* rows are this library's
+    batched entry points."""
+    import ctypes
+
     st = torch.cuda.current_stream().cuda_stream
     n, N = 1 << log_n, 1 << log_ext
-    P = lambda t: 0 if t is None else t.data_ptr()
-    cols = [random_fr(N, 700 + i, device) for i in range(8)]
-    small = [random_fr(n, 800 + i, device) for i in range(8)]
-    one = random_fr(1, 901, device)
-    y, beta, gamma = random_fr(1, 902, device), random_fr(1, 903, device), random_fr(1, 904, device)
-    res = random_fr(N, 905, device)
-    out_n = torch.empty_like(small[0])
-    scratch = H.scan_scratch(n)
-    scratch2 = torch.empty((n + L.zkp_scan_scratch_elems(n), 4), dtype=torch.int64, device=device)
-    omega_n = torch.zeros((n, 4), dtype=torch.int64, device=device)
-    omega_n[:2] = random_fr(2, 906, device)
-    omega_N = torch.zeros((N, 4), dtype=torch.int64, device=device)
-    omega_N[:2] = random_fr(2, 907, device)
-    coset = random_fr(3, 908, device)
-    ext = torch.empty((N, 4), dtype=torch.int64, device=device)
-    keep = []
-
-    def arr(ts):
-        t = H.ptr_array(ts)
-        keep.append(t)
-        return t
-
-    def check(e):
-        zkp.abi.check(e, "row kernel")
-
-    # field_op_batch_mul_sum: c0 a b + c1 d + c2 e f g (src/eval_h.rs term lists)
-    v = [P(one), P(cols[0]), P(cols[1]), 0, P(one), P(cols[2]), 0, P(one), P(cols[3]), P(cols[4]), P(cols[5]), 0]
-    rot = [0, 1, -1, 2, 0, -2]
-    vd = torch.tensor(v, dtype=torch.int64, device=device)
-    rd = torch.tensor(rot, dtype=torch.int32, device=device)
-    sets4, ins2, tabs2 = arr(cols[:4]), arr(small[:2]), arr(small[2:4])
-    pc, ps = arr(small[:4]), arr(small[4:8])
-    betas2 = random_fr(2, 909, device)
-    betas4 = random_fr(4, 910, device)
-    xt = random_fr(log_n, 911, device)
     E = 32
+
+    def fr(k, seed):
+        return random_fr(k, seed, device)
+
+    cols = [fr(N, 700 + i) for i in range(8)]
+    small = [fr(n, 800 + i) for i in range(8)]
+    one, y, beta, gamma = fr(1, 901), fr(1, 902), fr(1, 903), fr(1, 904)
+    res = fr(N, 905)
+    out_n, tmp_n, z_n = torch.empty_like(small[0]), torch.empty_like(small[0]), torch.empty_like(small[0])
+    last = fr(1, 912)
+    omega_n = torch.zeros((n, 4), dtype=torch.int64, device=device)
+    omega_n[:2] = fr(2, 906)
+    omega_N = torch.zeros((N, 4), dtype=torch.int64, device=device)
+    omega_N[:2] = fr(2, 907)
+    coset = fr(3, 908)
+    ext = torch.empty((N, 4), dtype=torch.int64, device=device)
+    ptrs = lambda ts: torch.tensor([t.data_ptr() for t in ts], dtype=torch.int64, device=device)
+    # field_op_batch_mul_sum: c0 a b + c1 d + c2 e f g (src/eval_h.rs term lists)
+    vd = torch.tensor([one.data_ptr(), cols[0].data_ptr(), cols[1].data_ptr(), 0, one.data_ptr(),
+                       cols[2].data_ptr(), 0, one.data_ptr(), cols[3].data_ptr(), cols[4].data_ptr(),
+                       cols[5].data_ptr(), 0], dtype=torch.int64, device=device)
+    rd = torch.tensor([0, 1, -1, 2, 0, -2], dtype=torch.int32, device=device)
+    sets4, ins2, tabs2 = ptrs(cols[:4]), ptrs(small[:2]), ptrs(small[2:4])
+    pc, ps = ptrs(small[:4]), ptrs(small[4:8])
+    betas2, betas4, xt = fr(2, 909), fr(4, 910), fr(log_n, 911)
+    P, I, S = "p", "i", "s"
+    # (label, algorithmic bytes, Fr products, symbol, args, reference symbol?)
     cases = [
-        ("a7 expand_omega_buffer (w^i, 2^24)", N * E, N,
-         lambda: check(L.expand_omega_buffer(P(omega_N), log_ext, 0))),
-        ("a8 extended_prepare (zeta coset + zero pad, 2^22 -> 2^24)", (n + N) * E, n,
-         lambda: check(L.extended_prepare(P(ext), P(coset), 3, n, N, 0, st))),
-        ("a9 zkp_batch_inverse (2^22)", 2 * n * E, 3 * n,
-         lambda: check(L.zkp_batch_inverse(P(out_n), P(small[0]), 0, n, 0, P(scratch), st))),
-        ("a10 zkp_grand_sum (logup z prefix sum, 2^22)", 2 * n * E, 0,
-         lambda: check(L.zkp_grand_sum(P(out_n), P(small[1]), n, 0, P(scratch), st))),
-        ("a11 zkp_permutation_z (4 columns, 2^22)", (2 * 4 + 2) * n * E, (4 * 4 + 6) * n,
-         lambda: check(L.zkp_permutation_z(P(out_n), P(pc), P(ps), 4, P(beta), P(gamma), P(betas4), P(omega_n),
-                                           P(one), n, P(scratch), st))),
-        ("a12 zkp_shuffle_z (2 groups, 2^22)", (2 * 2 + 1) * n * E, (2 * 2 + 6) * n,
-         lambda: check(L.zkp_shuffle_z(P(out_n), P(ins2), P(tabs2), P(betas2), 2, n, P(scratch2), st))),
-        ("a13 field_op_batch_mul_sum (3 terms, 6 columns, 2^24)", 8 * N * E, 6 * N,
-         lambda: check(L.field_op_batch_mul_sum(P(res), P(vd), P(rd), len(v), N, st))),
+        ("a7 expand_omega_buffer (w^i, 2^24)", N * E, N, "expand_omega_buffer",
+         [(P, omega_N), (I, log_ext), (I, 0)], True),
+        ("a8 extended_prepare (zeta coset + zero pad, 2^22 -> 2^24)", (n + N) * E, n, "extended_prepare",
+         [(P, ext), (P, coset), (I, 3), (I, n), (I, N), (I, 0), (S, st)], True),
+        ("a9 logup_sum_input_inv (sum of 1/(input + beta), 2^22)", 3 * n * E, 4 * n, "logup_sum_input_inv",
+         [(P, out_n), (P, small[0]), (P, tmp_n), (P, beta), (I, 1), (I, n), (S, st)], True),
+        ("a10 eval_logup_z_compose (2^22)", 5 * n * E, 5 * n, "eval_logup_z_compose",
+         [(P, z_n), (P, small[1]), (P, small[2]), (P, small[3]), (P, beta), (P, last), (I, n - 9), (I, n),
+          (S, st)], True),
+        ("a13 field_op_batch_mul_sum (3 terms, 6 columns, 2^24)", 8 * N * E, 6 * N, "field_op_batch_mul_sum",
+         [(P, res), (P, vd), (P, rd), (I, 12), (I, N), (S, st)], True),
         ("a13 permutation_eval_h_p2 (4 sets, rotation, 2^24)", (4 + 1 + 2) * N * E, 6 * N,
-         lambda: check(L.permutation_eval_h_p2(P(res), P(sets4), P(cols[4]), P(cols[5]), P(y), 4, -8, N))),
-        ("a13 logup_eval_h (2^24)", (9 + 2) * N * E, 9 * N,
-         lambda: check(L.logup_eval_h(P(res), *[P(c) for c in cols[:8]], P(cols[0]), P(y), 4, N, st))),
-        ("a13 shuffle_eval_h (2^24)", (6 + 2) * N * E, 9 * N,
-         lambda: check(L.shuffle_eval_h(P(res), *[P(c) for c in cols[:6]], P(y), 4, N))),
-        ("f1 poly_eval (Horner levels in place, 2^22)", 2 * n * E, n,
-         lambda: check(L.poly_eval(P(small[5]), P(out_n), P(xt), n, st))),
+         "permutation_eval_h_p2", [(P, res), (P, sets4), (P, cols[4]), (P, cols[5]), (P, y), (I, 4), (I, -8),
+                                   (I, N)], True),
+        ("a13 logup_eval_h (2^24)", (9 + 2) * N * E, 9 * N, "logup_eval_h",
+         [(P, res)] + [(P, c) for c in cols[:8]] + [(P, cols[0]), (P, y), (I, 4), (I, N), (S, st)], True),
+        ("a13 shuffle_eval_h (2^24)", (6 + 2) * N * E, 9 * N, "shuffle_eval_h",
+         [(P, res)] + [(P, c) for c in cols[:6]] + [(P, y), (I, 4), (I, N)], True),
+        ("f1 poly_eval (Horner levels in place, 2^22)", 2 * n * E, n, "poly_eval",
+         [(P, small[5]), (P, out_n), (P, xt), (I, n), (S, st)], True),
+        ("a9 zkp_batch_inverse (2^22)", 2 * n * E, 3 * n, "zkp_batch_inverse",
+         [(P, out_n), (P, small[0]), (P, None), (I, n), (I, 0), (P, tmp_n), (S, st)], False),
+        ("a10 zkp_grand_sum (prefix sum, 2^22)", 2 * n * E, 0, "zkp_grand_sum",
+         [(P, out_n), (P, small[1]), (I, n), (P, None), (P, tmp_n), (S, st)], False),
+        ("a11 zkp_permutation_z (4 columns, 2^22)", (2 * 4 + 2) * n * E, (4 * 4 + 6) * n, "zkp_permutation_z",
+         [(P, out_n), (P, pc), (P, ps), (I, 4), (P, beta), (P, gamma), (P, betas4), (P, omega_n), (P, one), (I, n),
+          (P, tmp_n), (S, st)], False),
+        ("a12 zkp_shuffle_z (2 groups, 2^22)", (2 * 2 + 1) * n * E, (2 * 2 + 6) * n, "zkp_shuffle_z",
+         [(P, out_n), (P, ins2), (P, tabs2), (P, betas2), (I, 2), (I, n), (P, ext), (S, st)], False),
     ]
+
+    def conv(spec):
+        k, v = spec
+        if k == P:
+            addr = 0 if v is None else v.data_ptr()
+            return addr if ours else ctypes.c_void_p(addr)
+        if k == S:
+            return v if ours else ctypes.c_void_p(v)
+        return v if ours else ctypes.c_int(v)
+
     out = []
-    for name, nbytes, mults, fn in cases:
+    for name, nbytes, mults, sym, args, is_ref in cases:
+        if not ours and not is_ref:
+            continue
+        fn_c = getattr(lib, sym)
+        a = [conv(x) for x in args]
+
+        def fn():
+            err = fn_c(*a)
+            if err != 0:
+                raise RuntimeError(f"{sym} returned {err}")
+
         fn()
         torch.cuda.synchronize()
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record()
+        ea, eb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ea.record()
         for _ in range(reps):
             fn()
-        b.record()
-        b.synchronize()
-        ms = a.elapsed_time(b) / reps
-        t_hbm = nbytes / (peak_hbm * 1e9) * 1e3
-        t_int = mults / mont_rate * 1e3
-        bound = "int" if t_int > t_hbm else "hbm"
-        out.append({"row": name, "ms": round(ms, 4), "GB_s": round(nbytes / (ms / 1e3) / 1e9, 1),
-                    "Gmul_s": round(mults / (ms / 1e3) / 1e9, 2), "bound": bound,
-                    "frac": round(max(t_hbm, t_int) / ms, 3)})
-    del cols, small, res, ext, omega_N, omega_n, keep
+        eb.record()
+        eb.synchronize()
+        ms = ea.elapsed_time(eb) / reps
+        row = {"row": name, "ms": round(ms, 4), "GB_s": round(nbytes / (ms / 1e3) / 1e9, 1),
+               "Gmul_s": round(mults / (ms / 1e3) / 1e9, 2)}
+        if mont_rate:
+            t_hbm = nbytes / (peak_hbm * 1e9) * 1e3
+            t_int = mults / mont_rate * 1e3
+            row.update(bound="int" if t_int > t_hbm else "hbm", frac=round(max(t_hbm, t_int) / ms, 3))
+        out.append(row)
+    del cols, small, res, ext, omega_N, omega_n
     return out
 
 
@@ -619,7 +644,7 @@ def run_ours(args):
         msm = run_msm(zkp, device) if not args.no_msm else None
         msm_batch = run_msm_batch(zkp, device) if not args.no_msm else None
         msm_columns = run_msm_columns(zkp, device) if not args.no_msm else None
-        rows = run_rows(zkp, device, mont_rate, peak_hbm) if not args.no_rows else None
+        rows = run_rows(zkp.load_library(), device, mont_rate, peak_hbm) if not args.no_rows else None
         out = {
             "metric": f"NTT HBM GB/s: batched iNTT 2^{args.log_n} -> coset NTT 2^{args.log_n + args.ext_bits}, "
                       f"{args.columns} columns",
@@ -821,6 +846,8 @@ def reference_gpu_timings(args):
             del curves, idx16, sort16, accs, cols
         del bases, sc, curve, idx, sort, acc
     out["msm"] = res
+    peak, _ = load_peaks()
+    out["rows"] = run_rows(L, dev, None, peak, ours=False)
     return out
 
 
