@@ -47,6 +47,10 @@ struct FrCfg {
         return pick8(j, 0xae216da7u, 0x1bb8e645u, 0xe35c59e3u, 0x53fe3ab1u, 0x53bb8085u, 0x8c49833du, 0x7f4e44a5u,
                      0x0216d0b1u);
     }
+    static ZK_HD constexpr uint32_t R3(int j) {  // 2^768 mod r
+        return pick8(j, 0xb4bf0040u, 0x5e94d8e1u, 0x1cfbb6b8u, 0x2a489cbeu, 0xa19fcfedu, 0x893cc664u, 0x7fcc657cu,
+                     0x0cf8594bu);
+    }
 };
 
 struct FqCfg {
@@ -63,6 +67,10 @@ struct FqCfg {
     static ZK_HD constexpr uint32_t R2(int j) {
         return pick8(j, 0x538afa89u, 0xf32cfc5bu, 0xd44501fbu, 0xb5e71911u, 0x0a417ff6u, 0x47ab1effu, 0xcab8351fu,
                      0x06d89f71u);
+    }
+    static ZK_HD constexpr uint32_t R3(int j) {  // 2^768 mod p
+        return pick8(j, 0xda1530dfu, 0xb1cd6dafu, 0xa7283db6u, 0x62f210e6u, 0x0ada0afbu, 0xef7f0b0cu, 0x2d592544u,
+                     0x20fd6e90u);
     }
 };
 
@@ -416,27 +424,98 @@ ZK_HD Fe<C> fe_pow_u32(Fe<C> a, uint32_t e) {
 }
 
 // a^(m-2): multiplicative inverse by Fermat's little theorem (0 maps to 0).
+// 8-limb helpers of the binary inversion
+ZK_HD bool limbs_is_one(const uint32_t x[8]) {
+    uint32_t o = x[0] ^ 1u;
+#pragma unroll
+    for (int j = 1; j < 8; j++) o |= x[j];
+    return o == 0;
+}
+
+ZK_HD bool limbs_geq(const uint32_t a[8], const uint32_t b[8]) {
+    uint32_t t[8];
+    return sub8_borrow(t, a, b) == 0;
+}
+
+ZK_HD void limbs_shr1(uint32_t x[8]) {
+#pragma unroll
+    for (int j = 0; j < 7; j++) x[j] = (x[j] >> 1) | (x[j + 1] << 31);
+    x[7] >>= 1;
+}
+
+// x / 2 mod m for x < m (x + m < 2^255 fits)
 template <class C>
-ZK_HD Fe<C> fe_inv(const Fe<C>& a) {
-    // exponent e = m - 2, scanned from the most significant bit
-    uint32_t e[8];
-    uint32_t two[8] = {2, 0, 0, 0, 0, 0, 0, 0};
-    uint32_t m[8];
+ZK_HD void limbs_half_mod(uint32_t x[8]) {
+    if (x[0] & 1u) {
+        uint32_t m[8];
+#pragma unroll
+        for (int j = 0; j < 8; j++) m[j] = C::M(j);
+        add8_carry(x, x, m);
+    }
+    limbs_shr1(x);
+}
+
+// x - y mod m for x, y < m
+template <class C>
+ZK_HD void limbs_sub_mod(uint32_t x[8], const uint32_t y[8]) {
+    uint32_t t[8], u[8], m[8];
 #pragma unroll
     for (int j = 0; j < 8; j++) m[j] = C::M(j);
-    sub8_borrow(e, m, two);
-    Fe<C> r = fe_one<C>();
-    bool started = false;
-    for (int w = 7; w >= 0; w--) {
-        for (int b = 31; b >= 0; b--) {
-            if (started) r = fe_sqr<C>(r);
-            if ((e[w] >> b) & 1) {
-                r = started ? fe_mul<C>(r, a) : a;
-                started = true;
-            }
+    const uint32_t br = sub8_borrow(t, x, y);
+    add8_carry(u, t, m);
+    select8(x, br, u, t);
+}
+
+// Inverse of a Montgomery-form element (zero maps to zero).  Binary extended
+// Euclid (variable time) on the representative A = a R: u, v start at A and
+// m with u = x1 A, v = x2 A (mod m) kept invariant; halving and subtracting
+// until u or v is 1 gives A^-1, and the Montgomery product with R^3 turns it
+// into a^-1 R.  Each step is a few short 8-limb chains, so one thread takes
+// a fraction of the latency of the ~380 dependent products of a^(m-2).
+template <class C>
+ZK_HD Fe<C> fe_inv(const Fe<C>& a) {
+    if (fe_is_zero<C>(a)) return a;
+    uint32_t u[8], v[8], x1[8], x2[8];
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+        u[j] = a.v[j];
+        v[j] = C::M(j);
+        x1[j] = j == 0 ? 1u : 0u;
+        x2[j] = 0u;
+    }
+    const uint32_t* res = x1;
+    for (;;) {
+        while (!(u[0] & 1u)) {
+            limbs_shr1(u);
+            limbs_half_mod<C>(x1);
+        }
+        while (!(v[0] & 1u)) {
+            limbs_shr1(v);
+            limbs_half_mod<C>(x2);
+        }
+        if (limbs_is_one(u)) {
+            res = x1;
+            break;
+        }
+        if (limbs_is_one(v)) {
+            res = x2;
+            break;
+        }
+        if (limbs_geq(u, v)) {
+            sub8_borrow(u, u, v);
+            limbs_sub_mod<C>(x1, x2);
+        } else {
+            sub8_borrow(v, v, u);
+            limbs_sub_mod<C>(x2, x1);
         }
     }
-    return r;
+    Fe<C> x, r3;
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+        x.v[j] = res[j];
+        r3.v[j] = C::R3(j);
+    }
+    return fe_mul<C>(x, r3);
 }
 
 // n-bit field of a canonical (non-Montgomery) 256-bit value starting at bit `start`
