@@ -404,6 +404,60 @@ def run_rows(lib, device, mont_rate, peak_hbm, ours=True, log_n=22, log_ext=24, 
     return out
 
 
+def run_staging(zkp, device, cols=8, log_n=22, reps=2):
+    """Column copies between HBM and host memory, 2^22-element columns: the
+    library's staging (page-locked huge-page pool + bounded copy queue, two
+    copies in flight, the reference's src/hugetlb.rs + src/async_copy_queue.rs
+    arrangement) against plain copies to and from pageable host memory."""
+    import numpy as np
+
+    H = zkp.host
+    nbytes = (1 << log_n) * 32
+    dev = [random_fr(1 << log_n, 1200 + i, device) for i in range(cols)]
+    pool = H.HostPool(nbytes, chunks_per_block=2, flags=H.HostPool.PIN | H.HostPool.HUGE)
+    q = H.CopyQueue(max_in_flight=2)
+    host = [pool.alloc(nbytes) for _ in range(cols)]
+    pageable = [np.empty(nbytes, np.uint8) for _ in range(cols)]
+    cur = torch.cuda.current_stream()
+    res = {"columns": cols, "column_bytes": nbytes}
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            fn()
+        torch.cuda.synchronize()
+        return (time.perf_counter() - t0) / reps
+
+    def q_d2h():
+        for d, p in zip(dev, host):
+            q.push(p, d.data_ptr(), nbytes, q.D2H, after=cur)
+        q.sync()
+
+    def q_h2d():
+        for d, p in zip(dev, host):
+            q.push(d.data_ptr(), p, nbytes, q.H2D, after=cur)
+        q.sync()
+
+    def plain_d2h():
+        for d, h in zip(dev, pageable):
+            h[:] = d.view(torch.uint8).reshape(-1).cpu().numpy()
+
+    def plain_h2d():
+        for d, h in zip(dev, pageable):
+            d.view(torch.uint8).reshape(-1).copy_(torch.from_numpy(h))
+
+    for name, fn in (("pinned_queue_d2h", q_d2h), ("pinned_queue_h2d", q_h2d), ("pageable_d2h", plain_d2h),
+                     ("pageable_h2d", plain_h2d)):
+        sec = timed(fn)
+        res[name + "_GB_s"] = round(cols * nbytes / sec / 1e9, 2)
+    q.close()
+    pool.close()
+    del dev
+    return res
+
+
 def run_msm_columns(zkp, device, count=16, log_n=18, reps=3):
     """count MSMs of 2^log_n points over one base array (columns committed
     together): the drop-in reference ABI (msm per column, then one
@@ -645,6 +699,7 @@ def run_ours(args):
         msm_batch = run_msm_batch(zkp, device) if not args.no_msm else None
         msm_columns = run_msm_columns(zkp, device) if not args.no_msm else None
         rows = run_rows(zkp.load_library(), device, mont_rate, peak_hbm) if not args.no_rows else None
+        staging = run_staging(zkp, device) if not args.no_rows else None
         out = {
             "metric": f"NTT HBM GB/s: batched iNTT 2^{args.log_n} -> coset NTT 2^{args.log_n + args.ext_bits}, "
                       f"{args.columns} columns",
@@ -687,6 +742,7 @@ def run_ours(args):
             "msm_batch": msm_batch,
             "msm_columns": msm_columns,
             "rows": rows,
+            "staging": staging,
         }
         if clk:
             out["clocks"] = clk

@@ -356,6 +356,38 @@ int zkp_msm_schedule_predict(const float *params, const float *features, int c_m
  * and MSM kernels.  `out` (one element) is written only if the result is 0. */
 cudaError_t zkp_calib_mont_rate(void *out, uint32_t blocks, uint32_t iters, cudaStream_t stream);
 
+/* ======================================================================
+ * Part 4: host staging (replaces src/hugetlb.rs and src/async_copy_queue.rs)
+ * ==================================================================== */
+
+/* Host memory pool handing out chunks of chunk_bytes (rounded up to 4 KiB)
+ * from blocks of chunks_per_block chunks.  flags: 1 = page-lock each block
+ * with cudaHostRegister (what src/hugetlb.rs registers), 2 = map blocks with
+ * huge pages (MAP_HUGETLB, else transparent huge pages are requested).
+ * Thread-safe; NULL on failure. */
+void *zkp_host_pool_create(size_t chunk_bytes, int chunks_per_block, int flags);
+/* one chunk (bytes <= chunk_bytes) or NULL */
+void *zkp_host_pool_alloc(void *pool, size_t bytes);
+/* 0, or -1 for a pointer the pool did not hand out (or freed twice) */
+int zkp_host_pool_free(void *pool, void *ptr);
+/* blocks mapped so far and chunks handed out (either pointer may be NULL) */
+void zkp_host_pool_stats(void *pool, size_t *blocks, size_t *used_chunks);
+void zkp_host_pool_destroy(void *pool);
+
+/* Bounded asynchronous copy queue on `device` (src/async_copy_queue.rs): at
+ * most max_in_flight copies in flight, each on its own stream.  NULL on
+ * failure.  One owner thread. */
+void *zkp_copy_queue_create(int max_in_flight, int device);
+/* one cudaMemcpyAsync of `bytes` (kind: a cudaMemcpyKind value), ordered
+ * after the work already queued on `after`; when max_in_flight copies are in
+ * flight, first waits for the oldest.  Host buffers should come from a
+ * page-locked pool for the copy to be asynchronous. */
+cudaError_t zkp_copy_queue_push(void *queue, void *dst, const void *src, size_t bytes, int kind,
+                                cudaStream_t after);
+/* waits for every copy in flight */
+cudaError_t zkp_copy_queue_sync(void *queue);
+void zkp_copy_queue_destroy(void *queue);
+
 #ifdef __cplusplus
 }
 #endif

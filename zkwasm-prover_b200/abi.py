@@ -79,6 +79,16 @@ SIGNATURES = {
     "zkp_mlp_train_step": [P, P, P, P, P, P, P, U, ctypes.c_float, I, P, P, S],
     "zkp_msm_schedule_predict": ([P, P, I, I, P, S], I),
     "zkp_calib_mont_rate": [P, U, U, S],
+    # Part 4: host staging (csrc/staging.cu)
+    "zkp_host_pool_create": ([SZ, I, I], P),
+    "zkp_host_pool_alloc": ([P, SZ], P),
+    "zkp_host_pool_free": ([P, P], I),
+    "zkp_host_pool_stats": ([P, P, P], None),
+    "zkp_host_pool_destroy": ([P], None),
+    "zkp_copy_queue_create": ([I, I], P),
+    "zkp_copy_queue_push": [P, P, P, SZ, I, S],
+    "zkp_copy_queue_sync": [P],
+    "zkp_copy_queue_destroy": ([P], None),
 }
 
 _lib = None

@@ -274,3 +274,69 @@ def grand_sum(out, inp, init=None, scratch=None, stream=None):
     scratch = scan_scratch(n) if scratch is None else scratch
     abi.check(lib().zkp_grand_sum(ptr(out), ptr(inp), n, ptr(init), ptr(scratch), stream_handle(stream)),
               "zkp_grand_sum")
+
+
+# ------------------------------------------------------------- host staging
+
+
+class HostPool:
+    """Page-locked (optionally huge-page) host chunks for column transfers
+    (zkp_host_pool_*; replaces src/hugetlb.rs).  flags: 1 = pin, 2 = huge pages."""
+
+    PIN, HUGE = 1, 2
+
+    def __init__(self, chunk_bytes: int, chunks_per_block: int = 2, flags: int = 3):
+        self.chunk = chunk_bytes
+        self.h = lib().zkp_host_pool_create(chunk_bytes, chunks_per_block, flags)
+        if not self.h:
+            raise MemoryError("zkp_host_pool_create failed")
+
+    def alloc(self, nbytes: int) -> int:
+        p = lib().zkp_host_pool_alloc(self.h, nbytes)
+        if not p:
+            raise MemoryError("zkp_host_pool_alloc failed")
+        return p
+
+    def free(self, p: int):
+        if lib().zkp_host_pool_free(self.h, p) != 0:
+            raise ValueError("pointer not from this pool (or freed twice)")
+
+    def stats(self):
+        b, u = ctypes.c_size_t(), ctypes.c_size_t()
+        lib().zkp_host_pool_stats(self.h, ctypes.byref(b), ctypes.byref(u))
+        return b.value, u.value
+
+    @staticmethod
+    def view(p: int, nbytes: int, dtype=np.uint8) -> np.ndarray:
+        """numpy view of pool memory (no copy)."""
+        buf = (ctypes.c_char * nbytes).from_address(p)
+        return np.frombuffer(buf, dtype=dtype)
+
+    def close(self):
+        if self.h:
+            lib().zkp_host_pool_destroy(self.h)
+            self.h = None
+
+
+class CopyQueue:
+    """Bounded asynchronous copy queue (zkp_copy_queue_*; replaces
+    src/async_copy_queue.rs)."""
+
+    H2D, D2H, D2D = 1, 2, 3  # cudaMemcpyKind
+
+    def __init__(self, max_in_flight: int = 2, device: int = 0):
+        self.h = lib().zkp_copy_queue_create(max_in_flight, device)
+        if not self.h:
+            raise RuntimeError("zkp_copy_queue_create failed")
+
+    def push(self, dst: int, src: int, nbytes: int, kind: int, after=None):
+        abi.check(lib().zkp_copy_queue_push(self.h, dst, src, nbytes, kind, stream_handle(after)),
+                  "zkp_copy_queue_push")
+
+    def sync(self):
+        abi.check(lib().zkp_copy_queue_sync(self.h), "zkp_copy_queue_sync")
+
+    def close(self):
+        if self.h:
+            lib().zkp_copy_queue_destroy(self.h)
+            self.h = None
