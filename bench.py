@@ -490,7 +490,7 @@ def run_msm_columns(zkp, device, count=16, log_n=18, reps=3):
     return res
 
 
-def run_msm_batch(zkp, device, count=32, lo=14, hi=20, seed=2024, reps=3):
+def run_msm_batch(zkp, device, count=32, lo=14, hi=20, seed=2024, reps=3, reference_windows=False):
     """Batched uneven MSMs over one SRS (sizes 2^U, U uniform in [lo, hi];
     per MSM the scalars are uniform (50%), small < 2^20 (35%) or 90%-sparse
     (15%)): plain per-MSM zkp_msm launches against one zkp_msm_batch pipeline,
@@ -525,7 +525,12 @@ def run_msm_batch(zkp, device, count=32, lo=14, hi=20, seed=2024, reps=3):
         return a.elapsed_time(b) / reps
 
     outs = {}
-    for name, ws in (("default", default), ("learned", learned)):
+    pickers = [("default", default), ("learned", learned)]
+    if reference_windows:
+        ref = [H.msm_window_bits(count, n) for n in ns]
+        res["reference_windows"] = ref
+        pickers.append(("reference_formula", ref))
+    for name, ws in pickers:
         scratch = torch.empty(max(zkp.load_library().zkp_msm_scratch_bytes(n, c) for n, c in zip(ns, ws)),
                               dtype=torch.uint8, device=device)
         out = torch.empty((count, 12), dtype=torch.int64, device=device)
@@ -538,16 +543,36 @@ def run_msm_batch(zkp, device, count=32, lo=14, hi=20, seed=2024, reps=3):
         del scratch
         n_arr = (ctypes.c_uint32 * count)(*ns)
         c_arr = (ctypes.c_int * count)(*ws)
-        bscr = torch.empty(zkp.load_library().zkp_msm_batch_scratch_bytes(ctypes.addressof(n_arr),
-                                                                            ctypes.addressof(c_arr), count),
-                           dtype=torch.uint8, device=device)
+        need = zkp.load_library().zkp_msm_batch_scratch_bytes(ctypes.addressof(n_arr), ctypes.addressof(c_arr), count)
+        if need == 0:  # more than 2^32 sorted entries: not one pipeline
+            res[f"batched_{name}_ms"] = None
+            continue
+        bscr = torch.empty(need, dtype=torch.uint8, device=device)
         bout = torch.empty((count, 12), dtype=torch.int64, device=device)
         res[f"batched_{name}_ms"] = round(timed(lambda: H.msm_batch(bases, cols, ns, ws, scratch=bscr, out=bout)), 3)
         outs[name] = bout
         del bscr
-    res["speedup_batched_learned_vs_plain_default"] = round(res["plain_default_ms"] / res["batched_learned_ms"], 3)
-    res["mpts_per_s_batched_learned"] = round(res["total_points"] / res["batched_learned_ms"] / 1e3, 2)
+    if res.get("batched_learned_ms"):
+        res["speedup_batched_learned_vs_plain_default"] = round(res["plain_default_ms"] / res["batched_learned_ms"],
+                                                                3)
+        res["mpts_per_s_batched_learned"] = round(res["total_points"] / res["batched_learned_ms"] / 1e3, 2)
     return res
+
+
+def run_msm_config_c(args):
+    """256 uneven MSMs over one SRS, sizes 2^U with U uniform in [14, 22], the
+    mixed scalar distribution of run_msm_batch: plain per-MSM launches and
+    one batched pipeline, with the library's windows, the learned schedule
+    and the reference host's window formula (src/cuda/msm.rs:105)."""
+    torch.cuda.set_device(0)
+    zkp = importlib.import_module("zkwasm-prover_b200")
+    zkp.load_library()
+    r = run_msm_batch(zkp, torch.device("cuda", 0), count=256, lo=14, hi=22, reps=1, reference_windows=True)
+    r.pop("mixes", None)
+    r.pop("sizes_log2", None)
+    for k in ("learned_windows", "default_windows", "reference_windows"):
+        r.pop(k, None)
+    print(json.dumps({"metric": "256 uneven MSMs 2^14..2^22 (ms)", "msm_config_c": r}))
 
 
 def run_e2e(ph, steps):
@@ -697,7 +722,8 @@ def run_ours(args):
         cpu = cpu_baseline_port(args.log_n, args.ext_bits) if not args.no_cpu_baseline else None
         msm = run_msm(zkp, device) if not args.no_msm else None
         msm_batch = run_msm_batch(zkp, device) if not args.no_msm else None
-        msm_columns = run_msm_columns(zkp, device) if not args.no_msm else None
+        msm_columns = ([run_msm_columns(zkp, device), run_msm_columns(zkp, device, count=8, log_n=22, reps=2)]
+                       if not args.no_msm else None)
         rows = run_rows(zkp.load_library(), device, mont_rate, peak_hbm) if not args.no_rows else None
         staging = run_staging(zkp, device) if not args.no_rows else None
         out = {
@@ -862,11 +888,13 @@ def reference_gpu_timings(args):
         ok = bool((O.g1_jac_to_aff(curve[0:1].cpu().numpy().view(np.uint64)) == O.msm_known_dlog(d, O.rand_fr(nn, 902))).all())
         res.append({"n": nn, "ms": round(ms, 3), "mpts_per_s": round(nn / ms / 1e3, 2), "window_bits": c,
                     "matches_oracle": ok})
-        if nn == 1 << 18:
-            # 16 columns committed together, as src/cuda/msm.rs:239-455 issues them:
-            # msm per column into its own region, then one batch_msm_collect
-            B = 16
-            c16 = min(4, 3) + 10 + max((nn - 1).bit_length(), 22) - 22  # msm.rs:105 for 16 MSMs
+        if True:
+            # columns committed together (16 of 2^18, 8 of 2^22), as
+            # src/cuda/msm.rs:239-455 issues them: msm per column into its own
+            # region, then one batch_msm_collect
+            B = 16 if nn == 1 << 18 else 8
+            lgB = (B - 1).bit_length()
+            c16 = min(lgB, 3) + 10 + max((nn - 1).bit_length(), 22) - 22  # msm.rs:105 for B MSMs
             w16 = (254 + c16 - 1) // c16
             bucket16 = w16 << c16
             region = bucket16 + 2 * worker
@@ -897,8 +925,9 @@ def reference_gpu_timings(args):
             for _ in range(reps):
                 columns()
             torch.cuda.synchronize()
-            out["msm_columns"] = {"count": B, "n": nn, "window_bits": c16,
-                                  "reference_abi_ms": round((time.perf_counter() - t0) / reps * 1e3, 3)}
+            out.setdefault("msm_columns", []).append(
+                {"count": B, "n": nn, "window_bits": c16,
+                 "reference_abi_ms": round((time.perf_counter() - t0) / reps * 1e3, 3)})
             del curves, idx16, sort16, accs, cols
         del bases, sc, curve, idx, sort, acc
     out["msm"] = res
@@ -954,11 +983,14 @@ def main():
     ap.add_argument("--no-rows", action="store_true", help="skip the per-row kernel timings")
     ap.add_argument("--msm-only", action="store_true", help="time only single MSMs (sizes from --msm-log-sizes)")
     ap.add_argument("--msm-log-sizes", default="18,22")
+    ap.add_argument("--msm-config-c", action="store_true", help="256 uneven MSMs 2^14..2^22 (about a minute)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
     elif args.msm_only:
         run_msm_only(args)
+    elif args.msm_config_c:
+        run_msm_config_c(args)
     else:
         run_ours(args)
 
