@@ -138,3 +138,12 @@ extern "C" void hc_glv_phi(uint64_t* out, const uint64_t* pts, long n) {
         memcpy(out + 8 * i + 4, r.y.v, 32);
     }
 }
+
+// lazily reduced Fr operations on inputs in [0, 2r): op 0 mul, 1 add, 2 sub
+extern "C" void hc_lazy(int op, uint64_t* out, const uint64_t* a, const uint64_t* b, long n) {
+    for (long i = 0; i < n; i++) {
+        const Fr x = ld<FrCfg>(a + 4 * i), y = ld<FrCfg>(b + 4 * i);
+        st(out + 4 * i, op == 0 ? fe_mul_lazy<FrCfg>(x, y) : op == 1 ? fe_add_lazy<FrCfg>(x, y)
+                                                                      : fe_sub_lazy<FrCfg>(x, y));
+    }
+}

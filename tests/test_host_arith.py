@@ -34,6 +34,7 @@ def hc():
         "hc_xyzz_mul_u32": [P, P, ctypes.c_uint32],
         "hc_xyzz_to_jac": [P, P],
         "hc_glv_split": [P, P, P, P, ctypes.c_long],
+        "hc_lazy": [ctypes.c_int, P, P, P, ctypes.c_long],
         "hc_glv_phi": [P, P, ctypes.c_long],
     }.items():
         getattr(L, name).argtypes = args
@@ -196,3 +197,23 @@ def test_glv_phi_is_lambda_multiple(O, hc):
     hc.hc_glv_phi(_p(out), _p(pts), pts.shape[0])
     lam = O.fr_vec([x * O.GLV_LAMBDA % O.R_MOD for x in O.fr_ints(d)])
     assert (out == O.g1_gen_bases(lam)).all()
+
+
+@pytest.mark.parametrize("op", [0, 1, 2])
+def test_lazy_fr_ops(O, hc, op):
+    # representatives in [0, 2r): results stay below 2r and are congruent to
+    # the exact Montgomery product / sum / difference
+    r = O.R_MOD
+    rng = random.Random(40 + op)
+    xs = [0, 1, r - 1, r, r + 1, 2 * r - 1] + [rng.randrange(2 * r) for _ in range(2000)]
+    ys = [2 * r - 1, r, 1, 0, r - 1, 2 * r - 1] + [rng.randrange(2 * r) for _ in range(2000)]
+    lim = lambda v: np.array([[(v >> (64 * j)) & (2 ** 64 - 1) for j in range(4)]], np.uint64)
+    a = np.concatenate([lim(x) for x in xs])
+    b = np.concatenate([lim(y) for y in ys])
+    out = np.zeros_like(a)
+    hc.hc_lazy(op, _p(out), _p(a), _p(b), a.shape[0])
+    rinv = pow(1 << 256, -1, r)
+    for i, (x, y) in enumerate(zip(xs, ys)):
+        got = sum(int(out[i, j]) << (64 * j) for j in range(4))
+        exp = x * y * rinv if op == 0 else x + y if op == 1 else x - y
+        assert got < 2 * r and (got - exp) % r == 0

@@ -287,7 +287,9 @@ ZK_HD void merge_shift(uint32_t o[9], const uint32_t e[9]) {
 #endif
 }
 
-// Montgomery product a * b * 2^-256 mod m; a, b < 2m, result < m.
+// Montgomery product a * b * 2^-256 mod m without the final subtraction:
+// for a, b < 2m (and m < 2^254) the result is below (4m^2 + m 2^256) / 2^256
+// < 2m.
 //
 // Operand scanning with the running sum T split into an even accumulator E
 // (products of even limbs of a) and an odd accumulator O (odd limbs, one word
@@ -296,7 +298,7 @@ ZK_HD void merge_shift(uint32_t o[9], const uint32_t e[9]) {
 // operands, then folds E >> 32 into O, which becomes the next row's E.  This
 // measured about 1.5x the rate of the lo-chain / hi-chain row form on B200.
 template <class C>
-ZK_HD Fe<C> fe_mul(const Fe<C>& a, const Fe<C>& b) {
+ZK_HD Fe<C> fe_mul_lazy(const Fe<C>& a, const Fe<C>& b) {
     uint32_t m[8];
 #pragma unroll
     for (int j = 0; j < 8; j++) m[j] = C::M(j);
@@ -317,10 +319,57 @@ ZK_HD Fe<C> fe_mul(const Fe<C>& a, const Fe<C>& b) {
             o[j] = 0;
         }
     }
-    fe_reduce_once<C>(e);
     Fe<C> r;
 #pragma unroll
     for (int j = 0; j < 8; j++) r.v[j] = e[j];
+    return r;
+}
+
+// Montgomery product a * b * 2^-256 mod m; a, b < 2m, result < m.
+template <class C>
+ZK_HD Fe<C> fe_mul(const Fe<C>& a, const Fe<C>& b) {
+    Fe<C> r = fe_mul_lazy<C>(a, b);
+    fe_reduce_once<C>(r.v);
+    return r;
+}
+
+// 2m, limb j
+template <class C>
+ZK_HD constexpr uint32_t twice_m(int j) {
+    return (C::M(j) << 1) | (j ? C::M(j - 1) >> 31 : 0u);
+}
+
+// Lazily reduced representatives in [0, 2m) (m < 2^254, so sums of two stay
+// below 2^256): a + b and a - b for a, b < 2m, results < 2m; fe_canon maps
+// [0, 2m) to the canonical [0, m).
+template <class C>
+ZK_HD Fe<C> fe_add_lazy(const Fe<C>& a, const Fe<C>& b) {
+    uint32_t t[8], u[8], m2[8];
+#pragma unroll
+    for (int j = 0; j < 8; j++) m2[j] = twice_m<C>(j);
+    add8_carry(t, a.v, b.v);
+    const uint32_t br = sub8_borrow(u, t, m2);
+    Fe<C> r;
+    select8(r.v, br, t, u);
+    return r;
+}
+
+template <class C>
+ZK_HD Fe<C> fe_sub_lazy(const Fe<C>& a, const Fe<C>& b) {
+    uint32_t t[8], u[8], m2[8];
+#pragma unroll
+    for (int j = 0; j < 8; j++) m2[j] = twice_m<C>(j);
+    const uint32_t br = sub8_borrow(t, a.v, b.v);
+    add8_carry(u, t, m2);
+    Fe<C> r;
+    select8(r.v, br, u, t);
+    return r;
+}
+
+template <class C>
+ZK_HD Fe<C> fe_canon(const Fe<C>& a) {
+    Fe<C> r = a;
+    fe_reduce_once<C>(r.v);
     return r;
 }
 

@@ -30,10 +30,17 @@ namespace zk {
 // Every Fr product of the pass kernels goes through one out-of-line function:
 // inlined, the ~30 product sites of a pass (each ~350 instructions) overflow
 // the instruction cache and warps stall on instruction fetch.
+//
+// Inside a pass, values are kept lazily reduced in [0, 2r): the products skip
+// their final conditional subtraction (nt_mulz) and the butterflies add and
+// subtract modulo 2r; every value leaves a pass canonical (fe_canon at the
+// last sub-stage), so buffers in global memory always hold canonical values.
 #if defined(ZK_NTT_INLINE_MUL)
 __device__ __forceinline__ Fr nt_mul(const Fr& a, const Fr& b) { return fe_mul<FrCfg>(a, b); }
+__device__ __forceinline__ Fr nt_mulz(const Fr& a, const Fr& b) { return fe_mul_lazy<FrCfg>(a, b); }
 #else
 __device__ __noinline__ Fr nt_mul(const Fr a, const Fr b) { return fe_mul<FrCfg>(a, b); }
+__device__ __noinline__ Fr nt_mulz(const Fr a, const Fr b) { return fe_mul_lazy<FrCfg>(a, b); }
 #endif
 
 // ---------------------------------------------------------------- small DFTs
@@ -41,8 +48,8 @@ __device__ __noinline__ Fr nt_mul(const Fr a, const Fr b) { return fe_mul<FrCfg>
 // relabelled by the caller.
 
 __device__ __forceinline__ void dft2(Fr& a, Fr& b) {
-    Fr t = fe_add<FrCfg>(a, b);
-    b = fe_sub<FrCfg>(a, b);
+    Fr t = fe_add_lazy<FrCfg>(a, b);
+    b = fe_sub_lazy<FrCfg>(a, b);
     a = t;
 }
 
@@ -50,7 +57,7 @@ __device__ __forceinline__ void dft2(Fr& a, Fr& b) {
 __device__ __forceinline__ void dft4_dif(Fr& v0, Fr& v1, Fr& v2, Fr& v3, const Fr& w4) {
     dft2(v0, v2);
     dft2(v1, v3);
-    v3 = nt_mul(v3, w4);
+    v3 = nt_mulz(v3, w4);
     dft2(v0, v1);
     dft2(v2, v3);
 }
@@ -61,9 +68,9 @@ __device__ __forceinline__ void dft8_dif(Fr v[8], const Fr& w8, const Fr& w4, co
     dft2(v[1], v[5]);
     dft2(v[2], v[6]);
     dft2(v[3], v[7]);
-    v[5] = nt_mul(v[5], w8);
-    v[6] = nt_mul(v[6], w4);
-    v[7] = nt_mul(v[7], w83);
+    v[5] = nt_mulz(v[5], w8);
+    v[6] = nt_mulz(v[6], w4);
+    v[7] = nt_mulz(v[7], w83);
     dft4_dif(v[0], v[1], v[2], v[3], w4);
     dft4_dif(v[4], v[5], v[6], v[7], w4);
 }
@@ -100,11 +107,12 @@ struct PassOut {
     const Fr* wrow;  // when set: output y is multiplied by wrow[y] instead
 };
 
+// (the result is canonical: it leaves the pass)
 __device__ __forceinline__ Fr finish_out(const PassOut& o, Fr v, uint32_t y) {
-    if (o.wrow) return nt_mul(v, ldg_elem<FrCfg>(o.wrow + y));
-    if (o.qhi != 0 && y != 0) v = nt_mul(v, ldg_elem<FrCfg>(o.tw + ((size_t)(o.qhi * y) << o.log_p)));
-    if (o.scale) v = nt_mul(v, ldg_elem<FrCfg>(o.scale));
-    return v;
+    if (o.wrow) return fe_canon<FrCfg>(nt_mulz(v, ldg_elem<FrCfg>(o.wrow + y)));
+    if (o.qhi != 0 && y != 0) v = nt_mulz(v, ldg_elem<FrCfg>(o.tw + ((size_t)(o.qhi * y) << o.log_p)));
+    if (o.scale) v = nt_mulz(v, ldg_elem<FrCfg>(o.scale));
+    return fe_canon<FrCfg>(v);
 }
 
 // radix-8 sub-stage over one DFT of size R in shared memory
@@ -121,7 +129,7 @@ __device__ __forceinline__ void stage8(Fr* x, int u, int log_ps, bool last, cons
     if (in_mul) {
 #pragma unroll
         for (int i = 0; i < 8; i++)
-            v[i] = nt_mul(v[i], ldg_elem<FrCfg>(in_mul + in_base + ((size_t)(u + S * i) << log_items)));
+            v[i] = nt_mulz(v[i], ldg_elem<FrCfg>(in_mul + in_base + ((size_t)(u + S * i) << log_items)));
     }
     const int sh = log_n - LOGR;  // w_R^e = tw[e << sh]
     {
@@ -138,7 +146,7 @@ __device__ __forceinline__ void stage8(Fr* x, int u, int log_ps, bool last, cons
     for (int j = 0; j < 8; j++) {
         Fr y = v[rev[j]];
         if (j != 0 && ilo != 0)
-            y = nt_mul(y, ldg_elem<FrCfg>(tw + ((size_t)((ilo * j) << log_ps) << sh)));
+            y = nt_mulz(y, ldg_elem<FrCfg>(tw + ((size_t)((ilo * j) << log_ps) << sh)));
         const int pos = J + (j << log_ps) + (ilo << (log_ps + 3));
         if (last) y = finish_out(po, y, (uint32_t)pos);
         sm_st(x, pos, y);
@@ -169,7 +177,7 @@ __device__ __forceinline__ void stage4_last(Fr* x, int lt, const Fr* tw, int log
         if (in_mul) {
 #pragma unroll
             for (int i = 0; i < 4; i++)
-                v[4 * k + i] = nt_mul(
+                v[4 * k + i] = nt_mulz(
                     v[4 * k + i], ldg_elem<FrCfg>(in_mul + in_base + ((size_t)(u + S * i) << log_items)));
         }
         dft4_dif(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3], w4);
@@ -360,10 +368,10 @@ ntt_fused_extend_kernel(FusedExtendArgs a) {
             __syncthreads();
             for (int i = tid; i < R; i += T) {
                 const Fr cf = z == 0 ? sm_ld(A, i) : ld_elem<FrCfg>(coeff + q + ((size_t)i << log_items));
-                sm_st(B, i, nt_mul(cf, ldg_elem<FrCfg>(S + i)));
+                sm_st(B, i, nt_mulz(cf, ldg_elem<FrCfg>(S + i)));
             }
         } else {
-            for (int i = tid; i < R; i += T) sm_st(B, i, nt_mul(sm_ld(A, i), ldg_elem<FrCfg>(S + i)));
+            for (int i = tid; i < R; i += T) sm_st(B, i, nt_mulz(sm_ld(A, i), ldg_elem<FrCfg>(S + i)));
         }
         __syncthreads();
         PassOut pf;
