@@ -280,8 +280,31 @@ def run_msm(zkp, device, sizes=(1 << 18, 1 << 22), reps=5):
         b.synchronize()
         ms = a.elapsed_time(b) / reps
         c = zkp.load_library().zkp_msm_default_window(n)
-        res.append({"n": n, "ms": round(ms, 4), "mpts_per_s": round(n / ms / 1e3, 2), "window_bits": c})
-        del bases, scalars, scratch
+        line = {"n": n, "ms": round(ms, 4), "mpts_per_s": round(n / ms / 1e3, 2), "window_bits": c}
+        # the same MSM over a table of pre-multiplied bases (the bases stay
+        # resident across MSMs, as an SRS does); the one-time build is timed
+        # apart
+        a.record()
+        table, tc = H.msm_table_build(bases, n)
+        b.record()
+        b.synchronize()
+        build_ms = a.elapsed_time(b)
+        tscratch = torch.empty(max(1, zkp.load_library().zkp_msm_table_scratch_bytes(n, tc)), dtype=torch.uint8,
+                               device=device)
+        tout = torch.empty(12, dtype=torch.int64, device=device)
+        for _ in range(2):
+            H.msm_table(table, n, tc, scalars, n=n, scratch=tscratch, out=tout)
+        torch.cuda.synchronize()
+        a.record()
+        for _ in range(reps):
+            H.msm_table(table, n, tc, scalars, n=n, scratch=tscratch, out=tout)
+        b.record()
+        b.synchronize()
+        tms = a.elapsed_time(b) / reps
+        line.update({"table_ms": round(tms, 4), "table_mpts_per_s": round(n / tms / 1e3, 2),
+                     "table_window_bits": tc, "table_build_ms": round(build_ms, 2)})
+        res.append(line)
+        del bases, scalars, scratch, table, tscratch
     return res
 
 

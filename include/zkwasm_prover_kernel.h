@@ -203,6 +203,32 @@ int zkp_msm_default_window(uint32_t n);
 cudaError_t zkp_msm(void *out, const void *bases, const void *scalars, uint32_t n, int window_bits, void *scratch,
                     size_t scratch_bytes, cudaStream_t stream);
 
+/* Tables of pre-multiplied bases for MSMs over a resident base array (the
+ * SRS of a proving key; the reference host passes the same device bases to
+ * every msm call, src/cuda/msm.rs:256-455).  A table for window_bits c
+ * (4..22) holds W = ceil(128 / c) windows of 2 nsrs affine points:
+ * [2^(c j)] bases_i at j 2 nsrs + i and its endomorphism image at
+ * j 2 nsrs + nsrs + i.  zkp_msm_table_bytes is 0 for an unsupported width. */
+size_t zkp_msm_table_bytes(uint32_t nsrs, int window_bits);
+
+/* Window width the library picks for an MSM of n points over a table. */
+int zkp_msm_table_default_window(uint32_t n);
+
+/* Fills a table of zkp_msm_table_bytes(nsrs, window_bits) bytes from nsrs
+ * affine bases (Montgomery form, the identity as (0, 0)). */
+cudaError_t zkp_msm_table_build(void *table, const void *bases, uint32_t nsrs, int window_bits,
+                                cudaStream_t stream);
+
+/* Scratch bytes of zkp_msm_table for n points (0 for an unsupported width). */
+size_t zkp_msm_table_scratch_bytes(uint32_t n, int window_bits);
+
+/* out (96-byte Jacobian) = sum_{i < n} [scalars_i] bases_i over a table built
+ * with the same nsrs and window_bits (n <= nsrs).  All windows share one
+ * bucket set: no doublings between windows and one bucket reduction.  No
+ * allocation, no host synchronisation. */
+cudaError_t zkp_msm_table(void *out, const void *table, uint32_t nsrs, int window_bits, const void *scalars,
+                          uint32_t n, void *scratch, size_t scratch_bytes, cudaStream_t stream);
+
 /* Scratch bytes of zkp_msm_batch for `count` MSMs of n[i] points with window
  * widths window_bits[i] (host arrays; window_bits NULL or 0 entries pick the
  * default width for each size). */

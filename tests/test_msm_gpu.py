@@ -186,3 +186,103 @@ def test_reference_abi_batch_msm(O, gpu, n):
     res = H.batch_msm(bases, [H.to_device(c) for c in cols], n)
     for i, c in enumerate(cols):
         assert (_jac_to_aff(O, res[i]) == O.msm_known_dlog(d, c)).all()
+
+
+# ------------------------------------------------------- pre-multiplied base tables
+
+def _table_run(gpu, table, nsrs, c, scalars):
+    H = gpu.host
+    out = H.msm_table(table, nsrs, c, H.to_device(scalars), n=scalars.shape[0])
+    torch.cuda.synchronize()
+    return H.to_host(out)
+
+
+@pytest.mark.parametrize("c", [4, 7, 13, 22])
+def test_msm_table_entries(O, gpu, c):
+    # entry j 2N + i = [2^(c j) d_i] G and entry j 2N + N + i = [lambda 2^(c j) d_i] G
+    N = 37
+    d = O.rand_fr(N, 80 + c)
+    d[5] = 0                                   # identity base
+    bases = O.g1_gen_bases(d)
+    H = gpu.host
+    table, cc = H.msm_table_build(H.to_device(bases), N, c)
+    assert cc == c
+    torch.cuda.synchronize()
+    t = H.to_host(table).reshape(-1, 8)
+    W = (128 + c - 1) // c
+    assert t.shape[0] == W * 2 * N
+    dl = O.fr_ints(d)
+    for j in range(W):
+        m = pow(2, c * j, O.R_MOD)
+        assert (t[j * 2 * N: j * 2 * N + N] == O.g1_gen_bases(O.fr_vec([x * m for x in dl]))).all(), j
+        assert (t[j * 2 * N + N: (j + 1) * 2 * N] ==
+                O.g1_gen_bases(O.fr_vec([x * m * O.GLV_LAMBDA for x in dl]))).all(), j
+
+
+@pytest.mark.parametrize("c", [5, 9, 13, 16, 22])
+def test_msm_table_widths(O, gpu, c):
+    N = 3000
+    d = O.rand_fr(N, 90)
+    bases = O.g1_gen_bases(d)
+    H = gpu.host
+    table, _ = H.msm_table_build(H.to_device(bases), N, c)
+    for n in (N, 1, 2, 777):                   # the whole table and prefixes of it
+        s = O.rand_fr(n, 91 + n)
+        got = _jac_to_aff(O, _table_run(gpu, table, N, c, s))
+        assert (got == O.msm_known_dlog(d[:n], s)).all(), (c, n)
+
+
+def test_msm_table_edge_cases(O, gpu):
+    n = 2048
+    d = O.rand_fr(n, 95)
+    s = O.rand_fr(n, 96)
+    s[0:50] = 0
+    s[50:60] = O.fr(O.R_MOD - 1)
+    s[60:70] = O.fr(1)
+    d[70:80] = 0                               # identity bases
+    s[80:90] = O.fr((1 << 253) + 1)
+    d[100] = d[101]                            # repeated point: doubling in a bucket
+    s[100] = s[101]
+    s[200:1200] = s[3]                         # one bucket per window holds 1000 points
+    bases = O.g1_gen_bases(d)
+    H = gpu.host
+    for c in (0, 8, 16):
+        table, cc = H.msm_table_build(H.to_device(bases), n, c)
+        got = _jac_to_aff(O, _table_run(gpu, table, n, cc, s))
+        assert (got == O.msm_known_dlog(d, s)).all(), c
+
+
+def test_msm_table_zero_result_and_empty(O, gpu):
+    d = O.rand_fr(2, 97)
+    d[1] = O.fr(O.R_MOD - O.fr_ints(d[:1])[0])  # base 1 = -base 0
+    bases = O.g1_gen_bases(d)
+    H = gpu.host
+    table, c = H.msm_table_build(H.to_device(bases), 2, 0)
+    s = np.repeat(O.rand_fr(1, 98), 2, axis=0)
+    assert O.fq_ints(_table_run(gpu, table, 2, c, s)[8:])[0] == 0
+    out = H.msm_table(table, 2, c, H.to_device(s), n=0)
+    torch.cuda.synchronize()
+    assert O.fq_ints(H.to_host(out)[8:])[0] == 0
+
+
+def test_msm_table_2_18_matches_plain(O, gpu):
+    # the benchmark size through the default table width, against the known
+    # discrete log and the plain MSM on the same inputs
+    n = 1 << 18
+    d = O.rand_fr(n, 99)
+    bases = O.g1_gen_bases(d)
+    s = O.rand_fr(n, 100)
+    H = gpu.host
+    table, c = H.msm_table_build(H.to_device(bases), n, 0)
+    got = _table_run(gpu, table, n, c, s)
+    assert (_jac_to_aff(O, got) == O.msm_known_dlog(d, s)).all()
+    assert (_jac_to_aff(O, got) == _jac_to_aff(O, _run(gpu, bases, s))).all()
+
+
+def test_msm_table_rejects_bad_arguments(gpu):
+    L = gpu.load_library()
+    assert L.zkp_msm_table_bytes(100, 3) == 0 and L.zkp_msm_table_bytes(100, 23) == 0
+    assert L.zkp_msm_table_scratch_bytes(100, 3) == 0
+    # n above the table's points, and a table too large for 31-bit entry indices
+    assert L.zkp_msm_table(1, 1, 10, 16, 1, 11, 1, 1 << 30, None) != 0
+    assert L.zkp_msm_table_build(1, 1, 1 << 28, 4, None) != 0

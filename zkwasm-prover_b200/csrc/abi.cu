@@ -349,6 +349,42 @@ cudaError_t zkp_msm(void* out, const void* bases, const void* scalars, uint32_t 
     return msm_run(reinterpret_cast<Jac*>(out), reinterpret_cast<const Aff*>(bases), CF(scalars), pl, sc, stream);
 }
 
+size_t zkp_msm_table_bytes(uint32_t nsrs, int window_bits) {
+    return msm_table_points(nsrs, window_bits) * sizeof(Aff);
+}
+
+int zkp_msm_table_default_window(uint32_t n) { return msm_table_default_window(n); }
+
+// table entries are addressed by 31-bit indices
+static bool table_fits(uint32_t nsrs, int window_bits) {
+    const size_t pts = msm_table_points(nsrs, window_bits);
+    return pts > 0 && pts <= 0x80000000ull;
+}
+
+cudaError_t zkp_msm_table_build(void* table, const void* bases, uint32_t nsrs, int window_bits,
+                                cudaStream_t stream) {
+    if (nsrs && (!table || !bases)) return cudaErrorInvalidValue;
+    if (!table_fits(nsrs ? nsrs : 1, window_bits)) return cudaErrorInvalidValue;
+    return msm_table_build(reinterpret_cast<Aff*>(table), reinterpret_cast<const Aff*>(bases), nsrs, window_bits,
+                           stream);
+}
+
+size_t zkp_msm_table_scratch_bytes(uint32_t n, int window_bits) {
+    if (window_bits < 4 || window_bits > 22) return 0;
+    return msm_scratch_bytes(msm_make_table_plan(n, window_bits, n ? n : 1));
+}
+
+cudaError_t zkp_msm_table(void* out, const void* table, uint32_t nsrs, int window_bits, const void* scalars,
+                          uint32_t n, void* scratch, size_t scratch_bytes, cudaStream_t stream) {
+    if (!out || (n && (!table || !scalars || !scratch))) return cudaErrorInvalidValue;
+    if (n > nsrs || !table_fits(nsrs ? nsrs : 1, window_bits)) return cudaErrorInvalidValue;
+    MsmPlan pl = msm_make_table_plan(n, window_bits, nsrs);
+    if (n && msm_scratch_bytes(pl) > scratch_bytes) return cudaErrorInvalidValue;
+    MsmScratch sc = {};
+    if (n) msm_layout(pl, scratch, &sc);
+    return msm_run(reinterpret_cast<Jac*>(out), reinterpret_cast<const Aff*>(table), CF(scalars), pl, sc, stream);
+}
+
 size_t zkp_msm_batch_scratch_bytes(const uint32_t* n, const int* window_bits, uint32_t count) {
     if (!n) return 0;
     return msm_batch_scratch_bytes(n, window_bits, count);

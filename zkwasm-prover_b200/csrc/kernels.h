@@ -53,15 +53,17 @@ cudaError_t geometric(Fr* out, const Fr* base, const Fr* w, uint32_t n, cudaStre
 // ------------------------------------------------------------------ MSM
 struct MsmPlan {
     int c;          // window bits (signed digits in [-(2^(c-1)-1), 2^(c-1)])
-    int W;          // windows
+    int W;          // windows (digits per scalar)
     uint32_t B;     // buckets per window, 2^(c-1)
-    uint32_t NB;    // W * B
+    uint32_t NB;    // Wb * B
     uint32_t L;     // sorted entries per accumulation thread
     uint32_t nacc;  // accumulation threads
     uint32_t seg;   // buckets per reduction segment
-    uint32_t G;     // reduction segments per window
+    uint32_t G;     // reduction segments per bucket set
     uint32_t n;
     int glv;        // 1: scalars split k = k1 + k2 lambda over the bases and their endomorphism images
+    int Wb;         // bucket sets: W, or 1 over a table of pre-multiplied bases
+    uint32_t nsrs;  // table plans: points per window of the table (0: no table)
 };
 
 struct MsmScratch {
@@ -72,12 +74,22 @@ struct MsmScratch {
     uint32_t* part_key;  // 2 * nacc + msm_merge_extra(nacc)
     Xyzz* part_pt;       // 2 * nacc + msm_merge_extra(nacc)
     Xyzz* buckets;       // NB
-    Xyzz* segsum;        // W * G
-    Xyzz* winsum;        // W
-    Aff* phi;            // n endomorphism images of the bases (GLV plans), else null
+    Xyzz* segsum;        // Wb * G
+    Xyzz* winsum;        // Wb
+    Aff* phi;            // n endomorphism images of the bases (GLV plans without a table), else null
 };
 
 MsmPlan msm_make_plan(uint32_t n, int c, bool glv = true);
+// plan over a table of pre-multiplied bases (msm_table_*): all windows share
+// one bucket set; the table holds nsrs >= n points per window
+MsmPlan msm_make_table_plan(uint32_t n, int c, uint32_t nsrs);
+// window bits the library picks for an MSM of n points over a table
+int msm_table_default_window(uint32_t n);
+// Table of pre-multiplied bases: for window j < W (W = ceil(128 / c)) and
+// i < nsrs, entry j 2 nsrs + i is [2^(c j)] base_i and entry
+// j 2 nsrs + nsrs + i its endomorphism image, as affine points.
+size_t msm_table_points(uint32_t nsrs, int c);
+cudaError_t msm_table_build(Aff* table, const Aff* bases, uint32_t nsrs, int c, cudaStream_t st);
 // sorted entries (nonzero digits at most) of a plan: n W, or 2 n W with GLV
 inline size_t msm_entry_count(const MsmPlan& p) { return (size_t)p.n * p.W * (p.glv ? 2 : 1); }
 size_t msm_u32_words(const MsmPlan& p);     // count + offset + scan tmp + entries + part keys

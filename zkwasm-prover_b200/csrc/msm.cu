@@ -47,12 +47,15 @@ __device__ __forceinline__ uint32_t key_group(uint32_t key, int& leader, uint32_
 
 // histogram of the nonzero signed digits of one scalar magnitude v (whole
 // warps: lanes without a scalar pass zero)
-__device__ __forceinline__ void count_digits(const uint32_t v[8], int c, int W, uint32_t* __restrict__ count) {
-    const uint32_t B = 1u << (c - 1);
+// Bucket key of digit d of window w: w * kw + |d| - 1 (kw = 2^(c-1) gives
+// every window its own buckets; kw = 0 puts all windows into one set, for
+// tables of the bases pre-multiplied by 2^(c w)).
+__device__ __forceinline__ void count_digits(const uint32_t v[8], int c, int W, uint32_t kw,
+                                             uint32_t* __restrict__ count) {
     uint32_t carry = 0;
     for (int w = 0; w < W; w++) {
         const int d = msm_signed_digit(v, w, c, carry);
-        const uint32_t key = d != 0 ? (uint32_t)w * B + (uint32_t)(d > 0 ? d : -d) - 1 : KEY_NONE;
+        const uint32_t key = d != 0 ? (uint32_t)w * kw + (uint32_t)(d > 0 ? d : -d) - 1 : KEY_NONE;
         int leader;
         uint32_t rank;
         const uint32_t peers = key_group(key, leader, rank);
@@ -60,14 +63,14 @@ __device__ __forceinline__ void count_digits(const uint32_t v[8], int c, int W, 
     }
 }
 
-// entries (point | sign << 31) of the nonzero digits of one scalar magnitude v
-// whose point is `point`, negated when `neg`.  Windows go in groups of eight:
-// the digits, then eight independent slot claims (atomics with a return
-// value) in flight together, then the stores.
-__device__ __forceinline__ void scatter_digits(const uint32_t v[8], int c, int W, uint32_t point, bool neg,
-                                               const uint32_t* __restrict__ offset, uint32_t* __restrict__ count,
-                                               uint32_t* __restrict__ entries) {
-    const uint32_t B = 1u << (c - 1);
+// entries (point + w pw | sign << 31) of the nonzero digits of one scalar
+// magnitude v whose point is `point`, negated when `neg` (pw = 0, or the
+// window stride of a table of pre-multiplied bases).  Windows go in groups of
+// eight: the digits, then eight independent slot claims (atomics with a
+// return value) in flight together, then the stores.
+__device__ __forceinline__ void scatter_digits(const uint32_t v[8], int c, int W, uint32_t kw, uint32_t point,
+                                               uint32_t pw, bool neg, const uint32_t* __restrict__ offset,
+                                               uint32_t* __restrict__ count, uint32_t* __restrict__ entries) {
     const uint32_t nbit = neg ? 0x80000000u : 0u;
     uint32_t carry = 0;
     for (int w0 = 0; w0 < W; w0 += 8) {
@@ -79,7 +82,7 @@ __device__ __forceinline__ void scatter_digits(const uint32_t v[8], int c, int W
                 const int d = msm_signed_digit(v, w0 + u, c, carry);
                 if (d != 0) {
                     const uint32_t mag = d > 0 ? (uint32_t)d : (uint32_t)(-d);
-                    key[u] = ((uint32_t)(w0 + u) * B + mag - 1) | ((d < 0 ? 0x80000000u : 0u) ^ nbit);
+                    key[u] = ((uint32_t)(w0 + u) * kw + mag - 1) | ((d < 0 ? 0x80000000u : 0u) ^ nbit);
                 }
             }
         }
@@ -99,15 +102,16 @@ __device__ __forceinline__ void scatter_digits(const uint32_t v[8], int c, int W
         }
 #pragma unroll
         for (int u = 0; u < 8; u++)
-            if (key[u] != KEY_NONE) entries[base[u] + slot[u]] = point | (key[u] & 0x80000000u);
+            if (key[u] != KEY_NONE)
+                entries[base[u] + slot[u]] = (point + (uint32_t)(w0 + u) * pw) | (key[u] & 0x80000000u);
     }
 }
 
 // one thread per scalar: Montgomery -> canonical, then the digits of the
 // scalar (GLV = false) or of its two GLV halves |k1| (point i) and |k2|
-// (point n + i, the image of base i under the endomorphism)
+// (point phi_off + i, the image of base i under the endomorphism)
 template <bool GLV>
-__global__ void msm_count_kernel(const Fr* __restrict__ scalars, uint32_t n, int c, int W,
+__global__ void msm_count_kernel(const Fr* __restrict__ scalars, uint32_t n, int c, int W, uint32_t kw,
                                  uint32_t* __restrict__ count) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i - (threadIdx.x & 31) >= n) return;  // whole warps past the end
@@ -116,17 +120,17 @@ __global__ void msm_count_kernel(const Fr* __restrict__ scalars, uint32_t n, int
         uint32_t m1[8], m2[8];
         bool n1, n2;
         glv_split(k.v, m1, m2, n1, n2);
-        count_digits(m1, c, W, count);
-        count_digits(m2, c, W, count);
+        count_digits(m1, c, W, kw, count);
+        count_digits(m2, c, W, kw, count);
     } else {
-        count_digits(k.v, c, W, count);
+        count_digits(k.v, c, W, kw, count);
     }
 }
 
 template <bool GLV>
-__global__ void msm_scatter_kernel(const Fr* __restrict__ scalars, uint32_t n, int c, int W,
-                                   const uint32_t* __restrict__ offset, uint32_t* __restrict__ count,
-                                   uint32_t* __restrict__ entries) {
+__global__ void msm_scatter_kernel(const Fr* __restrict__ scalars, uint32_t n, int c, int W, uint32_t kw,
+                                   uint32_t pw, uint32_t phi_off, const uint32_t* __restrict__ offset,
+                                   uint32_t* __restrict__ count, uint32_t* __restrict__ entries) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i - (threadIdx.x & 31) >= n) return;  // whole warps past the end
     const Fr k = i < n ? fe_from_mont<FrCfg>(ldg_elem<FrCfg>(scalars + i)) : fe_zero<FrCfg>();
@@ -134,10 +138,10 @@ __global__ void msm_scatter_kernel(const Fr* __restrict__ scalars, uint32_t n, i
         uint32_t m1[8], m2[8];
         bool n1, n2;
         glv_split(k.v, m1, m2, n1, n2);
-        scatter_digits(m1, c, W, i, n1, offset, count, entries);
-        scatter_digits(m2, c, W, n + i, n2, offset, count, entries);
+        scatter_digits(m1, c, W, kw, i, pw, n1, offset, count, entries);
+        scatter_digits(m2, c, W, kw, phi_off + i, pw, n2, offset, count, entries);
     } else {
-        scatter_digits(k.v, c, W, i, false, offset, count, entries);
+        scatter_digits(k.v, c, W, kw, i, pw, false, offset, count, entries);
     }
 }
 
@@ -419,10 +423,61 @@ __global__ void __launch_bounds__(COOP_THREADS) msm_final_kernel(const Xyzz* __r
     }
 }
 
-// ------------------------------------------------------------------ planning
-
 // windows of c bits for 254-bit scalars, or for the < 2^127 GLV halves
 static int windows_for(int c, bool glv) { return glv ? (128 + c - 1) / c : (254 + c - 1) / c; }
+
+// ------------------------------------------------------------ base tables
+// For bases that stay resident across many MSMs (the SRS of a proving key),
+// entry j 2 nsrs + i = [2^(c j)] base_i and entry j 2 nsrs + nsrs + i its
+// endomorphism image.  Digit d of window j of a scalar then adds table entry
+// j directly into the one bucket set of |d|: the sum over windows needs no
+// doublings, and the bucket reduction runs once instead of once per window.
+
+// (X / ZZ, Y / ZZZ) with one inversion: 1 / ZZ = ZZZ / (ZZ ZZZ), 1 / ZZZ = ZZ / (ZZ ZZZ)
+__device__ __forceinline__ Aff xyzz_to_aff(const Xyzz& p) {
+    Aff r;
+    if (xyzz_is_id(p)) {
+        r.x = fe_zero<FqCfg>();
+        r.y = fe_zero<FqCfg>();
+        return r;
+    }
+    const Fq inv = fe_inv<FqCfg>(cmul(p.zz, p.zzz));
+    r.x = cmul(p.x, cmul(inv, p.zzz));
+    r.y = cmul(p.y, cmul(inv, p.zz));
+    return r;
+}
+
+__device__ __forceinline__ void st_aff(Aff* p, const Aff& a) {
+    st_elem<FqCfg>(&p->x, a.x);
+    st_elem<FqCfg>(&p->y, a.y);
+}
+
+// one thread per base: W windows of c doublings each
+__global__ void __launch_bounds__(128) msm_table_kernel(Aff* __restrict__ table, const Aff* __restrict__ bases,
+                                                        uint32_t nsrs, int c, int W) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nsrs) return;
+    const size_t stride = 2 * (size_t)nsrs;
+    Aff a = ld_aff(bases + i);
+    st_aff(table + i, a);
+    st_aff(table + nsrs + i, glv_phi(a));
+    Xyzz acc = xyzz_from_aff(a);
+    for (int j = 1; j < W; j++) {
+        for (int k = 0; k < c; k++) acc = xyzz_dbl(acc);
+        a = xyzz_to_aff(acc);
+        st_aff(table + j * stride + i, a);
+        st_aff(table + j * stride + nsrs + i, glv_phi(a));
+    }
+}
+
+cudaError_t msm_table_build(Aff* table, const Aff* bases, uint32_t nsrs, int c, cudaStream_t st) {
+    if (nsrs == 0) return cudaSuccess;
+    msm_table_kernel<<<(nsrs + 127) / 128, 128, 0, st>>>(table, bases, nsrs, c, windows_for(c, true));
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------ planning
+
 
 static size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
@@ -441,14 +496,28 @@ static int pick_c(uint32_t n, bool glv) {
     return best;
 }
 
-MsmPlan msm_make_plan(uint32_t n, int c, bool glv) {
-    MsmPlan p;
-    p.n = n;
-    p.glv = glv ? 1 : 0;
-    p.c = (c >= 4 && c <= 22) ? c : pick_c(n, glv);
-    p.W = windows_for(p.c, glv);
+// over a table: every window's digits go into one bucket set, so the
+// reduction is paid once and there is no Horner chain.  A bucket costs about
+// five sorted entries (its reduction and the shorter runs of a wider key
+// space), fitted to B200 timings at 2^14..2^22 points.
+static int pick_c_table(uint32_t n) {
+    int best = 4;
+    double best_cost = 1e300;
+    for (int c = 4; c <= 22; c++) {
+        const double cost = 2.0 * n * windows_for(c, true) + 5.0 * (double)(1u << (c - 1));
+        if (cost < best_cost) {
+            best_cost = cost;
+            best = c;
+        }
+    }
+    return best;
+}
+
+int msm_table_default_window(uint32_t n) { return pick_c_table(n); }
+
+static void plan_finish(MsmPlan& p) {
     p.B = 1u << (p.c - 1);
-    p.NB = (uint32_t)p.W * p.B;
+    p.NB = (uint32_t)p.Wb * p.B;
     const uint64_t max_entries = msm_entry_count(p);
     const uint64_t target_threads = 148ull * 4 * 128;
     uint64_t L = (max_entries + target_threads - 1) / target_threads;
@@ -458,12 +527,41 @@ MsmPlan msm_make_plan(uint32_t n, int c, bool glv) {
     if (p.nacc == 0) p.nacc = 1;
     // up to ZK_MSM_REDUCE_THREADS reduction threads in total (the running-sum
     // segments are latency bound, so they need many threads), at most 4096 per
-    // window
+    // window when there is one bucket set per window
+    const uint32_t gcap = p.Wb == 1 ? ZK_MSM_REDUCE_THREADS : 4096;
     uint32_t G = 1;
-    while (G < 4096 && (uint64_t)G * 2 * p.W <= ZK_MSM_REDUCE_THREADS && G * 2 <= p.B) G *= 2;
+    while (G < gcap && (uint64_t)G * 2 * p.Wb <= ZK_MSM_REDUCE_THREADS && G * 2 <= p.B) G *= 2;
     p.G = G;
     p.seg = p.B / G;
+}
+
+MsmPlan msm_make_plan(uint32_t n, int c, bool glv) {
+    MsmPlan p;
+    p.n = n;
+    p.glv = glv ? 1 : 0;
+    p.c = (c >= 4 && c <= 22) ? c : pick_c(n, glv);
+    p.W = windows_for(p.c, glv);
+    p.Wb = p.W;
+    p.nsrs = 0;
+    plan_finish(p);
     return p;
+}
+
+MsmPlan msm_make_table_plan(uint32_t n, int c, uint32_t nsrs) {
+    MsmPlan p;
+    p.n = n;
+    p.glv = 1;
+    p.c = (c >= 4 && c <= 22) ? c : pick_c_table(n);
+    p.W = windows_for(p.c, true);
+    p.Wb = 1;
+    p.nsrs = nsrs;
+    plan_finish(p);
+    return p;
+}
+
+size_t msm_table_points(uint32_t nsrs, int c) {
+    if (c < 4 || c > 22) return 0;
+    return (size_t)windows_for(c, true) * 2 * nsrs;
 }
 
 size_t msm_u32_words(const MsmPlan& p) {
@@ -477,12 +575,15 @@ size_t msm_u32_words(const MsmPlan& p) {
 }
 
 size_t msm_point_count(const MsmPlan& p) {
-    return (size_t)2 * p.nacc + msm_merge_extra(p.nacc) + p.NB + (size_t)p.W * p.G + p.W;
+    return (size_t)2 * p.nacc + msm_merge_extra(p.nacc) + p.NB + (size_t)p.Wb * p.G + p.Wb;
 }
+
+// endomorphism images are made per call unless a table holds them
+static bool needs_phi(const MsmPlan& p) { return p.glv && !p.nsrs; }
 
 size_t msm_scratch_bytes(const MsmPlan& p) {
     return align_up(msm_u32_words(p) * 4, 256) + msm_point_count(p) * sizeof(Xyzz) +
-           (p.glv ? (size_t)p.n * sizeof(Aff) : 0);
+           (needs_phi(p) ? (size_t)p.n * sizeof(Aff) : 0);
 }
 
 void msm_layout_split(const MsmPlan& p, uint32_t* words, Xyzz* points, MsmScratch* s) {
@@ -502,10 +603,10 @@ void msm_layout_split(const MsmPlan& p, uint32_t* words, Xyzz* points, MsmScratc
     s->buckets = q;
     q += p.NB;
     s->segsum = q;
-    q += (size_t)p.W * p.G;
+    q += (size_t)p.Wb * p.G;
     s->winsum = q;
-    q += p.W;
-    s->phi = p.glv ? reinterpret_cast<Aff*>(q) : nullptr;
+    q += p.Wb;
+    s->phi = needs_phi(p) ? reinterpret_cast<Aff*>(q) : nullptr;
 }
 
 bool msm_layout_arenas(const MsmPlan& p, void* const* arena, const size_t* arena_bytes, int n_arenas,
@@ -524,9 +625,9 @@ bool msm_layout_arenas(const MsmPlan& p, void* const* arena, const size_t* arena
                         parts * 4,
                         parts * sizeof(Xyzz),
                         (size_t)p.NB * sizeof(Xyzz),
-                        (size_t)p.W * p.G * sizeof(Xyzz),
-                        (size_t)p.W * sizeof(Xyzz),
-                        p.glv ? (size_t)p.n * sizeof(Aff) : 0};
+                        (size_t)p.Wb * p.G * sizeof(Xyzz),
+                        (size_t)p.Wb * sizeof(Xyzz),
+                        needs_phi(p) ? (size_t)p.n * sizeof(Aff) : 0};
     int order[10];
     for (int i = 0; i < 10; i++) order[i] = i;
     for (int i = 1; i < 10; i++)
@@ -552,7 +653,7 @@ bool msm_layout_arenas(const MsmPlan& p, void* const* arena, const size_t* arena
         }
         if (a == n_arenas) return false;
     }
-    if (!p.glv) s->phi = nullptr;
+    if (!needs_phi(p)) s->phi = nullptr;
     return true;
 }
 
@@ -634,40 +735,47 @@ cudaError_t msm_run(Jac* out, const Aff* bases, const Fr* scalars, const MsmPlan
     }
     const uint32_t tb = 256;
     const uint32_t nblk = (p.n + tb - 1) / tb;
+    // over a table all windows share one bucket set and entry j 2 nsrs + i
+    // is base i times 2^(c j)
+    const uint32_t kw = p.nsrs ? 0u : p.B;
+    const uint32_t pw = p.nsrs ? 2 * p.nsrs : 0u;
+    const uint32_t phi_off = p.nsrs ? p.nsrs : p.n;
     ZK_CHECK(cudaMemsetAsync(s.count, 0, sizeof(uint32_t) * p.NB, st));
     if (p.glv)
-        msm_count_kernel<true><<<nblk, tb, 0, st>>>(scalars, p.n, p.c, p.W, s.count);
+        msm_count_kernel<true><<<nblk, tb, 0, st>>>(scalars, p.n, p.c, p.W, kw, s.count);
     else
-        msm_count_kernel<false><<<nblk, tb, 0, st>>>(scalars, p.n, p.c, p.W, s.count);
+        msm_count_kernel<false><<<nblk, tb, 0, st>>>(scalars, p.n, p.c, p.W, kw, s.count);
     ZK_CHECK(cudaGetLastError());
     ZK_CHECK(scan_u32(s.count, s.offset, p.NB, s.scan_tmp, st));
     if (p.glv) {
-        msm_scatter_kernel<true><<<nblk, tb, 0, st>>>(scalars, p.n, p.c, p.W, s.offset, s.count, s.entries);
+        msm_scatter_kernel<true><<<nblk, tb, 0, st>>>(scalars, p.n, p.c, p.W, kw, pw, phi_off, s.offset, s.count,
+                                                      s.entries);
         ZK_CHECK(cudaGetLastError());
-        msm_phi_kernel<<<nblk, tb, 0, st>>>(bases, p.n, s.phi);
+        if (needs_phi(p)) msm_phi_kernel<<<nblk, tb, 0, st>>>(bases, p.n, s.phi);
     } else {
-        msm_scatter_kernel<false><<<nblk, tb, 0, st>>>(scalars, p.n, p.c, p.W, s.offset, s.count, s.entries);
+        msm_scatter_kernel<false><<<nblk, tb, 0, st>>>(scalars, p.n, p.c, p.W, kw, pw, phi_off, s.offset, s.count,
+                                                       s.entries);
     }
     ZK_CHECK(cudaGetLastError());
     msm_accumulate_kernel<<<(p.nacc + 127) / 128, 128, 0, st>>>(s.entries, s.offset, p.NB, bases, s.phi,
-                                                                p.glv ? p.n : 0xffffffffu, p.L, p.nacc,
+                                                                needs_phi(p) ? p.n : 0xffffffffu, p.L, p.nacc,
                                                                 s.buckets, s.part_key, s.part_pt);
     ZK_CHECK(cudaGetLastError());
     ZK_CHECK(msm_merge(s.part_key, s.part_pt, p.nacc, s.buckets, st));
-    const uint32_t nred = (uint32_t)p.W * p.G;
-    msm_reduce_kernel<<<(nred + 127) / 128, 128, 0, st>>>(s.buckets, s.offset, p.W, p.B, p.seg, p.G, s.segsum);
+    const uint32_t nred = (uint32_t)p.Wb * p.G;
+    msm_reduce_kernel<<<(nred + 127) / 128, 128, 0, st>>>(s.buckets, s.offset, p.Wb, p.B, p.seg, p.G, s.segsum);
     ZK_CHECK(cudaGetLastError());
     // partial sums per window left by the reduce kernel's group trees
     const uint32_t parts = p.G < 128 ? 1u : p.G / 128u;
     const uint32_t wt = parts < 256 ? parts : 256;
-    msm_window_kernel<<<p.W, wt, (size_t)wt * sizeof(Xyzz), st>>>(s.segsum, parts, s.winsum);
+    msm_window_kernel<<<p.Wb, wt, (size_t)wt * sizeof(Xyzz), st>>>(s.segsum, parts, s.winsum);
     ZK_CHECK(cudaGetLastError());
     if (park_note) {
-        msm_park_kernel<<<1, 1, 0, st>>>(reinterpret_cast<MsmParked*>(park_note), (uint32_t)p.W, (uint32_t)p.c,
+        msm_park_kernel<<<1, 1, 0, st>>>(reinterpret_cast<MsmParked*>(park_note), (uint32_t)p.Wb, (uint32_t)p.c,
                                           s.winsum);
         return cudaGetLastError();
     }
-    msm_final_kernel<<<1, COOP_THREADS, 0, st>>>(s.winsum, p.W, p.c, out);
+    msm_final_kernel<<<1, COOP_THREADS, 0, st>>>(s.winsum, p.Wb, p.c, out);
     return cudaGetLastError();
 }
 

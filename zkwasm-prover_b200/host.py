@@ -198,6 +198,38 @@ def msm(points_buf, scalars_buf, n: int | None = None, window_bits: int = 0, scr
     return out
 
 
+def msm_table_build(bases_buf, nsrs: int | None = None, window_bits: int = 0, stream=None):
+    """zkp_msm_table_build: the table of pre-multiplied bases (and their
+    endomorphism images) for MSMs over the resident bases_buf[:nsrs];
+    window_bits 0 picks the library's width for nsrs points.  Returns
+    (table, window_bits)."""
+    nsrs = bases_buf.shape[0] if nsrs is None else nsrs
+    c = window_bits or lib().zkp_msm_table_default_window(nsrs)
+    nbytes = lib().zkp_msm_table_bytes(nsrs, c)
+    if nbytes == 0:
+        raise ValueError(f"unsupported table window width {c}")
+    table = torch.empty(nbytes // 8, dtype=torch.int64, device="cuda")
+    abi.check(lib().zkp_msm_table_build(ptr(table), ptr(bases_buf), nsrs, c, stream_handle(stream)),
+              "zkp_msm_table_build")
+    return table, c
+
+
+def msm_table(table, nsrs: int, window_bits: int, scalars_buf, n: int | None = None, scratch=None, out=None,
+              stream=None):
+    """One MSM over a table from msm_table_build (same nsrs and window_bits);
+    returns the 96-byte Jacobian result as a (12,) int64 device tensor."""
+    n = scalars_buf.shape[0] if n is None else n
+    if scratch is None:
+        nbytes = lib().zkp_msm_table_scratch_bytes(n, window_bits)
+        scratch = torch.empty(max(1, nbytes), dtype=torch.uint8, device="cuda")
+    if out is None:
+        out = torch.empty(12, dtype=torch.int64, device="cuda")
+    err = lib().zkp_msm_table(ptr(out), ptr(table), nsrs, window_bits, ptr(scalars_buf), n, ptr(scratch),
+                              scratch.numel(), stream_handle(stream))
+    abi.check(err, "zkp_msm_table")
+    return out
+
+
 def msm_batch(bases_buf, scalar_bufs, ns, windows=None, scratch=None, out=None, stream=None):
     """zkp_msm_batch: one pipeline for len(scalar_bufs) MSMs over the prefix
     bases_buf[:ns[i]]; returns (count, 12) int64 Jacobian points on the device."""
