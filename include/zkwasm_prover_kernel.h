@@ -244,6 +244,22 @@ cudaError_t zkp_msm_batch(void *out, const void *bases, const void *scalars, con
                           const int *window_bits, uint32_t count, void *scratch, size_t scratch_bytes,
                           cudaStream_t stream);
 
+/* Table width the library picks for a batch of `count` MSMs of n[i] points
+ * (host array) over one table. */
+int zkp_msm_batch_table_default_window(const uint32_t *n, uint32_t count);
+
+/* Scratch bytes of zkp_msm_batch_table for `count` MSMs of n[i] <= nsrs points
+ * (host array) over a table of width window_bits; 0 when they do not fit one
+ * pipeline. */
+size_t zkp_msm_batch_table_scratch_bytes(const uint32_t *n, uint32_t count, uint32_t nsrs, int window_bits);
+
+/* zkp_msm_batch over a table from zkp_msm_table_build (same nsrs and
+ * window_bits): out[i] = sum_{j < n[i]} [scalars[i][j]] bases_j, one bucket set
+ * per MSM, one counting sort and accumulation pass for the whole batch. */
+cudaError_t zkp_msm_batch_table(void *out, const void *table, uint32_t nsrs, int window_bits, const void *scalars,
+                                const uint32_t *n, uint32_t count, void *scratch, size_t scratch_bytes,
+                                cudaStream_t stream);
+
 /* Batched NTT of ncols columns (column c at buf + c * col_stride elements)
  * by the natural twiddle table `omegas` (2^log_n entries), optional output
  * scale.  *result_in_tmp (host) tells whether the result is in tmp. */

@@ -286,3 +286,52 @@ def test_msm_table_rejects_bad_arguments(gpu):
     # n above the table's points, and a table too large for 31-bit entry indices
     assert L.zkp_msm_table(1, 1, 10, 16, 1, 11, 1, 1 << 30, None) != 0
     assert L.zkp_msm_table_build(1, 1, 1 << 28, 4, None) != 0
+
+
+@pytest.mark.parametrize("c", [6, 13, 16])
+def test_msm_batch_table_uneven(O, gpu, c):
+    # the uneven batch of test_msm_batch_uneven over one table of the bases
+    H = gpu.host
+    nmax = 1 << 13
+    d = O.rand_fr(nmax, 191)
+    bases = H.to_device(O.g1_gen_bases(d))
+    table, _ = H.msm_table_build(bases, nmax, c)
+    rng = np.random.default_rng(192)
+    ns = [nmax, 1000, 1, 0, 4096, 300, 2048, 5000]
+    cols = []
+    for i, n in enumerate(ns):
+        s = O.rand_fr(max(n, 1), 300 + i)[:n]
+        if i == 4:
+            s = O.fr_vec([int(x) for x in rng.integers(0, 1 << 20, n)])
+        if i == 6:
+            s[rng.random(n) < 0.9] = 0
+        if i == 7:
+            s[:2000] = s[0]                    # one bucket per window holds 2000 points
+        cols.append(s)
+    dev_cols = [H.to_device(x) if x.shape[0] else H.empty_fr(1) for x in cols]
+    out = H.msm_batch_table(table, nmax, c, dev_cols, ns)
+    torch.cuda.synchronize()
+    got = H.to_host(out)
+    for i, (n, s) in enumerate(zip(ns, cols)):
+        exp = O.msm_known_dlog(d[:n], s) if n else np.zeros((1, 8), np.uint64)
+        assert (_jac_to_aff(O, got[i]) == exp).all(), i
+
+
+def test_msm_batch_table_many(O, gpu):
+    # 300 MSMs share the reduction-thread budget (a few threads per bucket set)
+    H = gpu.host
+    nmax = 2048
+    d = O.rand_fr(nmax, 193)
+    bases = H.to_device(O.g1_gen_bases(d))
+    c = 15
+    table, _ = H.msm_table_build(bases, nmax, c)
+    rng = np.random.default_rng(194)
+    ns = [int(x) for x in rng.integers(1, nmax + 1, 300)]
+    cols = [O.rand_fr(n, 400 + i) for i, n in enumerate(ns)]
+    out = H.msm_batch_table(table, nmax, c, [H.to_device(x) for x in cols], ns)
+    plain = H.msm_batch(bases, [H.to_device(x) for x in cols], ns, [c] * len(ns))
+    torch.cuda.synchronize()
+    got, ref = H.to_host(out), H.to_host(plain)
+    for i in (0, 1, 150, 299):
+        assert (_jac_to_aff(O, got[i]) == O.msm_known_dlog(d[:ns[i]], cols[i])).all(), i
+    assert (_jac_to_aff(O, got) == _jac_to_aff(O, ref)).all()

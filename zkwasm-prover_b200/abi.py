@@ -57,6 +57,9 @@ SIGNATURES = {
     "zkp_msm_table_build": [P, P, U, I, S],
     "zkp_msm_table_scratch_bytes": ([U, I], SZ),
     "zkp_msm_table": [P, P, U, I, P, U, P, SZ, S],
+    "zkp_msm_batch_table_default_window": ([P, U], I),
+    "zkp_msm_batch_table_scratch_bytes": ([P, U, U, I], SZ),
+    "zkp_msm_batch_table": [P, P, U, I, P, P, U, P, SZ, S],
     "zkp_msm_batch_scratch_bytes": ([P, P, U], SZ),
     "zkp_msm_batch": [P, P, P, P, P, U, P, SZ, S],
     "zkp_ntt_batch": [P, P, P, P, I, U, SZ, P, S],

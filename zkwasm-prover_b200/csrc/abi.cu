@@ -400,6 +400,27 @@ cudaError_t zkp_msm_batch(void* out, const void* bases, const void* scalars, con
                          stream);
 }
 
+int zkp_msm_batch_table_default_window(const uint32_t* n, uint32_t count) {
+    if (!n || count == 0) return msm_table_default_window(0);
+    return msm_batch_table_default_window(n, count);
+}
+
+size_t zkp_msm_batch_table_scratch_bytes(const uint32_t* n, uint32_t count, uint32_t nsrs, int window_bits) {
+    if (!n || nsrs == 0 || !table_fits(nsrs, window_bits)) return 0;
+    return msm_batch_scratch_bytes(n, &window_bits, count, nsrs);
+}
+
+cudaError_t zkp_msm_batch_table(void* out, const void* table, uint32_t nsrs, int window_bits, const void* scalars,
+                                const uint32_t* n, uint32_t count, void* scratch, size_t scratch_bytes,
+                                cudaStream_t stream) {
+    if (count == 0) return cudaSuccess;
+    if (!out || !table || !scalars || !n || !scratch || nsrs == 0) return cudaErrorInvalidValue;
+    if (!table_fits(nsrs, window_bits)) return cudaErrorInvalidValue;
+    return msm_batch_run(reinterpret_cast<Jac*>(out), reinterpret_cast<const Aff*>(table),
+                         reinterpret_cast<const Fr* const*>(scalars), n, &window_bits, count, scratch, scratch_bytes,
+                         stream, nsrs);
+}
+
 cudaError_t zkp_ntt_batch(void* buf, void* tmp, const void* omegas, const void* scale, int log_n, uint32_t ncols,
                           size_t col_stride, int* result_in_tmp, cudaStream_t stream) {
     if (log_n < 1 || log_n > 28 || !buf || !omegas || !result_in_tmp || ncols == 0 || ncols > 65535)

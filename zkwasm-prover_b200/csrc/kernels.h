@@ -85,6 +85,7 @@ MsmPlan msm_make_plan(uint32_t n, int c, bool glv = true);
 MsmPlan msm_make_table_plan(uint32_t n, int c, uint32_t nsrs);
 // window bits the library picks for an MSM of n points over a table
 int msm_table_default_window(uint32_t n);
+int msm_batch_table_default_window(const uint32_t* n, uint32_t count);
 // Table of pre-multiplied bases: for window j < W (W = ceil(128 / c)) and
 // i < nsrs, entry j 2 nsrs + i is [2^(c j)] base_i and entry
 // j 2 nsrs + nsrs + i its endomorphism image, as affine points.
@@ -122,9 +123,11 @@ cudaError_t msm_accumulate_merge(const uint32_t* entries, const uint32_t* offset
 // phi[i] = (beta x_i, y_i) for i < n
 cudaError_t msm_phi(const Aff* bases, uint32_t n, Aff* phi, cudaStream_t st);
 
-size_t msm_batch_scratch_bytes(const uint32_t* n, const int* c, uint32_t count);
+// nsrs > 0: bases is a table of pre-multiplied bases (msm_table_build with
+// nsrs points and width c[0]) and every MSM runs over it with that width
+size_t msm_batch_scratch_bytes(const uint32_t* n, const int* c, uint32_t count, uint32_t nsrs = 0);
 cudaError_t msm_batch_run(Jac* out, const Aff* bases, const Fr* const* scalars, const uint32_t* n, const int* c,
-                          uint32_t count, void* scratch, size_t scratch_bytes, cudaStream_t st);
+                          uint32_t count, void* scratch, size_t scratch_bytes, cudaStream_t st, uint32_t nsrs = 0);
 
 // ------------------------------------------------------------------ scans
 size_t scan_tmp_words(uint32_t n);

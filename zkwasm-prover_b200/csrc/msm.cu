@@ -184,6 +184,11 @@ __global__ void __launch_bounds__(128) msm_accumulate_kernel(const uint32_t* __r
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= nacc) return;
     const uint32_t total = offset[NB];
+    // L covers the plan's largest entry count; zero digits (sparse or small
+    // scalars) leave fewer entries, which are spread over all nacc threads
+    // instead of the first total / L of them
+    const uint32_t fair = (total + nacc - 1) / nacc;
+    L = min(L, max(fair, 8u));
     const uint32_t s = t * L;
     uint32_t head_key = KEY_NONE, tail_key = KEY_NONE;
     if (s < total) {
@@ -514,6 +519,22 @@ static int pick_c_table(uint32_t n) {
 }
 
 int msm_table_default_window(uint32_t n) { return pick_c_table(n); }
+
+// one width for a batch over one table: each MSM has its own bucket set
+int msm_batch_table_default_window(const uint32_t* n, uint32_t count) {
+    double pts = 0;
+    for (uint32_t i = 0; i < count; i++) pts += 2.0 * n[i];
+    int best = 4;
+    double best_cost = 1e300;
+    for (int c = 4; c <= 22; c++) {
+        const double cost = pts * windows_for(c, true) + 5.0 * count * (double)(1u << (c - 1));
+        if (cost < best_cost) {
+            best_cost = cost;
+            best = c;
+        }
+    }
+    return best;
+}
 
 static void plan_finish(MsmPlan& p) {
     p.B = 1u << (p.c - 1);

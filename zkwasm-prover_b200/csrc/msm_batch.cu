@@ -20,6 +20,8 @@ namespace zk {
 
 struct BatchDesc {
     uint32_t n, c, W, B;
+    uint32_t Wb;       // bucket sets: W, or 1 over a table of pre-multiplied bases
+    uint32_t kw;       // key stride per window: B, or 0 over a table
     uint32_t key_off;  // first bucket key of this MSM
     uint32_t sc_off;   // first global scalar index of this MSM
     uint32_t G, seg;   // reduction segments per window and buckets per segment
@@ -42,8 +44,10 @@ __device__ __forceinline__ uint32_t find_desc(const BatchDesc* d, uint32_t count
 }
 
 // Every MSM of the batch runs on GLV halves: scalar j of an MSM becomes
-// |k1| on base j and |k2| on phi(base j), stored at point nmax + j (nmax: the
-// longest MSM's base prefix, whose images are computed once).
+// |k1| on base j and |k2| on phi(base j), stored at point phi_off + j
+// (phi_off = nmax, the longest MSM's base prefix, whose images are computed
+// once; or nsrs over a table, whose window j entry of point p sits at
+// p + j pw).
 
 __device__ __forceinline__ void batch_count_half(const uint32_t v[8], const BatchDesc& q, uint32_t* cnt) {
     uint32_t carry = 0;
@@ -51,7 +55,7 @@ __device__ __forceinline__ void batch_count_half(const uint32_t v[8], const Batc
         const int dg = msm_signed_digit(v, (int)w, (int)q.c, carry);
         if (dg != 0) {
             const uint32_t mag = dg > 0 ? (uint32_t)dg : (uint32_t)(-dg);
-            atomicAdd(&cnt[q.key_off + w * q.B + mag - 1], 1u);
+            atomicAdd(&cnt[q.key_off + w * q.kw + mag - 1], 1u);
         }
     }
 }
@@ -72,7 +76,7 @@ __global__ void batch_count_kernel(const BatchDesc* d, uint32_t count, const Fr*
 
 // as scatter_digits of the single MSM: eight slot claims in flight together
 __device__ __forceinline__ void batch_scatter_half(const uint32_t v[8], const BatchDesc& q, uint32_t point,
-                                                   bool negate, const uint32_t* offset, uint32_t* cnt,
+                                                   uint32_t pw, bool negate, const uint32_t* offset, uint32_t* cnt,
                                                    uint32_t* entries) {
     const uint32_t nbit = negate ? 0x80000000u : 0u;
     uint32_t carry = 0;
@@ -86,7 +90,7 @@ __device__ __forceinline__ void batch_scatter_half(const uint32_t v[8], const Ba
                 const int dg = msm_signed_digit(v, (int)(w0 + u), (int)q.c, carry);
                 if (dg != 0) {
                     const uint32_t mag = dg > 0 ? (uint32_t)dg : (uint32_t)(-dg);
-                    key[u] = q.key_off + (w0 + u) * q.B + mag - 1;
+                    key[u] = q.key_off + (w0 + u) * q.kw + mag - 1;
                     neg[u] = (dg < 0 ? 0x80000000u : 0u) ^ nbit;
                 }
             }
@@ -100,12 +104,13 @@ __device__ __forceinline__ void batch_scatter_half(const uint32_t v[8], const Ba
         }
 #pragma unroll
         for (uint32_t u = 0; u < 8; u++)
-            if (key[u] != 0xffffffffu) entries[base[u] + slot[u]] = point | neg[u];
+            if (key[u] != 0xffffffffu) entries[base[u] + slot[u]] = (point + (w0 + u) * pw) | neg[u];
     }
 }
 
 __global__ void batch_scatter_kernel(const BatchDesc* d, uint32_t count, const Fr* const* scalars, uint32_t total,
-                                     uint32_t nmax, const uint32_t* offset, uint32_t* cnt, uint32_t* entries) {
+                                     uint32_t phi_off, uint32_t pw, const uint32_t* offset, uint32_t* cnt,
+                                     uint32_t* entries) {
     for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < total; s += gridDim.x * blockDim.x) {
         const uint32_t i = find_desc<&BatchDesc::sc_off>(d, count, s);
         const BatchDesc q = d[i];
@@ -114,8 +119,8 @@ __global__ void batch_scatter_kernel(const BatchDesc* d, uint32_t count, const F
         uint32_t m1[8], m2[8];
         bool n1, n2;
         glv_split(k.v, m1, m2, n1, n2);
-        batch_scatter_half(m1, q, j, n1, offset, cnt, entries);
-        batch_scatter_half(m2, q, nmax + j, n2, offset, cnt, entries);
+        batch_scatter_half(m1, q, j, pw, n1, offset, cnt, entries);
+        batch_scatter_half(m2, q, phi_off + j, pw, n2, offset, cnt, entries);
     }
 }
 
@@ -131,7 +136,7 @@ __global__ void __launch_bounds__(128) batch_reduce_kernel(const BatchDesc* d, u
     const BatchDesc q = d[i];
     const uint32_t lt = t - q.red_off;
     Xyzz S = xyzz_identity();
-    if (t < total && lt < q.W * q.G) {
+    if (t < total && lt < q.Wb * q.G) {
         const uint32_t w = lt / q.G, g = lt % q.G;
         const uint32_t lo = g * q.seg;
         Xyzz T = xyzz_identity();
@@ -150,10 +155,10 @@ __global__ void __launch_bounds__(128) batch_reduce_kernel(const BatchDesc* d, u
         if ((k & (GS - 1)) < h) sm[k] = xyzz_add(sm[k], sm[k + h]);
         __syncthreads();
     }
-    if ((k & (GS - 1)) == 0 && t < total && lt < q.W * q.G) st_xyzz(segsum + q.red_off + lt / GS, sm[k]);
+    if ((k & (GS - 1)) == 0 && t < total && lt < q.Wb * q.G) st_xyzz(segsum + q.red_off + lt / GS, sm[k]);
 }
 
-// one CTA per (MSM, window): adds the window's G / min(G, 128) group sums,
+// one CTA per (MSM, bucket set): adds the set's G / min(G, 128) group sums,
 // each thread a strided subset first, then a tree (blockDim a power of two)
 __global__ void __launch_bounds__(256) batch_window_kernel(const BatchDesc* d, uint32_t count, const Xyzz* segsum, Xyzz* winsum) {
     extern __shared__ uint4 smem_u4[];
@@ -180,7 +185,7 @@ __global__ void __launch_bounds__(COOP_THREADS) batch_final_kernel(const BatchDe
     __shared__ Fq buf[8];
     const uint32_t i = blockIdx.x;
     const BatchDesc q = d[i];
-    const Jac j = coop_horner(buf, winsum + q.win_off, q.n ? (int)q.W : 0, (int)q.c);
+    const Jac j = coop_horner(buf, winsum + q.win_off, q.n ? (int)q.Wb : 0, (int)q.c);
     if (threadIdx.x == 0) {
         st_elem<FqCfg>(&out[i].x, j.x);
         st_elem<FqCfg>(&out[i].y, j.y);
@@ -200,16 +205,45 @@ struct BatchLayout {
 
 static size_t al(size_t x) { return (x + 255) / 256 * 256; }
 
-static bool batch_plan(const uint32_t* n, const int* c, uint32_t count, BatchLayout& L) {
+#ifndef ZK_MSM_BATCH_REDUCE_THREADS
+#define ZK_MSM_BATCH_REDUCE_THREADS 131072
+#endif
+static constexpr uint64_t BATCH_REDUCE_THREADS = ZK_MSM_BATCH_REDUCE_THREADS;
+
+// nsrs > 0: every MSM runs over one table of pre-multiplied bases of width
+// c[0] (one bucket set per MSM); otherwise per-MSM widths c[i] (0 or a null c:
+// the library's choice) over the bases and their images
+static bool batch_plan(const uint32_t* n, const int* c, uint32_t count, uint32_t nsrs, BatchLayout& L) {
     L.desc.resize(count);
+    std::vector<MsmPlan> plans(count);
+    uint64_t all_buckets = 0;
+    for (uint32_t i = 0; i < count; i++) {
+        if (nsrs && n[i] > nsrs) return false;
+        plans[i] = nsrs ? msm_make_table_plan(n[i], c[0], nsrs) : msm_make_plan(n[i], c ? c[i] : 0, true);
+        all_buckets += (uint64_t)plans[i].Wb * plans[i].B;
+    }
+    // The reduction threads of the whole batch share one budget, in
+    // proportion to each MSM's buckets: a segment's closing product lo * T
+    // costs about 1.5 c additions, so many MSMs with the single-MSM thread
+    // counts would spend more on those than on the running sums themselves.
+    for (uint32_t i = 0; i < count; i++) {
+        MsmPlan& p = plans[i];
+        const uint64_t share = BATCH_REDUCE_THREADS * (uint64_t)p.Wb * p.B / (all_buckets ? all_buckets : 1);
+        uint32_t G = 1;
+        while ((uint64_t)G * 2 * p.Wb <= share && G * 2 <= p.G) G *= 2;
+        p.G = G;
+        p.seg = p.B / G;
+    }
     uint64_t key = 0, sc = 0, red = 0, win = 0, ent = 0;
     for (uint32_t i = 0; i < count; i++) {
-        const MsmPlan p = msm_make_plan(n[i], c ? c[i] : 0, true);
+        const MsmPlan& p = plans[i];
         BatchDesc& q = L.desc[i];
         q.n = n[i];
         q.c = (uint32_t)p.c;
         q.W = (uint32_t)p.W;
         q.B = p.B;
+        q.Wb = (uint32_t)p.Wb;
+        q.kw = nsrs ? 0u : p.B;
         q.key_off = (uint32_t)key;
         q.sc_off = (uint32_t)sc;
         q.G = p.G;
@@ -217,11 +251,11 @@ static bool batch_plan(const uint32_t* n, const int* c, uint32_t count, BatchLay
         red = (red + 127) / 128 * 128;  // each MSM's reduction threads start a CTA
         q.red_off = (uint32_t)red;
         q.win_off = (uint32_t)win;
-        key += (uint64_t)p.W * p.B;
+        key += (uint64_t)p.Wb * p.B;
         sc += n[i];
-        red += (uint64_t)p.W * p.G;
+        red += (uint64_t)p.Wb * p.G;
         red = (red + 127) / 128 * 128;
-        win += p.W;
+        win += p.Wb;
         ent += msm_entry_count(p);
         if (p.G > L.maxG) L.maxG = p.G;
         if (n[i] > L.nmax) L.nmax = n[i];
@@ -262,22 +296,22 @@ static bool batch_plan(const uint32_t* n, const int* c, uint32_t count, BatchLay
     L.off_winsum = o;
     o = al(o + (size_t)L.win_total * sizeof(Xyzz));
     L.off_phi = o;
-    o = al(o + (size_t)L.nmax * sizeof(Aff));
+    o = al(o + (nsrs ? 0 : (size_t)L.nmax * sizeof(Aff)));
     L.bytes = o;
     return true;
 }
 
-size_t msm_batch_scratch_bytes(const uint32_t* n, const int* c, uint32_t count) {
+size_t msm_batch_scratch_bytes(const uint32_t* n, const int* c, uint32_t count, uint32_t nsrs) {
     BatchLayout L;
-    if (count == 0 || !batch_plan(n, c, count, L)) return 0;
+    if (count == 0 || !batch_plan(n, c, count, nsrs, L)) return 0;
     return L.bytes;
 }
 
 cudaError_t msm_batch_run(Jac* out, const Aff* bases, const Fr* const* scalars, const uint32_t* n, const int* c,
-                          uint32_t count, void* scratch, size_t scratch_bytes, cudaStream_t st) {
+                          uint32_t count, void* scratch, size_t scratch_bytes, cudaStream_t st, uint32_t nsrs) {
     if (count == 0) return cudaSuccess;
     BatchLayout L;
-    if (!batch_plan(n, c, count, L)) return cudaErrorInvalidValue;
+    if (!batch_plan(n, c, count, nsrs, L)) return cudaErrorInvalidValue;
     if (L.bytes > scratch_bytes) return cudaErrorInvalidValue;
     char* base = reinterpret_cast<char*>(scratch);
     BatchDesc* d = reinterpret_cast<BatchDesc*>(base + L.off_desc);
@@ -301,10 +335,18 @@ cudaError_t msm_batch_run(Jac* out, const Aff* bases, const Fr* const* scalars, 
     batch_count_kernel<<<g1, 256, 0, st>>>(d, count, scalars, L.total, cnt);
     ZK_CHECK(cudaGetLastError());
     ZK_CHECK(scan_u32(cnt, offset, L.NB, scan, st));
-    batch_scatter_kernel<<<g1, 256, 0, st>>>(d, count, scalars, L.total, L.nmax, offset, cnt, entries);
+    batch_scatter_kernel<<<g1, 256, 0, st>>>(d, count, scalars, L.total, nsrs ? nsrs : L.nmax, 2 * nsrs, offset,
+                                             cnt, entries);
     ZK_CHECK(cudaGetLastError());
-    ZK_CHECK(msm_phi(bases, L.nmax, phi, st));
-    ZK_CHECK(msm_accumulate_merge(entries, offset, L.NB, bases, phi, L.nmax, L.L, L.nacc, buckets, pkey, ppt, st));
+    if (nsrs) {
+        // bases is the table: every entry indexes it directly
+        ZK_CHECK(msm_accumulate_merge(entries, offset, L.NB, bases, nullptr, 0xffffffffu, L.L, L.nacc, buckets, pkey,
+                                      ppt, st));
+    } else {
+        ZK_CHECK(msm_phi(bases, L.nmax, phi, st));
+        ZK_CHECK(
+            msm_accumulate_merge(entries, offset, L.NB, bases, phi, L.nmax, L.L, L.nacc, buckets, pkey, ppt, st));
+    }
     batch_reduce_kernel<<<(L.red_total + 127) / 128, 128, 0, st>>>(d, count, L.red_total, buckets, offset, segsum);
     ZK_CHECK(cudaGetLastError());
     const uint32_t max_parts = L.maxG < 128 ? 1u : L.maxG / 128u;

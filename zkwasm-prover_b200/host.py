@@ -230,6 +230,26 @@ def msm_table(table, nsrs: int, window_bits: int, scalars_buf, n: int | None = N
     return out
 
 
+def msm_batch_table(table, nsrs: int, window_bits: int, scalar_bufs, ns, scratch=None, out=None, stream=None):
+    """zkp_msm_batch_table: len(scalar_bufs) MSMs over prefixes of the bases
+    of one table (msm_table_build); returns (count, 12) int64 Jacobian points."""
+    count = len(scalar_bufs)
+    n_arr = (ctypes.c_uint32 * count)(*[int(x) for x in ns])
+    ptrs = ptr_array(scalar_bufs)
+    if scratch is None:
+        nbytes = lib().zkp_msm_batch_table_scratch_bytes(ctypes.addressof(n_arr), count, nsrs, window_bits)
+        if nbytes == 0:
+            raise ValueError("batch does not fit one table pipeline")
+        scratch = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+    if out is None:
+        out = torch.empty((count, 12), dtype=torch.int64, device="cuda")
+    err = lib().zkp_msm_batch_table(ptr(out), ptr(table), nsrs, window_bits, ptr(ptrs), ctypes.addressof(n_arr),
+                                    count, ptr(scratch), scratch.numel(), stream_handle(stream))
+    abi.check(err, "zkp_msm_batch_table")
+    out._keep = (ptrs, scratch)
+    return out
+
+
 def msm_batch(bases_buf, scalar_bufs, ns, windows=None, scratch=None, out=None, stream=None):
     """zkp_msm_batch: one pipeline for len(scalar_bufs) MSMs over the prefix
     bases_buf[:ns[i]]; returns (count, 12) int64 Jacobian points on the device."""
