@@ -139,11 +139,34 @@ extern "C" void hc_glv_phi(uint64_t* out, const uint64_t* pts, long n) {
     }
 }
 
-// lazily reduced Fr operations on inputs in [0, 2r): op 0 mul, 1 add, 2 sub
+// lazily reduced operations on inputs in [0, 2m): op 0 mul, 1 add, 2 sub over
+// Fr; 3, 4, 5 the same over Fq
+template <class C>
+static Fe<C> lazy_op(int op, const Fe<C>& x, const Fe<C>& y) {
+    return op == 0 ? fe_mul_lazy<C>(x, y) : op == 1 ? fe_add_lazy<C>(x, y) : fe_sub_lazy<C>(x, y);
+}
+
 extern "C" void hc_lazy(int op, uint64_t* out, const uint64_t* a, const uint64_t* b, long n) {
     for (long i = 0; i < n; i++) {
-        const Fr x = ld<FrCfg>(a + 4 * i), y = ld<FrCfg>(b + 4 * i);
-        st(out + 4 * i, op == 0 ? fe_mul_lazy<FrCfg>(x, y) : op == 1 ? fe_add_lazy<FrCfg>(x, y)
-                                                                      : fe_sub_lazy<FrCfg>(x, y));
+        if (op < 3)
+            st(out + 4 * i, lazy_op<FrCfg>(op, ld<FrCfg>(a + 4 * i), ld<FrCfg>(b + 4 * i)));
+        else
+            st(out + 4 * i, lazy_op<FqCfg>(op - 3, ld<FqCfg>(a + 4 * i), ld<FqCfg>(b + 4 * i)));
     }
+}
+
+// a chain of n lazily reduced mixed additions onto acc (16 words, coordinates
+// in [0, 2p)), canonical result
+extern "C" void hc_madd_lazy_chain(uint64_t* out, const uint64_t* acc, const uint64_t* pts, long n) {
+    Xyzz a;
+    a.x = ld<FqCfg>(acc);
+    a.y = ld<FqCfg>(acc + 4);
+    a.zz = ld<FqCfg>(acc + 8);
+    a.zzz = ld<FqCfg>(acc + 12);
+    for (long i = 0; i < n; i++) a = xyzz_add_aff_lazy(a, ld<FqCfg>(pts + 8 * i), ld<FqCfg>(pts + 8 * i + 4));
+    a = xyzz_canon(a);
+    st(out, a.x);
+    st(out + 4, a.y);
+    st(out + 8, a.zz);
+    st(out + 12, a.zzz);
 }

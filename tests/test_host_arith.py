@@ -35,6 +35,7 @@ def hc():
         "hc_xyzz_to_jac": [P, P],
         "hc_glv_split": [P, P, P, P, ctypes.c_long],
         "hc_lazy": [ctypes.c_int, P, P, P, ctypes.c_long],
+        "hc_madd_lazy_chain": [P, P, P, ctypes.c_long],
         "hc_glv_phi": [P, P, ctypes.c_long],
     }.items():
         getattr(L, name).argtypes = args
@@ -199,11 +200,11 @@ def test_glv_phi_is_lambda_multiple(O, hc):
     assert (out == O.g1_gen_bases(lam)).all()
 
 
-@pytest.mark.parametrize("op", [0, 1, 2])
+@pytest.mark.parametrize("op", [0, 1, 2, 3, 4, 5])
 def test_lazy_fr_ops(O, hc, op):
-    # representatives in [0, 2r): results stay below 2r and are congruent to
-    # the exact Montgomery product / sum / difference
-    r = O.R_MOD
+    # representatives in [0, 2m): results stay below 2m and are congruent to
+    # the exact Montgomery product / sum / difference (ops 3-5: over Fq)
+    r = O.R_MOD if op < 3 else O.Q_MOD
     rng = random.Random(40 + op)
     xs = [0, 1, r - 1, r, r + 1, 2 * r - 1] + [rng.randrange(2 * r) for _ in range(2000)]
     ys = [2 * r - 1, r, 1, 0, r - 1, 2 * r - 1] + [rng.randrange(2 * r) for _ in range(2000)]
@@ -215,5 +216,36 @@ def test_lazy_fr_ops(O, hc, op):
     rinv = pow(1 << 256, -1, r)
     for i, (x, y) in enumerate(zip(xs, ys)):
         got = sum(int(out[i, j]) << (64 * j) for j in range(4))
-        exp = x * y * rinv if op == 0 else x + y if op == 1 else x - y
+        exp = x * y * rinv if op % 3 == 0 else x + y if op % 3 == 1 else x - y
         assert got < 2 * r and (got - exp) % r == 0
+
+
+def test_madd_lazy_chain(O, hc):
+    # mixed additions on [0, 2p) coordinates (the accumulation loop's form)
+    # equal the canonical chain, including the doubling and P + (-P) branches
+    ks = O.rand_fr(40, 47)
+    pts = O.g1_gen_bases(ks)
+    pts[7] = pts[6]                            # equal points: doubling branch
+    pts[9] = pts[8]
+    pts[9, 4:] = O.neg(pts[8][4:], 1)          # P + (-P) after the run so far
+    acc = np.zeros(16, np.uint64)
+    for p in pts:
+        out = np.empty(16, np.uint64)
+        hc.hc_xyzz_add_aff(_p(out), _p(acc), _p(np.ascontiguousarray(p)))
+        acc = out
+    got = np.empty(16, np.uint64)
+    hc.hc_madd_lazy_chain(_p(got), _p(np.zeros(16, np.uint64)), _p(np.ascontiguousarray(pts)), pts.shape[0])
+    assert (got == acc).all()
+    # a start point whose coordinates are lifted to [p, 2p)
+    start = _xyzz(hc, pts[0])
+    lifted = start.copy()
+    for k in range(4):
+        v = sum(int(start[4 * k + j]) << (64 * j) for j in range(4)) + O.Q_MOD
+        lifted[4 * k: 4 * k + 4] = [(v >> (64 * j)) & (2 ** 64 - 1) for j in range(4)]
+    ref = start
+    for p in pts[1:20]:
+        out = np.empty(16, np.uint64)
+        hc.hc_xyzz_add_aff(_p(out), _p(ref), _p(np.ascontiguousarray(p)))
+        ref = out
+    hc.hc_madd_lazy_chain(_p(got), _p(lifted), _p(np.ascontiguousarray(pts[1:20])), 19)
+    assert (got == ref).all()

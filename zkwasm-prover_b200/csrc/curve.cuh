@@ -20,14 +20,19 @@ namespace zk {
 // out-of-line function: a mixed addition alone is ten products of ~350
 // instructions each, and inlining every product of the accumulation loop
 // overflows the instruction cache.
+// cmul_lazy leaves out the final subtraction: for inputs below 2p the result
+// is below 2p and congruent to the product (4p < 2^256).
 #if defined(__CUDA_ARCH__)
 #if defined(ZK_CURVE_INLINE_MUL)
 __device__ __forceinline__ Fq cmul(const Fq& a, const Fq& b) { return fe_mul<FqCfg>(a, b); }
+__device__ __forceinline__ Fq cmul_lazy(const Fq& a, const Fq& b) { return fe_mul_lazy<FqCfg>(a, b); }
 #else
 __device__ __noinline__ Fq cmul(const Fq a, const Fq b) { return fe_mul<FqCfg>(a, b); }
+__device__ __noinline__ Fq cmul_lazy(const Fq a, const Fq b) { return fe_mul_lazy<FqCfg>(a, b); }
 #endif
 #else
 inline Fq cmul(const Fq& a, const Fq& b) { return fe_mul<FqCfg>(a, b); }
+inline Fq cmul_lazy(const Fq& a, const Fq& b) { return fe_mul_lazy<FqCfg>(a, b); }
 #endif
 
 struct Aff {
@@ -70,9 +75,11 @@ ZK_HD Xyzz xyzz_from_aff(const Aff& a) {
 // independent products of one formula.
 struct CurveMul {
     static ZK_HD Fq mul(const Fq& a, const Fq& b) { return cmul(a, b); }
+    static ZK_HD Fq mul_lazy(const Fq& a, const Fq& b) { return cmul_lazy(a, b); }
 };
 struct CurveMulInline {
     static ZK_HD Fq mul(const Fq& a, const Fq& b) { return fe_mul<FqCfg>(a, b); }
+    static ZK_HD Fq mul_lazy(const Fq& a, const Fq& b) { return fe_mul_lazy<FqCfg>(a, b); }
 };
 
 // 2 * (x, y) for affine (x, y), as XYZZ (mdbl-2008-s-1)
@@ -137,6 +144,50 @@ ZK_HD Xyzz xyzz_add_aff(const Xyzz& p, const Fq& x2, const Fq& y2) {
     r.y = fe_sub<FqCfg>(M::mul(rr, fe_sub<FqCfg>(q, r.x)), M::mul(p.y, ppp));
     r.zz = M::mul(p.zz, pp);
     r.zzz = M::mul(p.zzz, ppp);
+    return r;
+}
+
+// madd-2008-s on lazily reduced coordinates: p's coordinates lie in [0, 2p)
+// (congruent to the exact ones), (x2, y2) is canonical and not the identity,
+// and so are the result's coordinates.  Products skip their final subtraction
+// and sums and differences work modulo 2p; the equal-x test reduces first.
+// A non-identity p never has zz = 0 mod p, so the identity stays zz = 0.
+template <class M = CurveMul>
+ZK_HD Xyzz xyzz_add_aff_lazy(const Xyzz& p, const Fq& x2, const Fq& y2) {
+    if (xyzz_is_id(p)) {
+        Xyzz r;
+        r.x = x2;
+        r.y = y2;
+        r.zz = fe_one<FqCfg>();
+        r.zzz = fe_one<FqCfg>();
+        return r;
+    }
+    Fq u2 = M::mul_lazy(x2, p.zz);
+    Fq s2 = M::mul_lazy(y2, p.zzz);
+    Fq pp_ = fe_sub_lazy<FqCfg>(u2, p.x);
+    Fq rr = fe_sub_lazy<FqCfg>(s2, p.y);
+    if (fe_is_zero<FqCfg>(fe_canon<FqCfg>(pp_))) {
+        if (fe_is_zero<FqCfg>(fe_canon<FqCfg>(rr))) return aff_dbl<M>(x2, y2);
+        return xyzz_identity();
+    }
+    Fq pp = M::mul_lazy(pp_, pp_);
+    Fq ppp = M::mul_lazy(pp_, pp);
+    Fq q = M::mul_lazy(p.x, pp);
+    Xyzz r;
+    r.x = fe_sub_lazy<FqCfg>(fe_sub_lazy<FqCfg>(fe_sub_lazy<FqCfg>(M::mul_lazy(rr, rr), ppp), q), q);
+    r.y = fe_sub_lazy<FqCfg>(M::mul_lazy(rr, fe_sub_lazy<FqCfg>(q, r.x)), M::mul_lazy(p.y, ppp));
+    r.zz = M::mul_lazy(p.zz, pp);
+    r.zzz = M::mul_lazy(p.zzz, ppp);
+    return r;
+}
+
+// canonical coordinates of a lazily reduced point
+ZK_HD Xyzz xyzz_canon(const Xyzz& p) {
+    Xyzz r;
+    r.x = fe_canon<FqCfg>(p.x);
+    r.y = fe_canon<FqCfg>(p.y);
+    r.zz = fe_canon<FqCfg>(p.zz);
+    r.zzz = fe_canon<FqCfg>(p.zzz);
     return r;
 }
 

@@ -212,11 +212,12 @@ __global__ void __launch_bounds__(128) msm_accumulate_kernel(const uint32_t* __r
             Aff a = ld_aff(entry_point(bases, phi, nbase, ent & 0x7fffffffu));
             if (!aff_is_id(a)) {
                 if (ent >> 31) a.y = fe_neg<FqCfg>(a.y);
-                acc = xyzz_add_aff(acc, a.x, a.y);
+                acc = xyzz_add_aff_lazy(acc, a.x, a.y);
             }
             if (p + 1 == kend || p + 1 == e) {  // the run of this bucket ends here
                 const bool before = kbeg < s;
                 const bool after = kend > e;
+                acc = xyzz_canon(acc);
                 if (!before && !after) {
                     st_xyzz(buckets + key, acc);
                 } else if (before) {
