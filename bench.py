@@ -133,7 +133,7 @@ class ClockSampler:
 class ExtendPhase:
     """64 columns: iNTT 2^log_n -> coset NTT on 2^(log_n + ext_bits)."""
 
-    def __init__(self, zkp, device, columns=64, log_n=20, ext_bits=3, chunk=8, seed=1):
+    def __init__(self, zkp, device, columns=64, log_n=20, ext_bits=3, chunk=8, seed=1, pair_tables=True):
         self.zkp, self.H = zkp, zkp.host
         self.device = device
         self.C, self.log_n, self.e, self.chunk = columns, log_n, ext_bits, chunk
@@ -145,6 +145,10 @@ class ExtendPhase:
         self.tw_inv = H.generate_omega_buffers(mont(pow(w, -1, R_MOD)), log_n)
         self.n_inv = fr_tensor([pow(n, -1, R_MOD)], device)
         self.twist = H.twist_tables(mont(GENERATOR), mont(omega(log_n + ext_bits)), log_n, ext_bits, self.tw)
+        # the same tables as (w, w') pairs: products by known factors
+        self.pairs = pair_tables
+        self.tables = (H.extend_tables(self.tw, self.tw_inv, self.n_inv, mont(GENERATOR),
+                                       mont(omega(log_n + ext_bits)), log_n, ext_bits) if pair_tables else None)
         self.lag = random_fr(columns * n, seed, device)
         self.coeff = torch.empty((columns * n, 4), dtype=torch.int64, device=device)
         self.ext = torch.empty((columns * E * n, 4), dtype=torch.int64, device=device)
@@ -195,9 +199,13 @@ class ExtendPhase:
         n, E = self.n, self.E
         lag = self.lag if lag is None else lag
         coeff = self.coeff if coeff is None else coeff
-        self.H.extend_batch(self.ext[c0 * E * n:], coeff[c0 * n:], lag[c0 * n:], self.chunk, self.log_n, self.e,
-                            self.tw_inv, self.n_inv, self.tw, self.twist, self.scratch, stage_events=events,
-                            stream=stream)
+        if self.pairs:
+            self.H.extend_batch_tables(self.ext[c0 * E * n:], coeff[c0 * n:], lag[c0 * n:], self.chunk, self.log_n,
+                                       self.e, self.tables, self.scratch, stage_events=events, stream=stream)
+        else:
+            self.H.extend_batch(self.ext[c0 * E * n:], coeff[c0 * n:], lag[c0 * n:], self.chunk, self.log_n,
+                                self.e, self.tw_inv, self.n_inv, self.tw, self.twist, self.scratch,
+                                stage_events=events, stream=stream)
 
     def step(self, events=None):
         for i, c0 in enumerate(range(0, self.C, self.chunk)):
@@ -718,7 +726,7 @@ def run_ours(args):
     zkp = importlib.import_module("zkwasm-prover_b200")
     zkp.load_library()
     ph = ExtendPhase(zkp, device, columns=args.columns, log_n=args.log_n, ext_bits=args.ext_bits,
-                     chunk=args.chunk, seed=1 + rank)
+                     chunk=args.chunk, seed=1 + rank, pair_tables=not args.montgomery_tables)
     nchunks = ph.C // ph.chunk
     for _ in range(args.warmup):
         ph.step()
@@ -789,6 +797,7 @@ def run_ours(args):
                                    f"2^{args.log_n + args.ext_bits} (shift 7)",
                        "columns": args.columns, "log_n": args.log_n, "ext_bits": args.ext_bits,
                        "chunk_columns": args.chunk, "parallelism": f"replicas x{ws}",
+                       "multiplier_tables": "montgomery" if args.montgomery_tables else "shoup_pairs",
                        "l2": "inputs and outputs (2 GiB in, 18 GiB out per step) exceed L2; no flush needed"},
             "e2e": e2e,
             "gpu_launches": launches * 4,
@@ -1023,6 +1032,8 @@ def main():
     ap.add_argument("--ext-bits", type=int, default=3)
     ap.add_argument("--chunk", type=int, default=8)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--montgomery-tables", action="store_true",
+                    help="multiply by Montgomery-form twiddles instead of (w, w') pairs")
     ap.add_argument("--no-msm", action="store_true")
     ap.add_argument("--no-reference-gpu", action="store_true")
     ap.add_argument("--no-rows", action="store_true", help="skip the per-row kernel timings")

@@ -295,6 +295,26 @@ cudaError_t zkp_extend_batch(void *ext_out, void *coeff_out, const void *lagrang
                              int ext_bits, const void *tw_inv, const void *n_inv, const void *tw, const void *twist,
                              void *scratch, void *stage_events, cudaStream_t stream);
 
+/* Elements of the table blob of zkp_extend_batch_tables (0 when the sizes are
+ * unsupported): every twiddle, twist and scale of the phase as the pair
+ * (w, w') with w canonical and w' = floor(w 2^256 / r), two elements an
+ * entry: tw at [0, 2n), tw_inv at [2n, 4n), n^-1 at [4n, 4n + 2), then the
+ * coset tables of zkp_coset_twist_tables in the same pair layout. */
+size_t zkp_extend_table_elems(int log_n, int ext_bits);
+
+/* Fills the blob from the natural tables tw (w_n^i) and tw_inv (w_n^-i), n^-1
+ * and the coset generator shift * w_ext^j (all device values in Montgomery
+ * form). */
+cudaError_t zkp_extend_tables(void *tables, const void *tw, const void *tw_inv, const void *n_inv, const void *shift,
+                              const void *w_ext, int log_n, int ext_bits, cudaStream_t stream);
+
+/* zkp_extend_batch over the blob: the same outputs, every product by a table
+ * factor computed from the pair (a w - floor(a w' / 2^256) r, 207 instead of
+ * 264 integer multiply-adds). */
+cudaError_t zkp_extend_batch_tables(void *ext_out, void *coeff_out, const void *lagrange_in, uint32_t ncols,
+                                    int log_n, int ext_bits, const void *tables, void *scratch, void *stage_events,
+                                    cudaStream_t stream);
+
 /* out[i] = (accumulate ? out[i] : 0) + 1 / (in[i] + c[0]) (c may be NULL);
  * zero maps to zero. out may alias in.  scratch: NULL or
  * zkp_scan_scratch_elems(n) device elements (not aliasing out or in); with it

@@ -170,3 +170,9 @@ extern "C" void hc_madd_lazy_chain(uint64_t* out, const uint64_t* acc, const uin
     st(out + 8, a.zz);
     st(out + 12, a.zzz);
 }
+
+// Fr products by a known factor: out = fe_mul_shoup(a, w, wp)
+extern "C" void hc_mul_shoup(uint64_t* out, const uint64_t* a, const uint64_t* w, const uint64_t* wp, long n) {
+    for (long i = 0; i < n; i++)
+        st(out + 4 * i, fe_mul_shoup<FrCfg>(ld<FrCfg>(a + 4 * i), ld<FrCfg>(w + 4 * i), ld<FrCfg>(wp + 4 * i)));
+}

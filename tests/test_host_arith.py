@@ -36,6 +36,7 @@ def hc():
         "hc_glv_split": [P, P, P, P, ctypes.c_long],
         "hc_lazy": [ctypes.c_int, P, P, P, ctypes.c_long],
         "hc_madd_lazy_chain": [P, P, P, ctypes.c_long],
+        "hc_mul_shoup": [P, P, P, P, ctypes.c_long],
         "hc_glv_phi": [P, P, ctypes.c_long],
     }.items():
         getattr(L, name).argtypes = args
@@ -249,3 +250,21 @@ def test_madd_lazy_chain(O, hc):
         ref = out
     hc.hc_madd_lazy_chain(_p(got), _p(lifted), _p(np.ascontiguousarray(pts[1:20])), 19)
     assert (got == ref).all()
+
+
+def test_mul_by_known_factor(O, hc):
+    # a * w mod r from w and w' = floor(w 2^256 / r) for any a < 2^256:
+    # result below 2r and congruent; extreme a and w included
+    r = O.R_MOD
+    rng = random.Random(61)
+    A = [0, 1, 2 ** 256 - 1, 2 * r - 1, r] + [rng.randrange(2 ** 256) for _ in range(3000)]
+    Wv = [r - 1, 1, 0, r - 1, (r - 1) // 2] + [rng.randrange(r) for _ in range(3000)]
+    lim = lambda v: [(v >> (64 * j)) & (2 ** 64 - 1) for j in range(4)]
+    a = np.array([lim(x) for x in A], np.uint64)
+    w = np.array([lim(x) for x in Wv], np.uint64)
+    wp = np.array([lim((x << 256) // r) for x in Wv], np.uint64)
+    out = np.zeros_like(a)
+    hc.hc_mul_shoup(_p(out), _p(a), _p(w), _p(wp), a.shape[0])
+    for i, (x, y) in enumerate(zip(A, Wv)):
+        got = sum(int(out[i, j]) << (64 * j) for j in range(4))
+        assert got < 2 * r and (got - x * y) % r == 0, i

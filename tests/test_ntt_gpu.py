@@ -94,9 +94,11 @@ def test_ntt_batch_columns(O, gpu, log_n, ncols):
 
 
 # fused stage radices: 2^18 -> 2^9, 2^19 -> 2^9, 2^20 and 2^21 -> 2^10, 2^22 -> 2^11
+@pytest.mark.parametrize("pairs", [False, True])
 @pytest.mark.parametrize("log_n,ext_bits,ncols", [(4, 3, 2), (10, 3, 3), (13, 3, 2), (16, 2, 2),
                                                   (18, 3, 2), (19, 2, 1), (20, 3, 1), (22, 1, 1)])
-def test_extend_batch_matches_coset_ntt(O, gpu, log_n, ext_bits, ncols):
+def test_extend_batch_matches_coset_ntt(O, gpu, log_n, ext_bits, ncols, pairs):
+    # pairs: the same phase over (w, w') tables and products by known factors
     H = gpu.host
     n = 1 << log_n
     shift = 7  # the field's multiplicative generator
@@ -109,7 +111,11 @@ def test_extend_batch_matches_coset_ntt(O, gpu, log_n, ext_bits, ncols):
     ext = H.empty_fr(ncols * E * n)
     coeff = H.empty_fr(ncols * n)
     scratch = H.empty_fr(ncols * E * n)
-    H.extend_batch(ext, coeff, H.to_device(lag), ncols, log_n, ext_bits, tw_inv, n_inv, tw, twist, scratch)
+    if pairs:
+        tables = H.extend_tables(tw, tw_inv, n_inv, O.fr(shift), O.fr(O.omega(log_n + ext_bits)), log_n, ext_bits)
+        H.extend_batch_tables(ext, coeff, H.to_device(lag), ncols, log_n, ext_bits, tables, scratch)
+    else:
+        H.extend_batch(ext, coeff, H.to_device(lag), ncols, log_n, ext_bits, tw_inv, n_inv, tw, twist, scratch)
     torch.cuda.synchronize()
     ge, gc = H.to_host(ext), H.to_host(coeff)
     for c in range(ncols):

@@ -67,6 +67,9 @@ SIGNATURES = {
     "zkp_coset_table_elems": ([I, I], SZ),
     "zkp_coset_twist_tables": [P, P, P, I, I, P, S],
     "zkp_extend_batch": [P, P, P, U, I, I, P, P, P, P, P, P, S],
+    "zkp_extend_table_elems": ([I, I], SZ),
+    "zkp_extend_tables": [P, P, P, P, P, P, I, I, S],
+    "zkp_extend_batch_tables": [P, P, P, U, I, I, P, P, P, S],
     "zkp_batch_inverse": [P, P, P, U, I, P, S],
     "zkp_scan_scratch_elems": ([U], SZ),
     "zkp_g1_multiples": [P, P, U, S],

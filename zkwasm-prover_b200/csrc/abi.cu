@@ -14,7 +14,8 @@ static inline const Fr* CF(const void* p) { return reinterpret_cast<const Fr*>(p
 
 namespace zk {
 
-// twist[j * n + k] = (shift * w_ext^j)^k
+// twist[j * n + k] = (shift * w_ext^j)^k (as Montgomery elements or pairs)
+template <bool PAIRS>
 __global__ void twist_kernel(Fr* twist, const Fr* shift, const Fr* w_ext, uint32_t n, uint32_t chunk) {
     const uint32_t j = blockIdx.y;
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -23,9 +24,8 @@ __global__ void twist_kernel(Fr* twist, const Fr* shift, const Fr* w_ext, uint32
     if (s >= e) return;
     const Fr base = fe_mul<FrCfg>(ld_elem<FrCfg>(shift), fe_pow_u32<FrCfg>(ld_elem<FrCfg>(w_ext), j));
     Fr cur = fe_pow_u32<FrCfg>(base, s);
-    Fr* out = twist + (size_t)j * n;
     for (uint32_t i = s; i < e; i++) {
-        st_elem<FrCfg>(out + i, cur);
+        st_factor<PAIRS>(twist, (size_t)j * n + i, cur);
         cur = fe_mul<FrCfg>(cur, base);
     }
 }
@@ -482,13 +482,47 @@ cudaError_t zkp_coset_twist_tables(void* twist, const void* shift, const void* w
     const uint32_t chunk = 16;
     const uint32_t threads = (uint32_t)((n + chunk - 1) / chunk);
     dim3 grid((threads + 127) / 128, 1u << ext_bits);
-    zk::twist_kernel<<<grid, 128, 0, stream>>>(F(twist), CF(shift), CF(w_ext), (uint32_t)n, chunk);
+    zk::twist_kernel<false><<<grid, 128, 0, stream>>>(F(twist), CF(shift), CF(w_ext), (uint32_t)n, chunk);
     return cudaGetLastError();
 }
 
-cudaError_t zkp_extend_batch(void* ext_out, void* coeff_out, const void* lagrange_in, uint32_t ncols, int log_n,
-                             int ext_bits, const void* tw_inv, const void* n_inv, const void* tw, const void* twist,
-                             void* scratch, void* stage_events, cudaStream_t stream) {
+// Tables of zkp_extend_batch_tables, every factor as a (w, w') pair of
+// fe_mul_shoup (two elements an entry), in elements:
+//   [0, 2n) tw, [2n, 4n) tw_inv, [4n, 4n + 2) n^-1, then the coset tables of
+//   zkp_coset_twist_tables (2 E n + 2 E 2^r for the fused stage, else 2 E n)
+size_t zkp_extend_table_elems(int log_n, int ext_bits) {
+    const size_t c = zkp_coset_table_elems(log_n, ext_bits);
+    if (c == 0 || log_n > 24) return 0;
+    return 4 * ((size_t)1 << log_n) + 2 + 2 * c;
+}
+
+cudaError_t zkp_extend_tables(void* tables, const void* tw, const void* tw_inv, const void* n_inv, const void* shift,
+                              const void* w_ext, int log_n, int ext_bits, cudaStream_t stream) {
+    if (zkp_extend_table_elems(log_n, ext_bits) == 0 || !tables || !tw || !tw_inv || !n_inv || !shift || !w_ext)
+        return cudaErrorInvalidValue;
+    const size_t n = (size_t)1 << log_n;
+    Fr* t = F(tables);
+    ZK_CHECK(zk::shoup_pairs(t, CF(tw), n, stream));
+    ZK_CHECK(zk::shoup_pairs(t + 2 * n, CF(tw_inv), n, stream));
+    ZK_CHECK(zk::shoup_pairs(t + 4 * n, CF(n_inv), 1, stream));
+    Fr* twist = t + 4 * n + 2;
+    int rad[4];
+    if (extend_fused(log_n, rad))
+        return zk::ntt_fused_tables(twist, twist + 2 * (n << ext_bits), CF(tw), CF(shift), CF(w_ext), log_n, rad[1],
+                                    ext_bits, stream, true);
+    const uint32_t chunk = 16;
+    const uint32_t threads = (uint32_t)((n + chunk - 1) / chunk);
+    dim3 grid((threads + 127) / 128, 1u << ext_bits);
+    zk::twist_kernel<true><<<grid, 128, 0, stream>>>(twist, CF(shift), CF(w_ext), (uint32_t)n, chunk);
+    return cudaGetLastError();
+}
+
+// the extended-domain phase over either table layout: Montgomery tables
+// (pairs = 0) or (w, w') pairs; twist holds the coset tables (wtab then stab
+// for the fused stage), offsets counted in entries of the layout
+static cudaError_t extend_impl(void* ext_out, void* coeff_out, const void* lagrange_in, uint32_t ncols, int log_n,
+                               int ext_bits, const Fr* tw_inv, const Fr* n_inv, const Fr* tw, const Fr* twist,
+                               int pairs, void* stage_events, void* scratch, cudaStream_t stream) {
     cudaEvent_t* ev = reinterpret_cast<cudaEvent_t*>(stage_events);
 #define ZK_MARK(i) \
     if (ev) ZK_CHECK(cudaEventRecord(ev[i], stream))
@@ -497,6 +531,7 @@ cudaError_t zkp_extend_batch(void* ext_out, void* coeff_out, const void* lagrang
         return cudaErrorInvalidValue;
     if (!ext_out || !lagrange_in || !tw_inv || !n_inv || !tw || !twist || !scratch) return cudaErrorInvalidValue;
     const size_t n = (size_t)1 << log_n;
+    const size_t ew = pairs ? 2 : 1;  // elements an entry
     const uint32_t E = 1u << ext_bits;
     int rad[4];
     const int np = extend_plan(log_n, rad);
@@ -506,10 +541,11 @@ cudaError_t zkp_extend_batch(void* ext_out, void* coeff_out, const void* lagrang
         NttPassArgs a = {};
         a.src = CF(lagrange_in);
         a.dst = F(coeff_out);
-        a.tw = CF(tw_inv);
+        a.tw = tw_inv;
         a.log_n = log_n;
         a.src_ys = n;
         a.dst_ys = n;
+        a.pairs = pairs;
         ZK_CHECK(ntt_pass(a, rad[0], ncols, 1, stream));
         ZK_MARK(1);
         ZK_MARK(2);
@@ -518,21 +554,22 @@ cudaError_t zkp_extend_batch(void* ext_out, void* coeff_out, const void* lagrang
         f.src = F(coeff_out);
         f.coeff = F(coeff_out);
         f.sub = F(scratch);
-        f.tw_inv = CF(tw_inv);
-        f.n_inv = CF(n_inv);
-        f.tw = CF(tw);
-        f.wtab = CF(twist);
-        f.stab = CF(twist) + ((size_t)E * n);
+        f.tw_inv = tw_inv;
+        f.n_inv = n_inv;
+        f.tw = tw;
+        f.wtab = twist;
+        f.stab = twist + ew * E * n;
         f.log_n = log_n;
         f.E = (int)E;
         f.src_ys = n;
         f.coeff_ys = n;
         f.sub_ys = n * E;
+        f.pairs = pairs;
         ZK_CHECK(ntt_fused_extend(f, rad[1], ncols, stream));
         ZK_MARK(3);
         // 3. last pass of each coset's forward transform, interleaved output
         NttPassArgs b = {};
-        b.tw = CF(tw);
+        b.tw = tw;
         b.log_n = log_n;
         b.log_p = rad[1];
         b.src = F(scratch);
@@ -542,6 +579,7 @@ cudaError_t zkp_extend_batch(void* ext_out, void* coeff_out, const void* lagrang
         b.dst_ys = n * E;
         b.out_shift = ext_bits;
         b.out_off_z = 1;
+        b.pairs = pairs;
         ZK_CHECK(ntt_pass(b, rad[0], ncols, E, stream));
         ZK_MARK(4);
         return cudaGetLastError();
@@ -551,12 +589,13 @@ cudaError_t zkp_extend_batch(void* ext_out, void* coeff_out, const void* lagrang
     // 1. inverse transform: lagrange -> (scratch) -> coefficients, scaled by n^-1
     {
         NttPassArgs a = {};
-        a.tw = CF(tw_inv);
+        a.tw = tw_inv;
         a.log_n = log_n;
+        a.pairs = pairs;
         if (np == 1) {
             a.src = CF(lagrange_in);
             a.dst = coeff;
-            a.scale = CF(n_inv);
+            a.scale = n_inv;
             a.src_ys = n;
             a.dst_ys = n;
             // single pass cannot run in place across buffers, so copy first
@@ -576,7 +615,7 @@ cudaError_t zkp_extend_batch(void* ext_out, void* coeff_out, const void* lagrang
             a.src = scr;
             a.dst = coeff;
             a.log_p = rad[0];
-            a.scale = CF(n_inv);
+            a.scale = n_inv;
             ZK_CHECK(ntt_pass(a, rad[1], ncols, 1, stream));
         }
     }
@@ -584,12 +623,13 @@ cudaError_t zkp_extend_batch(void* ext_out, void* coeff_out, const void* lagrang
     // 2. 2^e forward transforms of the twisted coefficients, interleaved output
     {
         NttPassArgs a = {};
-        a.tw = CF(tw);
+        a.tw = tw;
         a.log_n = log_n;
+        a.pairs = pairs;
         if (np == 1) {
             a.src = coeff;
             a.dst = F(ext_out);
-            a.in_mul = CF(twist);
+            a.in_mul = twist;
             a.in_mul_zs = n;
             a.out_shift = ext_bits;
             a.out_off_z = 1;
@@ -601,7 +641,7 @@ cudaError_t zkp_extend_batch(void* ext_out, void* coeff_out, const void* lagrang
             if (!coeff_out) return cudaErrorInvalidValue;  // scratch holds the sub-transforms
             a.src = coeff;
             a.dst = scr;
-            a.in_mul = CF(twist);
+            a.in_mul = twist;
             a.in_mul_zs = n;
             a.src_ys = n;
             a.dst_ys = n * E;
@@ -609,8 +649,9 @@ cudaError_t zkp_extend_batch(void* ext_out, void* coeff_out, const void* lagrang
             ZK_CHECK(ntt_pass(a, rad[0], ncols, E, stream));
             ZK_MARK(3);
             NttPassArgs b = {};
-            b.tw = CF(tw);
+            b.tw = tw;
             b.log_n = log_n;
+            b.pairs = pairs;
             b.log_p = rad[0];
             b.src = scr;
             b.dst = F(ext_out);
@@ -625,6 +666,23 @@ cudaError_t zkp_extend_batch(void* ext_out, void* coeff_out, const void* lagrang
     ZK_MARK(4);
 #undef ZK_MARK
     return cudaGetLastError();
+}
+
+cudaError_t zkp_extend_batch(void* ext_out, void* coeff_out, const void* lagrange_in, uint32_t ncols, int log_n,
+                             int ext_bits, const void* tw_inv, const void* n_inv, const void* tw, const void* twist,
+                             void* scratch, void* stage_events, cudaStream_t stream) {
+    return extend_impl(ext_out, coeff_out, lagrange_in, ncols, log_n, ext_bits, CF(tw_inv), CF(n_inv), CF(tw),
+                       CF(twist), 0, stage_events, scratch, stream);
+}
+
+cudaError_t zkp_extend_batch_tables(void* ext_out, void* coeff_out, const void* lagrange_in, uint32_t ncols,
+                                    int log_n, int ext_bits, const void* tables, void* scratch, void* stage_events,
+                                    cudaStream_t stream) {
+    if (!tables || log_n < 3 || log_n > 24) return cudaErrorInvalidValue;
+    const size_t n = (size_t)1 << log_n;
+    const Fr* t = CF(tables);
+    return extend_impl(ext_out, coeff_out, lagrange_in, ncols, log_n, ext_bits, t + 2 * n, t + 4 * n, t,
+                       t + 4 * n + 2, 1, stage_events, scratch, stream);
 }
 
 cudaError_t zkp_batch_inverse(void* out, const void* in, const void* c, uint32_t n, int accumulate, void* scratch,

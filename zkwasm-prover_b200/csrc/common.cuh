@@ -34,6 +34,19 @@ __device__ __forceinline__ void st_elem(Fe<C>* p, const Fe<C>& v) {
     q[1] = make_uint4(v.v[4], v.v[5], v.v[6], v.v[7]);
 }
 
+// entry i of a multiplier table from the Montgomery form wm of its factor:
+// wm itself, or the pair (w, w' = floor(w 2^256 / r)) of fe_mul_shoup at
+// elements 2i and 2i + 1
+template <bool PAIRS>
+__device__ __forceinline__ void st_factor(Fr* t, size_t i, const Fr& wm) {
+    if (PAIRS) {
+        st_elem<FrCfg>(t + 2 * i, fe_from_mont<FrCfg>(wm));
+        st_elem<FrCfg>(t + 2 * i + 1, fe_shoup_companion<FrCfg>(wm));
+    } else {
+        st_elem<FrCfg>(t + i, wm);
+    }
+}
+
 }  // namespace zk
 
 #define ZK_CHECK(x)                           \

@@ -51,6 +51,10 @@ struct FrCfg {
         return pick8(j, 0xb4bf0040u, 0x5e94d8e1u, 0x1cfbb6b8u, 0x2a489cbeu, 0xa19fcfedu, 0x893cc664u, 0x7fcc657cu,
                      0x0cf8594bu);
     }
+    static ZK_HD constexpr uint32_t PINV(int j) {  // r^-1 mod 2^256
+        return pick8(j, 0x10000001u, 0x3d1e0a6cu, 0xb396ee4cu, 0x9a7979b4u, 0x66f9dc6eu, 0x1c6567d7u, 0xf27cbe4du,
+                     0x8c07d0e2u);
+    }
 };
 
 struct FqCfg {
@@ -322,6 +326,120 @@ ZK_HD Fe<C> fe_mul_lazy(const Fe<C>& a, const Fe<C>& b) {
     Fe<C> r;
 #pragma unroll
     for (int j = 0; j < 8; j++) r.v[j] = e[j];
+    return r;
+}
+
+// ---------------------------------------------------------------------------
+// Products by a known factor (Shoup): for a canonical w and its companion
+// w' = floor(w 2^256 / m), a * w mod m for any a < 2^256 from q = the high
+// half of a w' (truncated below column 7: short by at most one) and
+// a w - q m, which then lies in [0, 3m); one conditional subtraction of m
+// leaves [0, 2m).  With a in Montgomery form and w canonical the result is
+// the Montgomery form of the product, as fe_mul_lazy(a, w R mod m) would give,
+// for 207 multiply-adds instead of 264.
+
+// (c0, c1, c2) += x * y (product scanning, one column)
+ZK_HD void mac3(uint32_t& c0, uint32_t& c1, uint32_t& c2, uint32_t x, uint32_t y) {
+#if defined(__CUDA_ARCH__)
+    asm("mad.lo.cc.u32  %0, %3, %4, %0;\n\t"
+        "madc.hi.cc.u32 %1, %3, %4, %1;\n\t"
+        "addc.u32       %2, %2, 0;"
+        : "+r"(c0), "+r"(c1), "+r"(c2)
+        : "r"(x), "r"(y));
+#else
+    const uint64_t p = (uint64_t)x * y;
+    uint64_t s = (uint64_t)c0 + (uint32_t)p;
+    c0 = (uint32_t)s;
+    s = (uint64_t)c1 + (uint32_t)(p >> 32) + (s >> 32);
+    c1 = (uint32_t)s;
+    c2 += (uint32_t)(s >> 32);
+#endif
+}
+
+// (c1, c2) += high word of x * y
+ZK_HD void machi2(uint32_t& c1, uint32_t& c2, uint32_t x, uint32_t y) {
+#if defined(__CUDA_ARCH__)
+    asm("mad.hi.cc.u32 %0, %2, %3, %0;\n\t"
+        "addc.u32      %1, %1, 0;"
+        : "+r"(c1), "+r"(c2)
+        : "r"(x), "r"(y));
+#else
+    const uint64_t s = (uint64_t)c1 + (uint32_t)(((uint64_t)x * y) >> 32);
+    c1 = (uint32_t)s;
+    c2 += (uint32_t)(s >> 32);
+#endif
+}
+
+// r = a * b mod 2^256
+ZK_HD void mul_lo8(uint32_t r[8], const uint32_t a[8], const uint32_t b[8]) {
+    uint32_t c0 = 0, c1 = 0, c2 = 0;
+#pragma unroll
+    for (int k = 0; k < 7; k++) {
+#pragma unroll
+        for (int i = 0; i <= k; i++) mac3(c0, c1, c2, a[i], b[k - i]);
+        r[k] = c0;
+        c0 = c1;
+        c1 = c2;
+        c2 = 0;
+    }
+#pragma unroll
+    for (int i = 0; i < 8; i++) c0 += a[i] * b[7 - i];
+    r[7] = c0;
+}
+
+// q = floor(S / 2^256) for S the sum of the partial products of a * b from
+// column 7 up and the high words of column 6: floor(a b / 2^256) or one less
+// (the terms left out sum to less than 2^229)
+ZK_HD void mul_hi8_trunc(uint32_t q[8], const uint32_t a[8], const uint32_t b[8]) {
+    uint32_t c1 = 0, c2 = 0;
+#pragma unroll
+    for (int i = 0; i <= 6; i++) machi2(c1, c2, a[i], b[6 - i]);
+    uint32_t c0 = c1;
+    c1 = c2;
+    c2 = 0;
+#pragma unroll
+    for (int i = 0; i <= 7; i++) mac3(c0, c1, c2, a[i], b[7 - i]);
+#pragma unroll
+    for (int k = 8; k < 15; k++) {
+        c0 = c1;
+        c1 = c2;
+        c2 = 0;
+#pragma unroll
+        for (int i = k - 7; i <= 7; i++) mac3(c0, c1, c2, a[i], b[k - i]);
+        q[k - 8] = c0;
+    }
+    q[7] = c1;
+}
+
+template <class C>
+ZK_HD Fe<C> fe_mul_shoup(const Fe<C>& a, const Fe<C>& w, const Fe<C>& wp) {
+    uint32_t m[8], q[8], x[8], y[8], r[8], u[8];
+#pragma unroll
+    for (int j = 0; j < 8; j++) m[j] = C::M(j);
+    mul_hi8_trunc(q, a.v, wp.v);
+    mul_lo8(x, a.v, w.v);
+    mul_lo8(y, q, m);
+    sub8_borrow(r, x, y);
+    const uint32_t br = sub8_borrow(u, r, m);
+    Fe<C> o;
+    select8(o.v, br, r, u);
+    return o;
+}
+
+// The companion w' = floor(w 2^256 / m) of w from its Montgomery form
+// wm = w 2^256 mod m: w 2^256 = w' m + wm, so w' = -wm m^-1 mod 2^256 (exact,
+// as w' < 2^256).  Needs C::PINV = m^-1 mod 2^256.
+template <class C>
+ZK_HD Fe<C> fe_shoup_companion(const Fe<C>& wm) {
+    uint32_t neg[8], zero[8], pinv[8];
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+        zero[j] = 0;
+        pinv[j] = C::PINV(j);
+    }
+    sub8_borrow(neg, zero, wm.v);
+    Fe<C> r;
+    mul_lo8(r.v, neg, pinv);
     return r;
 }
 

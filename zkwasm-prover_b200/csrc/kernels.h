@@ -22,6 +22,7 @@ struct NttPassArgs {
     size_t src_ys, dst_ys;  // per-column strides (blockIdx.y), elements
     size_t src_zs, dst_zs;  // per-sub-transform strides (blockIdx.z), elements
     size_t in_mul_zs;
+    int pairs;           // tw, in_mul and scale hold (w, w') pairs (two elements an entry)
 };
 
 cudaError_t ntt_pass(const NttPassArgs& a, int log_r, unsigned ny, unsigned nz, cudaStream_t s);
@@ -38,10 +39,13 @@ struct FusedExtendArgs {
     const Fr* stab;    // E * 2^log_r
     int log_n, E;
     size_t src_ys, coeff_ys, sub_ys;
+    int pairs;         // every table holds (w, w') pairs (two elements an entry)
 };
 cudaError_t ntt_fused_extend(const FusedExtendArgs& a, int log_r, unsigned ncols, cudaStream_t s);
 cudaError_t ntt_fused_tables(Fr* wtab, Fr* stab, const Fr* tw, const Fr* shift, const Fr* w_ext, int log_n, int log_r,
-                             int ext_bits, cudaStream_t s);
+                             int ext_bits, cudaStream_t s, bool pairs = false);
+// out[2i], out[2i+1] = (w, w') of the Montgomery-form factors in[i], i < n
+cudaError_t shoup_pairs(Fr* out, const Fr* in, size_t n, cudaStream_t s);
 int ntt_plan(int log_n, int radices[4]);
 // Full transform of ncols columns (stride col_stride elements) by the twiddle
 // table tw; result in buf or tmp (*result_in_tmp), multiplied by *scale if given.

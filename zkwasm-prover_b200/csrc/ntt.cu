@@ -38,10 +38,39 @@ namespace zk {
 #if defined(ZK_NTT_INLINE_MUL)
 __device__ __forceinline__ Fr nt_mul(const Fr& a, const Fr& b) { return fe_mul<FrCfg>(a, b); }
 __device__ __forceinline__ Fr nt_mulz(const Fr& a, const Fr& b) { return fe_mul_lazy<FrCfg>(a, b); }
+__device__ __forceinline__ Fr nt_shoup(const Fr& a, const Fr& w, const Fr& wp) {
+    return fe_mul_shoup<FrCfg>(a, w, wp);
+}
 #else
 __device__ __noinline__ Fr nt_mul(const Fr a, const Fr b) { return fe_mul<FrCfg>(a, b); }
 __device__ __noinline__ Fr nt_mulz(const Fr a, const Fr b) { return fe_mul_lazy<FrCfg>(a, b); }
+__device__ __noinline__ Fr nt_shoup(const Fr a, const Fr w, const Fr wp) { return fe_mul_shoup<FrCfg>(a, w, wp); }
 #endif
+
+// Multiplier tables (twiddles, twists, scales) come in two layouts.
+// TwM: one Montgomery-form element per entry, multiplied with nt_mulz.
+// TwS: the pair (w, w') per entry, w canonical and w' = floor(w 2^256 / r),
+// multiplied with nt_shoup (207 multiply-adds instead of 264; both results
+// lie in [0, 2r)).  Every product of the pass kernels is by a table entry.
+struct TwM {
+    struct K {
+        Fr w;
+    };
+    static __device__ __forceinline__ K ld(const Fr* t, size_t i) { return {ldg_elem<FrCfg>(t + i)}; }
+    static __device__ __forceinline__ Fr mul(const Fr& v, const K& k) { return nt_mulz(v, k.w); }
+    static __host__ __device__ __forceinline__ const Fr* off(const Fr* t, size_t i) { return t + i; }
+};
+struct TwS {
+    struct K {
+        Fr w, wp;
+    };
+    static __device__ __forceinline__ K ld(const Fr* t, size_t i) {
+        return {ldg_elem<FrCfg>(t + 2 * i), ldg_elem<FrCfg>(t + 2 * i + 1)};
+    }
+    static __device__ __forceinline__ Fr mul(const Fr& v, const K& k) { return nt_shoup(v, k.w, k.wp); }
+    static __host__ __device__ __forceinline__ const Fr* off(const Fr* t, size_t i) { return t + 2 * i; }
+};
+
 
 // ---------------------------------------------------------------- small DFTs
 // Decimation in frequency, natural input; outputs land bit-reversed and are
@@ -54,25 +83,28 @@ __device__ __forceinline__ void dft2(Fr& a, Fr& b) {
 }
 
 // v[0..3] -> y[k] at position rev2(k): y0=v0, y1=v2, y2=v1, y3=v3
-__device__ __forceinline__ void dft4_dif(Fr& v0, Fr& v1, Fr& v2, Fr& v3, const Fr& w4) {
+template <class TW>
+__device__ __forceinline__ void dft4_dif(Fr& v0, Fr& v1, Fr& v2, Fr& v3, const typename TW::K& w4) {
     dft2(v0, v2);
     dft2(v1, v3);
-    v3 = nt_mulz(v3, w4);
+    v3 = TW::mul(v3, w4);
     dft2(v0, v1);
     dft2(v2, v3);
 }
 
 // v[0..7] -> y[j] at position rev3(j)
-__device__ __forceinline__ void dft8_dif(Fr v[8], const Fr& w8, const Fr& w4, const Fr& w83) {
+template <class TW>
+__device__ __forceinline__ void dft8_dif(Fr v[8], const typename TW::K& w8, const typename TW::K& w4,
+                                         const typename TW::K& w83) {
     dft2(v[0], v[4]);
     dft2(v[1], v[5]);
     dft2(v[2], v[6]);
     dft2(v[3], v[7]);
-    v[5] = nt_mulz(v[5], w8);
-    v[6] = nt_mulz(v[6], w4);
-    v[7] = nt_mulz(v[7], w83);
-    dft4_dif(v[0], v[1], v[2], v[3], w4);
-    dft4_dif(v[4], v[5], v[6], v[7], w4);
+    v[5] = TW::mul(v[5], w8);
+    v[6] = TW::mul(v[6], w4);
+    v[7] = TW::mul(v[7], w83);
+    dft4_dif<TW>(v[0], v[1], v[2], v[3], w4);
+    dft4_dif<TW>(v[4], v[5], v[6], v[7], w4);
 }
 
 // Shared-memory tiles hold 32-byte elements as two 16-byte halves.  Element
@@ -108,15 +140,16 @@ struct PassOut {
 };
 
 // (the result is canonical: it leaves the pass)
+template <class TW>
 __device__ __forceinline__ Fr finish_out(const PassOut& o, Fr v, uint32_t y) {
-    if (o.wrow) return fe_canon<FrCfg>(nt_mulz(v, ldg_elem<FrCfg>(o.wrow + y)));
-    if (o.qhi != 0 && y != 0) v = nt_mulz(v, ldg_elem<FrCfg>(o.tw + ((size_t)(o.qhi * y) << o.log_p)));
-    if (o.scale) v = nt_mulz(v, ldg_elem<FrCfg>(o.scale));
+    if (o.wrow) return fe_canon<FrCfg>(TW::mul(v, TW::ld(o.wrow, y)));
+    if (o.qhi != 0 && y != 0) v = TW::mul(v, TW::ld(o.tw, (size_t)(o.qhi * y) << o.log_p));
+    if (o.scale) v = TW::mul(v, TW::ld(o.scale, 0));
     return fe_canon<FrCfg>(v);
 }
 
 // radix-8 sub-stage over one DFT of size R in shared memory
-template <int LOGR>
+template <int LOGR, class TW>
 __device__ __forceinline__ void stage8(Fr* x, int u, int log_ps, bool last, const Fr* tw, int log_n,
                                        const Fr* in_mul, size_t in_base, int log_items,
                                        const PassOut& po) {
@@ -129,14 +162,14 @@ __device__ __forceinline__ void stage8(Fr* x, int u, int log_ps, bool last, cons
     if (in_mul) {
 #pragma unroll
         for (int i = 0; i < 8; i++)
-            v[i] = nt_mulz(v[i], ldg_elem<FrCfg>(in_mul + in_base + ((size_t)(u + S * i) << log_items)));
+            v[i] = TW::mul(v[i], TW::ld(in_mul, in_base + ((size_t)(u + S * i) << log_items)));
     }
     const int sh = log_n - LOGR;  // w_R^e = tw[e << sh]
     {
-        Fr w8 = ldg_elem<FrCfg>(tw + ((size_t)(S * 1) << sh));
-        Fr w4 = ldg_elem<FrCfg>(tw + ((size_t)(S * 2) << sh));
-        Fr w83 = ldg_elem<FrCfg>(tw + ((size_t)(S * 3) << sh));
-        dft8_dif(v, w8, w4, w83);
+        const typename TW::K w8 = TW::ld(tw, (size_t)(S * 1) << sh);
+        const typename TW::K w4 = TW::ld(tw, (size_t)(S * 2) << sh);
+        const typename TW::K w83 = TW::ld(tw, (size_t)(S * 3) << sh);
+        dft8_dif<TW>(v, w8, w4, w83);
     }
     const int J = u & ((1 << log_ps) - 1);
     const int ilo = u >> log_ps;
@@ -146,16 +179,16 @@ __device__ __forceinline__ void stage8(Fr* x, int u, int log_ps, bool last, cons
     for (int j = 0; j < 8; j++) {
         Fr y = v[rev[j]];
         if (j != 0 && ilo != 0)
-            y = nt_mulz(y, ldg_elem<FrCfg>(tw + ((size_t)((ilo * j) << log_ps) << sh)));
+            y = TW::mul(y, TW::ld(tw, (size_t)((ilo * j) << log_ps) << sh));
         const int pos = J + (j << log_ps) + (ilo << (log_ps + 3));
-        if (last) y = finish_out(po, y, (uint32_t)pos);
+        if (last) y = finish_out<TW>(po, y, (uint32_t)pos);
         sm_st(x, pos, y);
     }
     __syncthreads();
 }
 
 // final radix-4 sub-stage (two items per thread); P_s = R/4 so no sub-stage twiddle
-template <int LOGR>
+template <int LOGR, class TW>
 __device__ __forceinline__ void stage4_last(Fr* x, int lt, const Fr* tw, int log_n, const PassOut& po,
                                             const Fr* in_mul, size_t in_base, int log_items) {
     constexpr int R = 1 << LOGR;
@@ -170,29 +203,28 @@ __device__ __forceinline__ void stage4_last(Fr* x, int lt, const Fr* tw, int log
     }
     __syncthreads();
     const int sh = log_n - LOGR;
-    Fr w4 = ldg_elem<FrCfg>(tw + ((size_t)S << sh));
+    const typename TW::K w4 = TW::ld(tw, (size_t)S << sh);
 #pragma unroll
     for (int k = 0; k < 2; k++) {
         int u = lt + k * TH;
         if (in_mul) {
 #pragma unroll
             for (int i = 0; i < 4; i++)
-                v[4 * k + i] = nt_mulz(
-                    v[4 * k + i], ldg_elem<FrCfg>(in_mul + in_base + ((size_t)(u + S * i) << log_items)));
+                v[4 * k + i] = TW::mul(v[4 * k + i], TW::ld(in_mul, in_base + ((size_t)(u + S * i) << log_items)));
         }
-        dft4_dif(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3], w4);
+        dft4_dif<TW>(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3], w4);
         const int rev[4] = {0, 2, 1, 3};
 #pragma unroll
         for (int j = 0; j < 4; j++) {
             const int pos = u + S * j;  // J = u, P_s = S, ilo = 0
-            sm_st(x, pos, finish_out(po, v[4 * k + rev[j]], (uint32_t)pos));
+            sm_st(x, pos, finish_out<TW>(po, v[4 * k + rev[j]], (uint32_t)pos));
         }
     }
     __syncthreads();
 }
 
 // final radix-2 sub-stage (four items per thread)
-template <int LOGR>
+template <int LOGR, class TW>
 __device__ __forceinline__ void stage2_last(Fr* x, int lt, const PassOut& po) {
     constexpr int R = 1 << LOGR;
     constexpr int S = R / 2;
@@ -204,8 +236,8 @@ __device__ __forceinline__ void stage2_last(Fr* x, int lt, const PassOut& po) {
         const int u = lt + k * TH;
         Fr v0 = sm_ld(x, u), v1 = sm_ld(x, u + S);
         dft2(v0, v1);
-        sm_st(x, u, finish_out(po, v0, (uint32_t)u));
-        sm_st(x, u + S, finish_out(po, v1, (uint32_t)(u + S)));
+        sm_st(x, u, finish_out<TW>(po, v0, (uint32_t)u));
+        sm_st(x, u + S, finish_out<TW>(po, v1, (uint32_t)(u + S)));
     }
     __syncthreads();
 }
@@ -222,7 +254,7 @@ __host__ __device__ constexpr int pass_min_blocks(int logr, int g) {
            : ((g << logr) / 8 >= 32 ? 512 / ((g << logr) / 8) : 16);
 }
 
-template <int LOGR, int G>
+template <int LOGR, int G, class TW>
 __global__ void __launch_bounds__((G << LOGR) / 8, pass_min_blocks(LOGR, G))
 ntt_pass_kernel(NttPassArgs a) {
     constexpr int R = 1 << LOGR;
@@ -254,7 +286,7 @@ ntt_pass_kernel(NttPassArgs a) {
     po.qhi = q >> a.log_p;
     po.scale = a.scale;
     po.wrow = nullptr;
-    const Fr* in_mul = a.in_mul ? a.in_mul + blockIdx.z * a.in_mul_zs : nullptr;
+    const Fr* in_mul = a.in_mul ? TW::off(a.in_mul, blockIdx.z * a.in_mul_zs) : nullptr;
     const size_t in_base = q;  // natural input position = q + (i << log_items)
 
     constexpr int NS8 = LOGR / 3;
@@ -263,11 +295,12 @@ ntt_pass_kernel(NttPassArgs a) {
 #pragma unroll 1
     for (int s = 0; s < NS8; s++) {
         const bool last = (s == NS8 - 1) && (REM == 0);
-        stage8<LOGR>(x, lt, log_ps, last, a.tw, a.log_n, s == 0 ? in_mul : nullptr, in_base, log_items, po);
+        stage8<LOGR, TW>(x, lt, log_ps, last, a.tw, a.log_n, s == 0 ? in_mul : nullptr, in_base, log_items, po);
         log_ps += 3;
     }
-    if (REM == 2) stage4_last<LOGR>(x, lt, a.tw, a.log_n, po, NS8 == 0 ? in_mul : nullptr, in_base, log_items);
-    if (REM == 1) stage2_last<LOGR>(x, lt, po);
+    if (REM == 2)
+        stage4_last<LOGR, TW>(x, lt, a.tw, a.log_n, po, NS8 == 0 ? in_mul : nullptr, in_base, log_items);
+    if (REM == 1) stage2_last<LOGR, TW>(x, lt, po);
 
     // coalesced store: dst[(J + P*j + P*R*Q) << out_shift + z*out_off_z]
     const uint32_t pm = (1u << a.log_p) - 1;
@@ -290,18 +323,18 @@ ntt_pass_kernel(NttPassArgs a) {
 }
 
 // in-CTA DFT of size 2^LOGR on tile x (natural order in and out)
-template <int LOGR>
+template <int LOGR, class TW>
 __device__ __forceinline__ void dft_tile(Fr* x, int lt, const Fr* tw, int log_n, const PassOut& po) {
     constexpr int NS8 = LOGR / 3;
     constexpr int REM = LOGR % 3;
     int log_ps = 0;
 #pragma unroll 1
     for (int s = 0; s < NS8; s++) {
-        stage8<LOGR>(x, lt, log_ps, (s == NS8 - 1) && (REM == 0), tw, log_n, nullptr, 0, 0, po);
+        stage8<LOGR, TW>(x, lt, log_ps, (s == NS8 - 1) && (REM == 0), tw, log_n, nullptr, 0, 0, po);
         log_ps += 3;
     }
-    if (REM == 2) stage4_last<LOGR>(x, lt, tw, log_n, po, nullptr, 0, 0);
-    if (REM == 1) stage2_last<LOGR>(x, lt, po);
+    if (REM == 2) stage4_last<LOGR, TW>(x, lt, tw, log_n, po, nullptr, 0, 0);
+    if (REM == 1) stage2_last<LOGR, TW>(x, lt, po);
 }
 
 // Fused extended-domain stage.  For one column and work item q it runs
@@ -328,7 +361,7 @@ __host__ __device__ constexpr int fused_min_blocks(int logr) {
     return logr <= 9 ? 7 : logr == 10 ? (ZK_FUSED_ONE_TILE ? 4 : 3) : 1;
 }
 
-template <int LOGR>
+template <int LOGR, class TW>
 __global__ void __launch_bounds__((1 << LOGR) / 8, fused_min_blocks(LOGR))
 ntt_fused_extend_kernel(FusedExtendArgs a) {
     constexpr int R = 1 << LOGR;
@@ -355,23 +388,23 @@ ntt_fused_extend_kernel(FusedExtendArgs a) {
     po.qhi = 0;
     po.scale = a.n_inv;
     po.wrow = nullptr;
-    dft_tile<LOGR>(A, tid, a.tw_inv, a.log_n, po);
+    dft_tile<LOGR, TW>(A, tid, a.tw_inv, a.log_n, po);
     for (int c = tid; c < R * 2; c += T) {
         const int h = c & 1, j = c >> 1;
         reinterpret_cast<uint4*>(coeff + q + ((size_t)j << log_items))[h] = *sm_slot(A, j, h);
     }
     for (int z = 0; z < a.E; z++) {
-        const Fr* S = a.stab + (size_t)z * R;
+        const Fr* S = TW::off(a.stab, (size_t)z * R);
         if (ZK_FUSED_ONE_TILE) {
             // the tile is the workspace: coset 0 twists it in place, later
             // cosets re-read the coefficients this CTA wrote (L2-resident)
             __syncthreads();
             for (int i = tid; i < R; i += T) {
                 const Fr cf = z == 0 ? sm_ld(A, i) : ld_elem<FrCfg>(coeff + q + ((size_t)i << log_items));
-                sm_st(B, i, nt_mulz(cf, ldg_elem<FrCfg>(S + i)));
+                sm_st(B, i, TW::mul(cf, TW::ld(S, i)));
             }
         } else {
-            for (int i = tid; i < R; i += T) sm_st(B, i, nt_mulz(sm_ld(A, i), ldg_elem<FrCfg>(S + i)));
+            for (int i = tid; i < R; i += T) sm_st(B, i, TW::mul(sm_ld(A, i), TW::ld(S, i)));
         }
         __syncthreads();
         PassOut pf;
@@ -379,8 +412,8 @@ ntt_fused_extend_kernel(FusedExtendArgs a) {
         pf.log_p = 0;
         pf.qhi = 0;
         pf.scale = nullptr;
-        pf.wrow = a.wtab + (size_t)z * n + (size_t)q * R;
-        dft_tile<LOGR>(B, tid, a.tw, a.log_n, pf);
+        pf.wrow = TW::off(a.wtab, (size_t)z * n + (size_t)q * R);
+        dft_tile<LOGR, TW>(B, tid, a.tw, a.log_n, pf);
         Fr* out = sub + (size_t)z * n + (size_t)q * R;
         for (int c = tid; c < R * 2; c += T) {
             const int h = c & 1, y = c >> 1;
@@ -390,33 +423,39 @@ ntt_fused_extend_kernel(FusedExtendArgs a) {
     }
 }
 
-template <int LOGR>
+template <int LOGR, class TW>
 static cudaError_t launch_fused(const FusedExtendArgs& a, unsigned ncols, cudaStream_t s) {
     constexpr int R = 1 << LOGR;
     const size_t smem = (size_t)(ZK_FUSED_ONE_TILE ? 1 : 2) * R * sizeof(Fr);
     static bool attr_set = false;
     if (!attr_set) {
-        ZK_CHECK(cudaFuncSetAttribute(ntt_fused_extend_kernel<LOGR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        ZK_CHECK(cudaFuncSetAttribute(ntt_fused_extend_kernel<LOGR, TW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)smem));
         attr_set = true;
     }
     dim3 grid(1u << (a.log_n - LOGR), ncols, 1);
-    ntt_fused_extend_kernel<LOGR><<<grid, R / 8, smem, s>>>(a);
+    ntt_fused_extend_kernel<LOGR, TW><<<grid, R / 8, smem, s>>>(a);
     return cudaGetLastError();
 }
 
-cudaError_t ntt_fused_extend(const FusedExtendArgs& a, int log_r, unsigned ncols, cudaStream_t s) {
+template <class TW>
+static cudaError_t fused_dispatch(const FusedExtendArgs& a, int log_r, unsigned ncols, cudaStream_t s) {
     switch (log_r) {
-        case 9: return launch_fused<9>(a, ncols, s);
-        case 10: return launch_fused<10>(a, ncols, s);
-        case 11: return launch_fused<11>(a, ncols, s);
+        case 9: return launch_fused<9, TW>(a, ncols, s);
+        case 10: return launch_fused<10, TW>(a, ncols, s);
+        case 11: return launch_fused<11, TW>(a, ncols, s);
         default: return cudaErrorInvalidValue;
     }
+}
+
+cudaError_t ntt_fused_extend(const FusedExtendArgs& a, int log_r, unsigned ncols, cudaStream_t s) {
+    return a.pairs ? fused_dispatch<TwS>(a, log_r, ncols, s) : fused_dispatch<TwM>(a, log_r, ncols, s);
 }
 
 // Tables of the fused stage for radix R = 2^log_r: wtab[z n + q R + y] =
 // w^(q y) t_z^q (q < n/R, y < R) and stab[z R + i] = (t_z^(n/R))^i, with
 // t_z = shift * w_ext^z and w^k read from the natural table tw.
+template <bool PAIRS>
 __global__ void fused_tables_kernel(Fr* wtab, Fr* stab, const Fr* tw, const Fr* shift, const Fr* w_ext, int log_n,
                                     int log_r) {
     const uint32_t z = blockIdx.y;
@@ -428,21 +467,37 @@ __global__ void fused_tables_kernel(Fr* wtab, Fr* stab, const Fr* tw, const Fr* 
         const Fr tq = fe_pow_u32<FrCfg>(tz, q);
         for (uint32_t y = threadIdx.x; y < R; y += blockDim.x) {
             const Fr w = ld_elem<FrCfg>(tw + (size_t)q * y);
-            st_elem<FrCfg>(wtab + (size_t)z * n + (size_t)q * R + y, y == 0 ? tq : nt_mul(w, tq));
+            st_factor<PAIRS>(wtab, (size_t)z * n + (size_t)q * R + y, y == 0 ? tq : nt_mul(w, tq));
         }
     }
     if (blockIdx.x == 0) {
         const Fr s = fe_pow_u32<FrCfg>(tz, items);
         for (uint32_t i = threadIdx.x; i < R; i += blockDim.x)
-            st_elem<FrCfg>(stab + (size_t)z * R + i, fe_pow_u32<FrCfg>(s, i));
+            st_factor<PAIRS>(stab, (size_t)z * R + i, fe_pow_u32<FrCfg>(s, i));
     }
 }
 
 cudaError_t ntt_fused_tables(Fr* wtab, Fr* stab, const Fr* tw, const Fr* shift, const Fr* w_ext, int log_n, int log_r,
-                             int ext_bits, cudaStream_t s) {
+                             int ext_bits, cudaStream_t s, bool pairs) {
     const uint32_t items = 1u << (log_n - log_r);
     dim3 grid(items < 4096 ? items : 4096, 1u << ext_bits);
-    fused_tables_kernel<<<grid, 256, 0, s>>>(wtab, stab, tw, shift, w_ext, log_n, log_r);
+    if (pairs)
+        fused_tables_kernel<true><<<grid, 256, 0, s>>>(wtab, stab, tw, shift, w_ext, log_n, log_r);
+    else
+        fused_tables_kernel<false><<<grid, 256, 0, s>>>(wtab, stab, tw, shift, w_ext, log_n, log_r);
+    return cudaGetLastError();
+}
+
+// out[i] = (w, w') for the Montgomery-form factors in[i], i < n
+__global__ void shoup_pairs_kernel(Fr* out, const Fr* in, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        st_factor<true>(out, i, ld_elem<FrCfg>(in + i));
+}
+
+cudaError_t shoup_pairs(Fr* out, const Fr* in, size_t n, cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    const size_t blocks = (n + 255) / 256;
+    shoup_pairs_kernel<<<(unsigned)(blocks < 148 * 32 ? blocks : 148 * 32), 256, 0, s>>>(out, in, n);
     return cudaGetLastError();
 }
 
@@ -473,20 +528,20 @@ __global__ void ntt_tiny_kernel(NttPassArgs a) {
 
 // ---------------------------------------------------------------- launchers
 
-template <int LOGR, int G>
+template <int LOGR, int G, class TW>
 static cudaError_t launch_pass(const NttPassArgs& a, unsigned ny, unsigned nz, cudaStream_t s) {
     constexpr int R = 1 << LOGR;
     constexpr int T = (G * R) / 8;
     const size_t smem = (size_t)G * R * sizeof(Fr);
     static bool attr_set = false;
     if (!attr_set) {
-        ZK_CHECK(cudaFuncSetAttribute(ntt_pass_kernel<LOGR, G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        ZK_CHECK(cudaFuncSetAttribute(ntt_pass_kernel<LOGR, G, TW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)smem));
         attr_set = true;
     }
     const unsigned items = 1u << (a.log_n - LOGR);
     dim3 grid(items / G, ny, nz);
-    ntt_pass_kernel<LOGR, G><<<grid, T, smem, s>>>(a);
+    ntt_pass_kernel<LOGR, G, TW><<<grid, T, smem, s>>>(a);
     return cudaGetLastError();
 }
 
@@ -500,14 +555,11 @@ static int pass_group(int log_r, int log_n) {
     return g;
 }
 
-cudaError_t ntt_pass(const NttPassArgs& a, int log_r, unsigned ny, unsigned nz, cudaStream_t s) {
-    if (a.log_n <= 2) {
-        ntt_tiny_kernel<<<dim3(1, ny, nz), 32, 0, s>>>(a);
-        return cudaGetLastError();
-    }
+template <class TW>
+static cudaError_t pass_dispatch(const NttPassArgs& a, int log_r, unsigned ny, unsigned nz, cudaStream_t s) {
     const int g = pass_group(log_r, a.log_n);
 #define ZK_PASS(LR, GG) \
-    if (log_r == LR && g == GG) return launch_pass<LR, GG>(a, ny, nz, s);
+    if (log_r == LR && g == GG) return launch_pass<LR, GG, TW>(a, ny, nz, s);
     ZK_PASS(3, 1) ZK_PASS(4, 1) ZK_PASS(5, 1) ZK_PASS(6, 1) ZK_PASS(7, 1) ZK_PASS(8, 1)
     ZK_PASS(9, 1) ZK_PASS(10, 1) ZK_PASS(11, 1) ZK_PASS(12, 1)
     ZK_PASS(6, 2) ZK_PASS(6, 4) ZK_PASS(6, 8) ZK_PASS(6, 16)
@@ -516,6 +568,15 @@ cudaError_t ntt_pass(const NttPassArgs& a, int log_r, unsigned ny, unsigned nz, 
     ZK_PASS(9, 2)
 #undef ZK_PASS
     return cudaErrorInvalidValue;
+}
+
+cudaError_t ntt_pass(const NttPassArgs& a, int log_r, unsigned ny, unsigned nz, cudaStream_t s) {
+    if (a.log_n <= 2) {
+        if (a.pairs) return cudaErrorInvalidValue;  // the direct kernel reads Montgomery tables
+        ntt_tiny_kernel<<<dim3(1, ny, nz), 32, 0, s>>>(a);
+        return cudaGetLastError();
+    }
+    return a.pairs ? pass_dispatch<TwS>(a, log_r, ny, nz, s) : pass_dispatch<TwM>(a, log_r, ny, nz, s);
 }
 
 // split log_n into pass radices (at most 12 bits per pass, as even as possible)

@@ -296,6 +296,29 @@ def extend_batch(ext_out, coeff_out, lagrange_in, ncols: int, log_n: int, ext_bi
                                      stream_handle(stream)), "zkp_extend_batch")
 
 
+def extend_tables(tw, tw_inv, n_inv, shift, w_ext, log_n: int, ext_bits: int, stream=None) -> torch.Tensor:
+    """Tables of zkp_extend_batch_tables: every twiddle, twist and scale as a
+    (w, w') pair for products by a known factor (tw, tw_inv: natural w_n and
+    w_n^-1 tables; n_inv on the device; shift, w_ext as Montgomery limbs)."""
+    t = empty_fr(lib().zkp_extend_table_elems(log_n, ext_bits))
+    sh = to_device(np.asarray(shift, np.uint64).reshape(1, 4))
+    we = to_device(np.asarray(w_ext, np.uint64).reshape(1, 4))
+    abi.check(lib().zkp_extend_tables(ptr(t), ptr(tw), ptr(tw_inv), ptr(n_inv), ptr(sh), ptr(we), log_n, ext_bits,
+                                      stream_handle(stream)), "zkp_extend_tables")
+    torch.cuda.synchronize()
+    return t
+
+
+def extend_batch_tables(ext_out, coeff_out, lagrange_in, ncols: int, log_n: int, ext_bits: int, tables, scratch,
+                        stage_events=None, stream=None):
+    """zkp_extend_batch_tables: extend_batch over the pair tables of
+    extend_tables."""
+    abi.check(lib().zkp_extend_batch_tables(ptr(ext_out), ptr(coeff_out), ptr(lagrange_in), ncols, log_n, ext_bits,
+                                            ptr(tables), ptr(scratch),
+                                            None if stage_events is None else ctypes.addressof(stage_events),
+                                            stream_handle(stream)), "zkp_extend_batch_tables")
+
+
 def ntt_batch(buf, tmp, omegas, log_n: int, ncols: int, scale=None, stream=None):
     res = ctypes.c_int(0)
     abi.check(lib().zkp_ntt_batch(ptr(buf), ptr(tmp), ptr(omegas), ptr(scale), log_n, ncols, 1 << log_n,
