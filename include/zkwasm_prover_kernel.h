@@ -418,6 +418,10 @@ int zkp_msm_schedule_predict(const float *params, const float *features, int c_m
  * and MSM kernels.  `out` (one element) is written only if the result is 0. */
 cudaError_t zkp_calib_mont_rate(void *out, uint32_t blocks, uint32_t iters, cudaStream_t stream);
 
+/* The same for products by a known factor (the (w, w') pair at `pair`, the
+ * product form of zkp_extend_batch_tables). */
+cudaError_t zkp_calib_shoup_rate(void *out, const void *pair, uint32_t blocks, uint32_t iters, cudaStream_t stream);
+
 /* ======================================================================
  * Part 4: host staging (replaces src/hugetlb.rs and src/async_copy_queue.rs)
  * ==================================================================== */

@@ -90,6 +90,7 @@ SIGNATURES = {
     "zkp_mlp_train_step": [P, P, P, P, P, P, P, U, ctypes.c_float, I, P, P, S],
     "zkp_msm_schedule_predict": ([P, P, I, I, P, S], I),
     "zkp_calib_mont_rate": [P, U, U, S],
+    "zkp_calib_shoup_rate": [P, P, U, U, S],
     # Part 4: host staging (csrc/staging.cu)
     "zkp_host_pool_create": ([SZ, I, I], P),
     "zkp_host_pool_alloc": ([P, SZ], P),

@@ -764,10 +764,40 @@ __global__ void __launch_bounds__(256) mont_rate_kernel(Fr* out, uint32_t iters)
     Fr s = fe_add<FrCfg>(fe_add<FrCfg>(a, b), fe_add<FrCfg>(c, d));
     if (fe_is_zero<FrCfg>(s)) st_elem<FrCfg>(out, s);
 }
+
+// The same for products by a known factor (fe_mul_shoup), the form of every
+// product of the extend-phase kernels over pair tables; wtab[0], wtab[1] is a
+// (w, w') pair.
+__global__ void __launch_bounds__(256) shoup_rate_kernel(Fr* out, const Fr* wtab, uint32_t iters) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    Fr a = fe_one<FrCfg>(), b = fe_one<FrCfg>(), c = fe_one<FrCfg>(), d = fe_one<FrCfg>();
+    a.v[0] ^= t;
+    b.v[1] ^= t;
+    c.v[2] ^= t;
+    d.v[3] ^= t;
+    const Fr w = ld_elem<FrCfg>(wtab), wp = ld_elem<FrCfg>(wtab + 1);
+    for (uint32_t i = 0; i < iters; i++) {
+        a = fe_mul_shoup<FrCfg>(a, w, wp);
+        b = fe_mul_shoup<FrCfg>(b, w, wp);
+        c = fe_mul_shoup<FrCfg>(c, w, wp);
+        d = fe_mul_shoup<FrCfg>(d, w, wp);
+    }
+    Fr s = fe_add<FrCfg>(fe_add<FrCfg>(a, b), fe_add<FrCfg>(c, d));
+    if (fe_is_zero<FrCfg>(s)) st_elem<FrCfg>(out, s);
+}
 }  // namespace zk
 
 extern "C" cudaError_t zkp_calib_mont_rate(void* out, uint32_t blocks, uint32_t iters, cudaStream_t stream) {
     if (!out || blocks == 0) return cudaErrorInvalidValue;
     zk::mont_rate_kernel<<<blocks, 256, 0, stream>>>(F(out), iters);
+    return cudaGetLastError();
+}
+
+// out: one element of scratch (written only when a sum is zero); pair: a
+// (w, w') pair on the device
+extern "C" cudaError_t zkp_calib_shoup_rate(void* out, const void* pair, uint32_t blocks, uint32_t iters,
+                                            cudaStream_t stream) {
+    if (!out || !pair || blocks == 0) return cudaErrorInvalidValue;
+    zk::shoup_rate_kernel<<<blocks, 256, 0, stream>>>(F(out), CF(pair), iters);
     return cudaGetLastError();
 }
