@@ -47,6 +47,34 @@ __device__ __noinline__ Fr nt_mulz(const Fr a, const Fr b) { return fe_mul_lazy<
 __device__ __noinline__ Fr nt_shoup(const Fr a, const Fr w, const Fr wp) { return fe_mul_shoup<FrCfg>(a, w, wp); }
 #endif
 
+// Two or three independent products in one call, so the scheduler can
+// interleave their carry chains.
+struct Fr2 {
+    Fr a, b;
+};
+struct Fr3 {
+    Fr a, b, c;
+};
+#if defined(ZK_NTT_INLINE_MUL)
+#define ZK_NTMUL __device__ __forceinline__
+#else
+#define ZK_NTMUL __device__ __noinline__
+#endif
+ZK_NTMUL Fr2 nt_mulz2(const Fr a0, const Fr w0, const Fr a1, const Fr w1) {
+    return {fe_mul_lazy<FrCfg>(a0, w0), fe_mul_lazy<FrCfg>(a1, w1)};
+}
+ZK_NTMUL Fr3 nt_mulz3(const Fr a0, const Fr w0, const Fr a1, const Fr w1, const Fr a2, const Fr w2) {
+    return {fe_mul_lazy<FrCfg>(a0, w0), fe_mul_lazy<FrCfg>(a1, w1), fe_mul_lazy<FrCfg>(a2, w2)};
+}
+ZK_NTMUL Fr2 nt_shoup2(const Fr a0, const Fr w0, const Fr p0, const Fr a1, const Fr w1, const Fr p1) {
+    return {fe_mul_shoup<FrCfg>(a0, w0, p0), fe_mul_shoup<FrCfg>(a1, w1, p1)};
+}
+ZK_NTMUL Fr3 nt_shoup3(const Fr a0, const Fr w0, const Fr p0, const Fr a1, const Fr w1, const Fr p1, const Fr a2,
+                       const Fr w2, const Fr p2) {
+    return {fe_mul_shoup<FrCfg>(a0, w0, p0), fe_mul_shoup<FrCfg>(a1, w1, p1), fe_mul_shoup<FrCfg>(a2, w2, p2)};
+}
+#undef ZK_NTMUL
+
 // Multiplier tables (twiddles, twists, scales) come in two layouts.
 // TwM: one Montgomery-form element per entry, multiplied with nt_mulz.
 // TwS: the pair (w, w') per entry, w canonical and w' = floor(w 2^256 / r),
@@ -58,6 +86,13 @@ struct TwM {
     };
     static __device__ __forceinline__ K ld(const Fr* t, size_t i) { return {ldg_elem<FrCfg>(t + i)}; }
     static __device__ __forceinline__ Fr mul(const Fr& v, const K& k) { return nt_mulz(v, k.w); }
+    static __device__ __forceinline__ Fr2 mul2(const Fr& v0, const K& k0, const Fr& v1, const K& k1) {
+        return nt_mulz2(v0, k0.w, v1, k1.w);
+    }
+    static __device__ __forceinline__ Fr3 mul3(const Fr& v0, const K& k0, const Fr& v1, const K& k1, const Fr& v2,
+                                               const K& k2) {
+        return nt_mulz3(v0, k0.w, v1, k1.w, v2, k2.w);
+    }
     static __host__ __device__ __forceinline__ const Fr* off(const Fr* t, size_t i) { return t + i; }
 };
 struct TwS {
@@ -68,6 +103,13 @@ struct TwS {
         return {ldg_elem<FrCfg>(t + 2 * i), ldg_elem<FrCfg>(t + 2 * i + 1)};
     }
     static __device__ __forceinline__ Fr mul(const Fr& v, const K& k) { return nt_shoup(v, k.w, k.wp); }
+    static __device__ __forceinline__ Fr2 mul2(const Fr& v0, const K& k0, const Fr& v1, const K& k1) {
+        return nt_shoup2(v0, k0.w, k0.wp, v1, k1.w, k1.wp);
+    }
+    static __device__ __forceinline__ Fr3 mul3(const Fr& v0, const K& k0, const Fr& v1, const K& k1, const Fr& v2,
+                                               const K& k2) {
+        return nt_shoup3(v0, k0.w, k0.wp, v1, k1.w, k1.wp, v2, k2.w, k2.wp);
+    }
     static __host__ __device__ __forceinline__ const Fr* off(const Fr* t, size_t i) { return t + 2 * i; }
 };
 
@@ -100,11 +142,22 @@ __device__ __forceinline__ void dft8_dif(Fr v[8], const typename TW::K& w8, cons
     dft2(v[1], v[5]);
     dft2(v[2], v[6]);
     dft2(v[3], v[7]);
-    v[5] = TW::mul(v[5], w8);
-    v[6] = TW::mul(v[6], w4);
-    v[7] = TW::mul(v[7], w83);
-    dft4_dif<TW>(v[0], v[1], v[2], v[3], w4);
-    dft4_dif<TW>(v[4], v[5], v[6], v[7], w4);
+    const Fr3 m = TW::mul3(v[5], w8, v[6], w4, v[7], w83);
+    v[5] = m.a;
+    v[6] = m.b;
+    v[7] = m.c;
+    // the two radix-4 DFTs side by side
+    dft2(v[0], v[2]);
+    dft2(v[1], v[3]);
+    dft2(v[4], v[6]);
+    dft2(v[5], v[7]);
+    const Fr2 m4 = TW::mul2(v[3], w4, v[7], w4);
+    v[3] = m4.a;
+    v[7] = m4.b;
+    dft2(v[0], v[1]);
+    dft2(v[2], v[3]);
+    dft2(v[4], v[5]);
+    dft2(v[6], v[7]);
 }
 
 // Shared-memory tiles hold 32-byte elements as two 16-byte halves.  Element
@@ -175,11 +228,19 @@ __device__ __forceinline__ void stage8(Fr* x, int u, int log_ps, bool last, cons
     const int ilo = u >> log_ps;
     // y[j] sits in v[rev3(j)]
     const int rev[8] = {0, 4, 2, 6, 1, 5, 3, 7};
+    if (ilo != 0) {
+#pragma unroll
+        for (int j = 1; j < 7; j += 2) {
+            const Fr2 t = TW::mul2(v[rev[j]], TW::ld(tw, (size_t)((ilo * j) << log_ps) << sh), v[rev[j + 1]],
+                                   TW::ld(tw, (size_t)((ilo * (j + 1)) << log_ps) << sh));
+            v[rev[j]] = t.a;
+            v[rev[j + 1]] = t.b;
+        }
+        v[rev[7]] = TW::mul(v[rev[7]], TW::ld(tw, (size_t)((ilo * 7) << log_ps) << sh));
+    }
 #pragma unroll
     for (int j = 0; j < 8; j++) {
         Fr y = v[rev[j]];
-        if (j != 0 && ilo != 0)
-            y = TW::mul(y, TW::ld(tw, (size_t)((ilo * j) << log_ps) << sh));
         const int pos = J + (j << log_ps) + (ilo << (log_ps + 3));
         if (last) y = finish_out<TW>(po, y, (uint32_t)pos);
         sm_st(x, pos, y);
