@@ -50,12 +50,15 @@ def test_ntt_reference_test_input(O, gpu):
 
 def test_expand_omega_buffer_natural(O, gpu):
     H = gpu.host
-    for log_n in (1, 5, 11, 22):
+    # 2^13: every entry (two coarse threads of 64 runs of 64)
+    buf = H.generate_omega_buffers(_omega_mont(O, 13), 13, True)
+    assert (H.to_host(buf) == O.expand_omega(O.omega(13), 13)).all()
+    for log_n in (1, 2, 5, 6, 7, 11, 12, 22):
         buf = H.generate_omega_buffers(_omega_mont(O, log_n), log_n, True)
         got = H.to_host(buf)
         n = 1 << log_n
-        # spot check against w^i
-        idx = sorted({i for i in (0, 1, 2, 3, n // 2, n - 1) if i < n}
+        # spot check against w^i, run and coarse-thread boundaries included
+        idx = sorted({i for i in (0, 1, 2, 3, 63, 64, 65, 4095, 4096, 4097, n // 2, n - 1) if i < n}
                      | set(np.random.default_rng(1).integers(0, n, 50).tolist()))
         w = O.omega(log_n)
         for i in idx:
@@ -122,3 +125,21 @@ def test_extend_batch_matches_coset_ntt(O, gpu, log_n, ext_bits, ncols, pairs):
         co = O.intt(lag[c * n:(c + 1) * n], log_n)
         assert (gc[c * n:(c + 1) * n] == co).all()
         assert (ge[c * E * n:(c + 1) * E * n] == O.coset_ntt(co, log_n, log_n + ext_bits, shift)).all()
+
+
+@pytest.mark.parametrize("n", [1, 2, 63, 64, 65, 4097, 5000, 70000])
+def test_powers(O, gpu, n):
+    # zkp_powers: out[i] = base * w^i for every i < n
+    H = gpu.host
+    base, w = 0x1234567 * 7 % O.R_MOD, O.omega(20)
+    out = H.empty_fr(n)
+    b_dev, w_dev = H.to_device(O.fr(base)), H.to_device(O.fr(w))
+    gpu.abi.check(gpu.load_library().zkp_powers(out.data_ptr(), b_dev.data_ptr(), w_dev.data_ptr(), n,
+                                                H.stream_handle()))
+    torch.cuda.synchronize()
+    got = O.fr_ints(H.to_host(out))
+    exp, v = [], base
+    for _ in range(n):
+        exp.append(v)
+        v = v * w % O.R_MOD
+    assert got == exp

@@ -679,48 +679,58 @@ cudaError_t ntt_run(Fr* buf, Fr* tmp, const Fr* tw, const Fr* scale, int log_n, 
 
 // ---------------------------------------------------------------- tables
 
-// buf[i] = w^i for 2 <= i < n, with w = buf[1] (entries 0 and 1 written by the host)
-__global__ void expand_powers_kernel(Fr* buf, uint32_t n, uint32_t chunk) {
-    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    uint32_t s = t * chunk, e = s + chunk;
-    if (s < 2) s = 2;
-    if (e > n) e = n;
-    if (s >= e) return;
-    Fr w = ld_elem<FrCfg>(buf + 1);
-    Fr cur = fe_pow_u32<FrCfg>(w, s);
-    for (uint32_t i = s; i < e; i++) {
-        st_elem<FrCfg>(buf + i, cur);
-        cur = nt_mul(cur, w);
+// Geometric sequences out[i] = base * w^i for i0 <= i < n (base null: 1) in
+// two launches, one product per element instead of a power per thread:
+//   coarse  out[k C] for every k: a thread takes GEO_C2 consecutive k, starts
+//           from one power and steps by w^C;
+//   fine    the run out[k C + 1 .. k C + C - 1] from out[k C] by steps of w.
+// Each run is C dependent products on one thread, and the thread count stays
+// n / C.
+static constexpr uint32_t GEO_C = 64;
+static constexpr uint32_t GEO_C2 = 64;
+
+__device__ __forceinline__ Fr geo_base(const Fr* base) { return base ? ld_elem<FrCfg>(base) : fe_one<FrCfg>(); }
+
+__global__ void geo_coarse_kernel(Fr* out, const Fr* base, const Fr* w, uint32_t n, uint32_t i0) {
+    const uint64_t k0 = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) * GEO_C2;
+    if (k0 * GEO_C >= n) return;
+    const Fr r = fe_pow_u32<FrCfg>(ld_elem<FrCfg>(w), GEO_C);
+    Fr cur = nt_mul(geo_base(base), fe_pow_u32<FrCfg>(r, (uint32_t)k0));
+    for (uint64_t k = k0; k < k0 + GEO_C2 && k * GEO_C < n; k++) {
+        if (k * GEO_C >= i0) st_elem<FrCfg>(out + k * GEO_C, cur);
+        cur = nt_mul(cur, r);
     }
 }
 
-cudaError_t expand_powers(Fr* buf, uint32_t n, cudaStream_t s) {
-    if (n <= 2) return cudaSuccess;
-    const uint32_t chunk = 16;
-    const uint32_t threads = (n + chunk - 1) / chunk;
-    expand_powers_kernel<<<(threads + 127) / 128, 128, 0, s>>>(buf, n, chunk);
+__global__ void geo_fine_kernel(Fr* out, const Fr* base, const Fr* w, uint32_t n, uint32_t i0) {
+    const uint64_t s = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) * GEO_C;
+    if (s >= n) return;
+    const Fr ww = ld_elem<FrCfg>(w);
+    // a run start below i0 was not written by the coarse pass
+    Fr cur = s >= i0 ? ld_elem<FrCfg>(out + s) : nt_mul(geo_base(base), fe_pow_u32<FrCfg>(ww, (uint32_t)s));
+    for (uint64_t i = s + 1; i < s + GEO_C && i < n; i++) {
+        cur = nt_mul(cur, ww);
+        if (i >= i0) st_elem<FrCfg>(out + i, cur);
+    }
+}
+
+static cudaError_t geometric_from(Fr* out, const Fr* base, const Fr* w, uint32_t n, uint32_t i0, cudaStream_t s) {
+    if (n <= i0) return cudaSuccess;
+    const uint64_t runs = (n + GEO_C - 1) / GEO_C;
+    const uint64_t coarse = (runs + GEO_C2 - 1) / GEO_C2;
+    geo_coarse_kernel<<<(unsigned)((coarse + 127) / 128), 128, 0, s>>>(out, base, w, n, i0);
+    ZK_CHECK(cudaGetLastError());
+    geo_fine_kernel<<<(unsigned)((runs + 127) / 128), 128, 0, s>>>(out, base, w, n, i0);
     return cudaGetLastError();
 }
+
+// buf[i] = w^i for 2 <= i < n, with w = buf[1] (entries 0 and 1 written by the
+// host and left as they are)
+cudaError_t expand_powers(Fr* buf, uint32_t n, cudaStream_t s) { return geometric_from(buf, nullptr, buf + 1, n, 2, s); }
 
 // out[i] = base * w^i for i < n, w and base given by value in device memory
-__global__ void geometric_kernel(Fr* out, const Fr* base, const Fr* w, uint32_t n, uint32_t chunk) {
-    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    uint32_t s = t * chunk, e = s + chunk;
-    if (e > n) e = n;
-    if (s >= e) return;
-    Fr ww = ld_elem<FrCfg>(w);
-    Fr cur = nt_mul(ld_elem<FrCfg>(base), fe_pow_u32<FrCfg>(ww, s));
-    for (uint32_t i = s; i < e; i++) {
-        st_elem<FrCfg>(out + i, cur);
-        cur = nt_mul(cur, ww);
-    }
-}
-
 cudaError_t geometric(Fr* out, const Fr* base, const Fr* w, uint32_t n, cudaStream_t s) {
-    const uint32_t chunk = 16;
-    const uint32_t threads = (n + chunk - 1) / chunk;
-    geometric_kernel<<<(threads + 127) / 128, 128, 0, s>>>(out, base, w, n, chunk);
-    return cudaGetLastError();
+    return geometric_from(out, base, w, n, 0, s);
 }
 
 }  // namespace zk
