@@ -575,7 +575,6 @@ def run_msm_batch(zkp, device, count=32, lo=14, hi=20, seed=2024, reps=3, refere
         b.synchronize()
         return a.elapsed_time(b) / reps
 
-    outs = {}
     pickers = [("default", default), ("learned", learned)]
     if reference_windows:
         ref = [H.msm_window_bits(count, n) for n in ns]
@@ -601,8 +600,26 @@ def run_msm_batch(zkp, device, count=32, lo=14, hi=20, seed=2024, reps=3, refere
         bscr = torch.empty(need, dtype=torch.uint8, device=device)
         bout = torch.empty((count, 12), dtype=torch.int64, device=device)
         res[f"batched_{name}_ms"] = round(timed(lambda: H.msm_batch(bases, cols, ns, ws, scratch=bscr, out=bout)), 3)
-        outs[name] = bout
-        del bscr
+        # the result keeps its scratch alive (tens of GB for a 256-MSM pipeline)
+        del bscr, bout
+    if reference_windows:
+        # the exhaustive autotuner over one window for the whole pipeline
+        tuned = {}
+        n_arr = (ctypes.c_uint32 * count)(*ns)
+        for c in range(10, 20):
+            c_arr = (ctypes.c_int * count)(*([c] * count))
+            need = zkp.load_library().zkp_msm_batch_scratch_bytes(ctypes.addressof(n_arr), ctypes.addressof(c_arr),
+                                                                   count)
+            if need == 0:
+                continue
+            bscr = torch.empty(need, dtype=torch.uint8, device=device)
+            bout = torch.empty((count, 12), dtype=torch.int64, device=device)
+            tuned[c] = timed(lambda: H.msm_batch(bases, cols, ns, [c] * count, scratch=bscr, out=bout))
+            del bscr, bout
+        if tuned:
+            best = min(tuned, key=tuned.get)
+            res["batched_autotuned_one_window"] = {"window_bits": best, "ms": round(tuned[best], 3),
+                                                   "all_ms": {k: round(v, 3) for k, v in sorted(tuned.items())}}
     # one table of the SRS (built once per proving key; the build is timed
     # apart) and one pipeline for the whole batch over it
     nmax = max(ns)
@@ -620,7 +637,7 @@ def run_msm_batch(zkp, device, count=32, lo=14, hi=20, seed=2024, reps=3, refere
         tout = torch.empty((count, 12), dtype=torch.int64, device=device)
         res["batched_table_ms"] = round(timed(lambda: H.msm_batch_table(table, nmax, tc, cols, ns, scratch=tscr,
                                                                          out=tout)), 3)
-        del tscr
+        del tscr, tout
     del table
     if res.get("batched_learned_ms"):
         res["speedup_batched_learned_vs_plain_default"] = round(res["plain_default_ms"] / res["batched_learned_ms"],

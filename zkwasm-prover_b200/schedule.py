@@ -85,8 +85,15 @@ def histogram(s: torch.Tensor) -> list:
     return list(v / max(1.0, v.sum()))
 
 
+# largest batch the model is trained on; larger batches are presented as this
+# one instead of being extrapolated (a 256-MSM pipeline otherwise drew windows
+# of 13 bits for 2^22-point MSMs, against 16 at batch 32)
+BATCH_TRAINED_MAX = 32
+
+
 def shape_features(n: int, batch: int, hist) -> list:
-    return [math.log2(max(n, 1)) / 24.0, math.log2(max(batch, 1)) / 8.0] + [float(x) for x in hist]
+    b = min(max(batch, 1), BATCH_TRAINED_MAX)
+    return [math.log2(max(n, 1)) / 24.0, math.log2(b) / 8.0] + [float(x) for x in hist]
 
 
 def model_input(feats, c: int) -> list:
