@@ -521,14 +521,18 @@ static int pick_c_table(uint32_t n) {
 
 int msm_table_default_window(uint32_t n) { return pick_c_table(n); }
 
-// one width for a batch over one table: each MSM has its own bucket set
+// one width for a batch over one table: each MSM has its own bucket set, and
+// with many sets in one pipeline a bucket costs about 25 sorted entries (their
+// reductions share one thread budget), fitted to 256 MSMs of 2^14..2^22
+// points on B200 (c = 13..17: 456, 450, 431, 413, 429 ms; 19: 525 ms)
 int msm_batch_table_default_window(const uint32_t* n, uint32_t count) {
     double pts = 0;
     for (uint32_t i = 0; i < count; i++) pts += 2.0 * n[i];
+    const double per_bucket = count > 1 ? 25.0 : 5.0;
     int best = 4;
     double best_cost = 1e300;
     for (int c = 4; c <= 22; c++) {
-        const double cost = pts * windows_for(c, true) + 5.0 * count * (double)(1u << (c - 1));
+        const double cost = pts * windows_for(c, true) + per_bucket * count * (double)(1u << (c - 1));
         if (cost < best_cost) {
             best_cost = cost;
             best = c;
