@@ -238,8 +238,9 @@ size_t zkp_msm_batch_scratch_bytes(const uint32_t *n, const int *window_bits, ui
  * msm loop and batch_msm_collect of src/cuda/msm.rs:256-455):
  * out[i] (96-byte Jacobian, contiguous) = sum_{j < n[i]} [scalars[i][j]] bases[j],
  * scalars a device array of `count` device pointers, n and window_bits host
- * arrays.  The descriptor table is uploaded with one cudaMemcpyAsync from
- * host memory; no allocation and no host synchronisation. */
+ * arrays.  The per-MSM descriptors travel as kernel parameters (one small
+ * launch per 64 MSMs), so the call is capturable in a CUDA graph; no
+ * allocation and no host synchronisation. */
 cudaError_t zkp_msm_batch(void *out, const void *bases, const void *scalars, const uint32_t *n,
                           const int *window_bits, uint32_t count, void *scratch, size_t scratch_bytes,
                           cudaStream_t stream);

@@ -193,6 +193,20 @@ __global__ void __launch_bounds__(COOP_THREADS) batch_final_kernel(const BatchDe
     }
 }
 
+// The descriptor table reaches the device through kernel parameters, DESC_CHUNK
+// descriptors per launch (under the 4 KB classic parameter limit): a graph
+// that captures the pipeline keeps them by value, where a copy from host
+// memory would read a host buffer long gone at replay.
+static constexpr uint32_t DESC_CHUNK = 64;
+struct DescChunk {
+    uint32_t count;
+    BatchDesc d[DESC_CHUNK];
+};
+
+__global__ void batch_desc_kernel(BatchDesc* out, DescChunk c) {
+    for (uint32_t i = threadIdx.x; i < c.count; i += blockDim.x) out[i] = c.d[i];
+}
+
 // ------------------------------------------------------------------ planning
 
 struct BatchLayout {
@@ -325,9 +339,13 @@ cudaError_t msm_batch_run(Jac* out, const Aff* bases, const Fr* const* scalars, 
     Xyzz* segsum = reinterpret_cast<Xyzz*>(base + L.off_segsum);
     Xyzz* winsum = reinterpret_cast<Xyzz*>(base + L.off_winsum);
     Aff* phi = reinterpret_cast<Aff*>(base + L.off_phi);
-    // the descriptor table goes up from pageable host memory; the copy is
-    // staged before cudaMemcpyAsync returns, so the vector may go away after
-    ZK_CHECK(cudaMemcpyAsync(d, L.desc.data(), count * sizeof(BatchDesc), cudaMemcpyHostToDevice, st));
+    for (uint32_t i0 = 0; i0 < count; i0 += DESC_CHUNK) {
+        DescChunk ch;
+        ch.count = count - i0 < DESC_CHUNK ? count - i0 : DESC_CHUNK;
+        for (uint32_t i = 0; i < ch.count; i++) ch.d[i] = L.desc[i0 + i];
+        batch_desc_kernel<<<1, DESC_CHUNK, 0, st>>>(d + i0, ch);
+        ZK_CHECK(cudaGetLastError());
+    }
     ZK_CHECK(cudaMemsetAsync(cnt, 0, (size_t)L.NB * 4, st));
     unsigned g1 = (L.total + 255) / 256;
     if (g1 > 148u * 64u) g1 = 148u * 64u;

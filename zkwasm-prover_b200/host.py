@@ -230,12 +230,15 @@ def msm_table(table, nsrs: int, window_bits: int, scalars_buf, n: int | None = N
     return out
 
 
-def msm_batch_table(table, nsrs: int, window_bits: int, scalar_bufs, ns, scratch=None, out=None, stream=None):
+def msm_batch_table(table, nsrs: int, window_bits: int, scalar_bufs, ns, scratch=None, out=None, stream=None,
+                    ptrs=None):
     """zkp_msm_batch_table: len(scalar_bufs) MSMs over prefixes of the bases
-    of one table (msm_table_build); returns (count, 12) int64 Jacobian points."""
+    of one table (msm_table_build); returns (count, 12) int64 Jacobian points.
+    ptrs: the device array of scalar pointers, prepared beforehand (required
+    under CUDA-graph capture, where no host-to-device copy may run)."""
     count = len(scalar_bufs)
     n_arr = (ctypes.c_uint32 * count)(*[int(x) for x in ns])
-    ptrs = ptr_array(scalar_bufs)
+    ptrs = ptr_array(scalar_bufs) if ptrs is None else ptrs
     if scratch is None:
         nbytes = lib().zkp_msm_batch_table_scratch_bytes(ctypes.addressof(n_arr), count, nsrs, window_bits)
         if nbytes == 0:
@@ -250,13 +253,15 @@ def msm_batch_table(table, nsrs: int, window_bits: int, scalar_bufs, ns, scratch
     return out
 
 
-def msm_batch(bases_buf, scalar_bufs, ns, windows=None, scratch=None, out=None, stream=None):
+def msm_batch(bases_buf, scalar_bufs, ns, windows=None, scratch=None, out=None, stream=None, ptrs=None):
     """zkp_msm_batch: one pipeline for len(scalar_bufs) MSMs over the prefix
-    bases_buf[:ns[i]]; returns (count, 12) int64 Jacobian points on the device."""
+    bases_buf[:ns[i]]; returns (count, 12) int64 Jacobian points on the device.
+    ptrs: the device array of scalar pointers, prepared beforehand (required
+    under CUDA-graph capture, where no host-to-device copy may run)."""
     count = len(scalar_bufs)
     n_arr = (ctypes.c_uint32 * count)(*[int(x) for x in ns])
     c_arr = None if windows is None else (ctypes.c_int * count)(*[int(x) for x in windows])
-    ptrs = ptr_array(scalar_bufs)
+    ptrs = ptr_array(scalar_bufs) if ptrs is None else ptrs
     if scratch is None:
         nbytes = lib().zkp_msm_batch_scratch_bytes(ctypes.addressof(n_arr),
                                                    None if c_arr is None else ctypes.addressof(c_arr), count)
