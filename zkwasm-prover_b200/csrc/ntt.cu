@@ -417,9 +417,14 @@ __device__ __forceinline__ void dft_tile(Fr* x, int lt, const Fr* tw, int log_n,
 
 // resident CTAs per SM the register budget is sized for: two tiles of 2^LOGR
 // elements in shared memory allow 7 CTAs of 2^9, 3 of 2^10 and 1 of 2^11; one
-// tile (the coefficients re-read from L2 for each coset) allows 4 of 2^10
+// tile (the coefficients re-read from L2 for each coset) allows 4 of 2^10 and,
+// at 128 registers a thread, 2 of 2^11 (the 2^22 -> 2^25 extension: 82.1 ->
+// 73.0 ms per 8 columns on B200 against one CTA of 255 registers)
+#ifndef ZK_FUSED11_MIN_BLOCKS
+#define ZK_FUSED11_MIN_BLOCKS 2
+#endif
 __host__ __device__ constexpr int fused_min_blocks(int logr) {
-    return logr <= 9 ? 7 : logr == 10 ? (ZK_FUSED_ONE_TILE ? 4 : 3) : 1;
+    return logr <= 9 ? 7 : logr == 10 ? (ZK_FUSED_ONE_TILE ? 4 : 3) : ZK_FUSED11_MIN_BLOCKS;
 }
 
 template <int LOGR, class TW>
