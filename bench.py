@@ -421,7 +421,35 @@ def run_rows(lib, device, mont_rate, peak_hbm, ours=True, log_n=22, log_ext=24, 
             return addr if ours else ctypes.c_void_p(addr)
         if k == S:
             return v if ours else ctypes.c_void_p(v)
+        if k == "hostptr":
+            return ctypes.byref(v)
         return v if ours else ctypes.c_int(v)
+
+    # a6: the drop-in ntt on one column, with each library's own twiddle
+    # table (expand_omega_buffer, as the reference host builds it,
+    # src/cuda/ntt.rs:15-59) and the reference's radix table pq
+    def ntt_case(log_nt):
+        nt = 1 << log_nt
+        w = omega(log_nt)
+        om = torch.zeros((nt, 4), dtype=torch.int64, device=device)
+        om[:2] = fr_tensor([1, w], device)
+        torch.cuda.synchronize()
+        assert lib.expand_omega_buffer(conv((P, om)), conv((I, log_nt)), conv((I, 1))) == 0
+        md = min(8, log_nt)
+        tw8 = pow(w, nt >> md, R_MOD)
+        pq = fr_tensor([pow(tw8, i, R_MOD) for i in range((1 << md) >> 1)], device)
+        buf = random_fr(nt, 1300 + log_nt, device)
+        tmp = torch.empty_like(buf)
+        swap = ctypes.c_bool(False)
+        return (f"a6 ntt (one column, 2^{log_nt})", 2 * nt * E, (nt // 2) * log_nt, "ntt",
+                [(P, buf), (P, tmp), (P, pq), (P, om), (P, None), (I, log_nt), (I, 8), ("hostptr", swap), (S, st)],
+                True), (om, pq, buf, tmp, swap)
+
+    keep = []
+    for lg in (22, 25):
+        case, held = ntt_case(lg)
+        cases.append(case)
+        keep.append(held)
 
     out = []
     for name, nbytes, mults, sym, args, is_ref in cases:
@@ -451,7 +479,7 @@ def run_rows(lib, device, mont_rate, peak_hbm, ours=True, log_n=22, log_ext=24, 
             t_int = mults / mont_rate * 1e3
             row.update(bound="int" if t_int > t_hbm else "hbm", frac=round(max(t_hbm, t_int) / ms, 3))
         out.append(row)
-    del cols, small, res, ext, omega_N, omega_n
+    del cols, small, res, ext, omega_N, omega_n, keep
     return out
 
 

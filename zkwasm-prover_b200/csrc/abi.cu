@@ -439,19 +439,22 @@ cudaError_t zkp_powers(void* out, const void* base, const void* w, uint32_t n, c
 }
 
 #ifndef ZK_EXTEND_SECOND_RADIX
-#define ZK_EXTEND_SECOND_RADIX 0  // 0: the general NTT plan's split
+#define ZK_EXTEND_SECOND_RADIX 0  // 0: the even two-pass split
 #endif
 
-// passes of the extend phase: the NTT plan, or with ZK_EXTEND_SECOND_RADIX a
-// two-pass split whose second (fused) radix is that value
+// passes of the extend phase: one pass up to 2^12, else two (first radix the
+// larger half, at most 2^12), or with ZK_EXTEND_SECOND_RADIX a two-pass split
+// whose second (fused) radix is that value.  The standalone NTT may split the
+// same size into three passes; this phase is built on two.
 static int extend_plan(int log_n, int* rad) {
-    const int np = ntt_plan(log_n, rad);
-    if (ZK_EXTEND_SECOND_RADIX > 0 && np == 2 && log_n - ZK_EXTEND_SECOND_RADIX >= 3 &&
-        log_n - ZK_EXTEND_SECOND_RADIX <= 12) {
+    if (log_n <= 12) return ntt_plan(log_n, rad);
+    rad[0] = (log_n + 1) / 2;
+    rad[1] = log_n / 2;
+    if (ZK_EXTEND_SECOND_RADIX > 0 && log_n - ZK_EXTEND_SECOND_RADIX >= 3 && log_n - ZK_EXTEND_SECOND_RADIX <= 12) {
         rad[1] = ZK_EXTEND_SECOND_RADIX;
         rad[0] = log_n - ZK_EXTEND_SECOND_RADIX;
     }
-    return np;
+    return 2;
 }
 
 // the fused stage applies when the transform takes two passes whose second

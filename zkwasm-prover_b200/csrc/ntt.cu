@@ -645,13 +645,19 @@ cudaError_t ntt_pass(const NttPassArgs& a, int log_r, unsigned ny, unsigned nz, 
     return a.pairs ? pass_dispatch<TwS>(a, log_r, ny, nz, s) : pass_dispatch<TwM>(a, log_r, ny, nz, s);
 }
 
-// split log_n into pass radices (at most 12 bits per pass, as even as possible)
+// split log_n into pass radices (at most ZK_NTT_MAX_PASS_BITS bits per pass,
+// as even as possible).  11: 2^24 runs as three passes of 2^8 (4.25 ms on
+// B200) rather than two of 2^12 (4.78 ms; one 512-thread CTA of 128 KB per
+// SM); 10 would slow 2^21 and 2^22.
+#ifndef ZK_NTT_MAX_PASS_BITS
+#define ZK_NTT_MAX_PASS_BITS 11
+#endif
 int ntt_plan(int log_n, int radices[4]) {
     if (log_n <= 12) {
         radices[0] = log_n;
         return 1;
     }
-    int np = (log_n + 11) / 12;
+    int np = (log_n + ZK_NTT_MAX_PASS_BITS - 1) / ZK_NTT_MAX_PASS_BITS;
     if (np < 2) np = 2;
     for (int i = 0; i < np; i++) radices[i] = log_n / np + (i < log_n % np ? 1 : 0);
     return np;
