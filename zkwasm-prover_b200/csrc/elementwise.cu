@@ -84,21 +84,50 @@ cudaError_t field_op(Fr* res, const Fr* l, int l_rot, const Fr* l_c, const Fr* r
 // v = [coeff0, a00, a01, .., null, coeff1, a10, .., null, ...] (device array of
 // device pointers), rot = rotation per non-coefficient entry.
 
+// The term list (pointers and rotations) is staged in shared memory once per
+// block when it fits (every row walks it), and each term's product is kept
+// lazily reduced in [0, 2r) until the row's sum is stored.
+static constexpr int BMS_SMEM_ENTRIES = 256;
+
 __global__ void batch_mul_sum_kernel(Fr* res, Fr* const* v, const int* rot, int n_v, uint32_t n) {
+    __shared__ const Fr* sv[BMS_SMEM_ENTRIES];
+    __shared__ int srot[BMS_SMEM_ENTRIES];
+    const bool staged = n_v <= BMS_SMEM_ENTRIES;
+    if (staged) {
+        // rotations are indexed by the non-null, non-coefficient entries, at
+        // most n_v of them
+        for (int k = threadIdx.x; k < n_v; k += blockDim.x) sv[k] = v[k];
+        int nrot = 0;
+        {
+            int vi = 0;
+            while (vi < n_v) {
+                vi++;
+                while (vi < n_v && v[vi]) {
+                    vi++;
+                    nrot++;
+                }
+                vi++;
+            }
+        }
+        for (int k = threadIdx.x; k < nrot; k += blockDim.x) srot[k] = rot[k];
+        __syncthreads();
+    }
+    Fr* const* vv = staged ? const_cast<Fr* const*>(reinterpret_cast<const Fr* const*>(sv)) : v;
+    const int* rr = staged ? srot : rot;
     ZK_GRID_LOOP(i, n) {
         Fr acc = fe_zero<FrCfg>();
         int vi = 0, ri = 0;
         while (vi < n_v) {
-            Fr t = ld_elem<FrCfg>(v[vi++]);
-            while (vi < n_v && v[vi]) {
-                t = fe_mul<FrCfg>(t, ld_elem<FrCfg>(v[vi] + rot_pow2(i, rot[ri], n)));
+            Fr t = ld_elem<FrCfg>(vv[vi++]);
+            while (vi < n_v && vv[vi]) {
+                t = fe_mul_lazy<FrCfg>(t, ld_elem<FrCfg>(vv[vi] + rot_pow2(i, rr[ri], n)));
                 vi++;
                 ri++;
             }
-            acc = fe_add<FrCfg>(acc, t);
+            acc = fe_add_lazy<FrCfg>(acc, t);
             vi++;
         }
-        st_elem<FrCfg>(res + i, fe_add<FrCfg>(ld_elem<FrCfg>(res + i), acc));
+        st_elem<FrCfg>(res + i, fe_add<FrCfg>(ld_elem<FrCfg>(res + i), fe_canon<FrCfg>(acc)));
     }
 }
 
@@ -161,12 +190,13 @@ __global__ void perm_p2_kernel(Fr* res, const Fr* const* set, const Fr* l0, cons
         const uint32_t rp = rot_pow2(i, rot, n);
         Fr t1 = ld_elem<FrCfg>(res + i);
         const Fr l = ld_elem<FrCfg>(l0 + i);
+        // lazily reduced in [0, 2r) until the store
         for (int j = 1; j < n_set; j++) {
-            t1 = fe_mul<FrCfg>(t1, yy);
-            Fr t2 = fe_sub<FrCfg>(ld_elem<FrCfg>(set[j] + i), ld_elem<FrCfg>(set[j - 1] + rp));
-            t1 = fe_add<FrCfg>(t1, fe_mul<FrCfg>(t2, l));
+            t1 = fe_mul_lazy<FrCfg>(t1, yy);
+            Fr t2 = fe_sub_lazy<FrCfg>(ld_elem<FrCfg>(set[j] + i), ld_elem<FrCfg>(set[j - 1] + rp));
+            t1 = fe_add_lazy<FrCfg>(t1, fe_mul_lazy<FrCfg>(t2, l));
         }
-        st_elem<FrCfg>(res + i, t1);
+        st_elem<FrCfg>(res + i, fe_canon<FrCfg>(t1));
     }
 }
 
