@@ -131,15 +131,22 @@ __global__ void __launch_bounds__(ST) batch_prod_kernel(Src src, uint32_t n, Fr*
 
 // inv_tots: the inverses of the block products (three-phase form), or null
 // to invert each block's product in the block (one Fermat inversion per block)
+// The per-thread prefix products live in shared memory (SK x ST elements,
+// 64 KB), not registers: at about 80 registers three blocks fit an SM, so
+// while one block waits on its inversion (about 36 us on one thread) two
+// others compute.
+static constexpr size_t BATCH_INV_SMEM = (size_t)SK * ST * sizeof(Fr);
+
 template <class Src, class Dst>
-__global__ void __launch_bounds__(ST) batch_inv_kernel(Src src, Dst dst, uint32_t n, const Fr* inv_tots) {
+__global__ void __launch_bounds__(ST, 3) batch_inv_kernel(Src src, Dst dst, uint32_t n, const Fr* inv_tots) {
     __shared__ Fr wsm[32];
     __shared__ Fr rev[ST];
     __shared__ Fr inv_tot;
+    extern __shared__ uint4 smem_u4[];
+    Fr* pre_sm = reinterpret_cast<Fr*>(smem_u4);  // [k][t]
     const size_t base = (size_t)blockIdx.x * SBLK;
     const int t = threadIdx.x;
     const Fr one = fe_one<FrCfg>();
-    Fr pre[SK];
     Fr run = one;
 #pragma unroll
     for (int k = 0; k < SK; k++) {
@@ -150,7 +157,7 @@ __global__ void __launch_bounds__(ST) batch_inv_kernel(Src src, Dst dst, uint32_
             if (fe_is_zero<FrCfg>(a)) a = one;
         }
         run = fe_mul<FrCfg>(run, a);
-        pre[k] = run;
+        pre_sm[k * ST + t] = run;
     }
     Fr tot;
     Fr E = block_excl_scan_fr(OP_MUL, run, wsm, tot);
@@ -176,7 +183,7 @@ __global__ void __launch_bounds__(ST) batch_inv_kernel(Src src, Dst dst, uint32_
             zero = fe_is_zero<FrCfg>(a);
             if (zero) a = one;
         }
-        Fr inv_k = k ? fe_mul<FrCfg>(cur, pre[k - 1]) : cur;
+        Fr inv_k = k ? fe_mul<FrCfg>(cur, pre_sm[(k - 1) * ST + t]) : cur;
         cur = fe_mul<FrCfg>(cur, a);
         if (i < n) dst((uint32_t)i, zero ? fe_zero<FrCfg>() : inv_k);
     }
@@ -202,6 +209,12 @@ static constexpr uint32_t BATCH_INV_THREE_PHASE_ABOVE = 1u << 22;
 template <class Src, class Dst>
 static cudaError_t launch_batch_inv(Src src, Dst dst, uint32_t n, Fr* scratch, size_t scratch_elems, cudaStream_t s) {
     if (n == 0) return cudaSuccess;
+    static bool attr = false;
+    if (!attr) {
+        ZK_CHECK(cudaFuncSetAttribute(batch_inv_kernel<Src, Dst>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)BATCH_INV_SMEM));
+        attr = true;
+    }
     const uint32_t nb = (n + SBLK - 1) / SBLK;
     if (n > BATCH_INV_THREE_PHASE_ABOVE && scratch && scratch_elems >= batch_inv_scratch_elems(n)) {
         Fr* tot = scratch;
@@ -210,10 +223,10 @@ static cudaError_t launch_batch_inv(Src src, Dst dst, uint32_t n, Fr* scratch, s
         ZK_CHECK(cudaGetLastError());
         ZK_CHECK(launch_batch_inv(SrcPlus{tot, nullptr}, DstStore{inv, 0}, nb, scratch + 2 * (size_t)nb,
                                   scratch_elems - 2 * (size_t)nb, s));
-        batch_inv_kernel<Src, Dst><<<nb, ST, 0, s>>>(src, dst, n, inv);
+        batch_inv_kernel<Src, Dst><<<nb, ST, BATCH_INV_SMEM, s>>>(src, dst, n, inv);
         return cudaGetLastError();
     }
-    batch_inv_kernel<Src, Dst><<<nb, ST, 0, s>>>(src, dst, n, nullptr);
+    batch_inv_kernel<Src, Dst><<<nb, ST, BATCH_INV_SMEM, s>>>(src, dst, n, nullptr);
     return cudaGetLastError();
 }
 
