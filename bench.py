@@ -674,6 +674,13 @@ def run_msm_batch(zkp, device, count=32, lo=14, hi=20, seed=2024, reps=3, refere
     if res.get("batched_table_ms"):
         res["speedup_batched_table_vs_plain_default"] = round(res["plain_default_ms"] / res["batched_table_ms"], 3)
         res["mpts_per_s_batched_table"] = round(res["total_points"] / res["batched_table_ms"] / 1e3, 2)
+    # against the reference host's own plain schedule: one MSM launch per
+    # column with its window formula (src/cuda/msm.rs:105)
+    if res.get("plain_reference_formula_ms"):
+        for k in ("batched_learned_ms", "batched_table_ms"):
+            if res.get(k):
+                res[f"speedup_{k[:-3]}_vs_plain_reference_formula"] = round(
+                    res["plain_reference_formula_ms"] / res[k], 3)
     return res
 
 
