@@ -267,6 +267,17 @@ cudaError_t zkp_msm_batch_table(void *out, const void *table, uint32_t nsrs, int
 cudaError_t zkp_ntt_batch(void *buf, void *tmp, const void *omegas, const void *scale, int log_n, uint32_t ncols,
                           size_t col_stride, int *result_in_tmp, cudaStream_t stream);
 
+/* The library's pass split for a transform of 2^log_n points: writes the
+ * radices (log2, at most 4) and returns their count (0 if unsupported). */
+int zkp_ntt_default_plan(int log_n, int *radices);
+
+/* zkp_ntt_batch with the pass split given (host array of npasses radices,
+ * log2, summing to log_n; each in 6..12 when there is more than one pass), for
+ * a radix autotuner. */
+cudaError_t zkp_ntt_batch_plan(void *buf, void *tmp, const void *omegas, const void *scale, int log_n,
+                               uint32_t ncols, size_t col_stride, const int *radices, int npasses,
+                               int *result_in_tmp, cudaStream_t stream);
+
 /* out[i] = base * w^i for i < n (base and w device scalars). */
 cudaError_t zkp_powers(void *out, const void *base, const void *w, uint32_t n, cudaStream_t stream);
 

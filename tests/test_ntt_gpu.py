@@ -143,3 +143,34 @@ def test_powers(O, gpu, n):
         exp.append(v)
         v = v * w % O.R_MOD
     assert got == exp
+
+
+def test_ntt_every_pass_split_same_result(O, gpu):
+    # every split the radix autotuner may pick gives the same transform
+    H, S = gpu.host, gpu.schedule
+    log_n, ncols = 16, 2
+    n = 1 << log_n
+    a = O.rand_fr(n * ncols, 1401)
+    om = H.generate_omega_buffers(_omega_mont(O, log_n), log_n, False)
+    exp = np.concatenate([O.ntt(a[c * n:(c + 1) * n], log_n) for c in range(ncols)])
+    splits = S.ntt_splits(log_n)
+    assert [10, 6] in splits and [6, 10] in splits and H.ntt_default_plan(log_n) in splits
+    for split in splits:
+        buf, tmp = H.to_device(a), H.empty_fr(n * ncols)
+        out = H.ntt_batch_plan(buf, tmp, om, log_n, ncols, split)
+        torch.cuda.synchronize()
+        assert (H.to_host(out) == exp).all(), split
+
+
+def test_ntt_plan_rejects_bad_splits(gpu):
+    H = gpu.host
+    buf, tmp = H.empty_fr(1 << 16), H.empty_fr(1 << 16)
+    om = H.empty_fr(1 << 16)
+    for bad in ([10, 5], [13, 3], [8, 8, 1], [9, 9]):
+        with pytest.raises(gpu.abi.CudaError):
+            H.ntt_batch_plan(buf, tmp, om, 16, 1, bad)
+
+
+def test_autotune_ntt_picks_a_split(gpu):
+    best, times = gpu.schedule.autotune_ntt(14, ncols=4, reps=1)
+    assert tuple(best) in times and sum(best) == 14 and len(times) == len(gpu.schedule.ntt_splits(14))

@@ -50,3 +50,15 @@ def test_dataset_is_consistent(zkp):
         times = {int(c): v for c, v in r["times_ms"].items()}
         assert r["best"] == min(times, key=times.get)
         assert all(v > 0 and math.isfinite(v) for v in times.values())
+
+
+def test_ntt_splits_enumeration(zkp):
+    # the radix autotuner's candidates: ordered splits into 2-3 passes of 2^6..2^12
+    S = zkp.schedule
+    for log_n in (13, 16, 20, 24, 25):
+        splits = S.ntt_splits(log_n)
+        assert splits and len({tuple(x) for x in splits}) == len(splits)
+        for sp in splits:
+            assert sum(sp) == log_n and 2 <= len(sp) <= 3 and all(6 <= r <= 12 for r in sp)
+    assert sorted(map(tuple, S.ntt_splits(13))) == [(6, 7), (7, 6)]
+    assert [8, 8, 8] in S.ntt_splits(24) and [12, 12] in S.ntt_splits(24)

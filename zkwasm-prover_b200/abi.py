@@ -63,6 +63,8 @@ SIGNATURES = {
     "zkp_msm_batch_scratch_bytes": ([P, P, U], SZ),
     "zkp_msm_batch": [P, P, P, P, P, U, P, SZ, S],
     "zkp_ntt_batch": [P, P, P, P, I, U, SZ, P, S],
+    "zkp_ntt_default_plan": ([I, P], I),
+    "zkp_ntt_batch_plan": [P, P, P, P, I, U, SZ, P, I, P, S],
     "zkp_powers": [P, P, P, U, S],
     "zkp_coset_table_elems": ([I, I], SZ),
     "zkp_coset_twist_tables": [P, P, P, I, I, P, S],

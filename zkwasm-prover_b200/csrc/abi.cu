@@ -432,6 +432,32 @@ cudaError_t zkp_ntt_batch(void* buf, void* tmp, const void* omegas, const void* 
     return cudaGetLastError();
 }
 
+int zkp_ntt_default_plan(int log_n, int* radices) {
+    if (log_n < 1 || log_n > 28 || !radices) return 0;
+    return ntt_plan(log_n, radices);
+}
+
+cudaError_t zkp_ntt_batch_plan(void* buf, void* tmp, const void* omegas, const void* scale, int log_n,
+                               uint32_t ncols, size_t col_stride, const int* radices, int npasses,
+                               int* result_in_tmp, cudaStream_t stream) {
+    if (log_n < 3 || log_n > 28 || !buf || !omegas || !result_in_tmp || !radices || ncols == 0 || ncols > 65535)
+        return cudaErrorInvalidValue;
+    if (npasses < 1 || npasses > 4 || (npasses > 1 && !tmp)) return cudaErrorInvalidValue;
+    int sum = 0;
+    for (int i = 0; i < npasses; i++) {
+        // every pass radix the pass kernels are built for at any size
+        if (npasses > 1 && (radices[i] < 6 || radices[i] > 12)) return cudaErrorInvalidValue;
+        if (npasses == 1 && radices[i] > 12) return cudaErrorInvalidValue;
+        sum += radices[i];
+    }
+    if (sum != log_n) return cudaErrorInvalidValue;
+    bool in_tmp = false;
+    ZK_CHECK(ntt_run_plan(F(buf), F(tmp), CF(omegas), CF(scale), log_n, ncols, col_stride, radices, npasses, &in_tmp,
+                          stream));
+    *result_in_tmp = in_tmp ? 1 : 0;
+    return cudaGetLastError();
+}
+
 cudaError_t zkp_powers(void* out, const void* base, const void* w, uint32_t n, cudaStream_t stream) {
     if (!out || !base || !w) return cudaErrorInvalidValue;
     if (n == 0) return cudaSuccess;

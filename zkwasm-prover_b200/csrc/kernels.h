@@ -51,6 +51,9 @@ int ntt_plan(int log_n, int radices[4]);
 // table tw; result in buf or tmp (*result_in_tmp), multiplied by *scale if given.
 cudaError_t ntt_run(Fr* buf, Fr* tmp, const Fr* tw, const Fr* scale, int log_n, unsigned ncols,
                     size_t col_stride, bool* result_in_tmp, cudaStream_t s);
+// the same with the pass radices given (np passes, sum log_n)
+cudaError_t ntt_run_plan(Fr* buf, Fr* tmp, const Fr* tw, const Fr* scale, int log_n, unsigned ncols,
+                         size_t col_stride, const int* rad, int np, bool* result_in_tmp, cudaStream_t s);
 cudaError_t expand_powers(Fr* buf, uint32_t n, cudaStream_t s);
 cudaError_t geometric(Fr* out, const Fr* base, const Fr* w, uint32_t n, cudaStream_t s);
 

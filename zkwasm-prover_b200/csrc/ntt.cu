@@ -652,10 +652,23 @@ cudaError_t ntt_pass(const NttPassArgs& a, int log_r, unsigned ny, unsigned nz, 
 #ifndef ZK_NTT_MAX_PASS_BITS
 #define ZK_NTT_MAX_PASS_BITS 11
 #endif
+// The splits the radix autotuner (zkp_ntt_batch_plan over every split into
+// 2-3 passes of 2^6..2^12, one column) measured fastest on B200 for 2^13..2^25;
+// other sizes use the even split below.
+static const int8_t TUNED_SPLIT[13][3] = {{7, 6, 0},  {6, 8, 0},  {6, 9, 0},   {8, 8, 0},  {8, 9, 0},
+                                          {9, 9, 0},  {11, 8, 0}, {10, 10, 0}, {11, 10, 0}, {11, 11, 0},
+                                          {11, 6, 6}, {9, 9, 6},  {9, 10, 6}};
+
 int ntt_plan(int log_n, int radices[4]) {
     if (log_n <= 12) {
         radices[0] = log_n;
         return 1;
+    }
+    if (log_n <= 25) {
+        const int8_t* t = TUNED_SPLIT[log_n - 13];
+        const int np = t[2] ? 3 : 2;
+        for (int i = 0; i < np; i++) radices[i] = t[i];
+        return np;
     }
     int np = (log_n + ZK_NTT_MAX_PASS_BITS - 1) / ZK_NTT_MAX_PASS_BITS;
     if (np < 2) np = 2;
@@ -667,6 +680,11 @@ cudaError_t ntt_run(Fr* buf, Fr* tmp, const Fr* tw, const Fr* scale, int log_n, 
                     size_t col_stride, bool* result_in_tmp, cudaStream_t s) {
     int rad[4];
     const int np = ntt_plan(log_n, rad);
+    return ntt_run_plan(buf, tmp, tw, scale, log_n, ncols, col_stride, rad, np, result_in_tmp, s);
+}
+
+cudaError_t ntt_run_plan(Fr* buf, Fr* tmp, const Fr* tw, const Fr* scale, int log_n, unsigned ncols,
+                         size_t col_stride, const int* rad, int np, bool* result_in_tmp, cudaStream_t s) {
     int log_p = 0;
     for (int p = 0; p < np; p++) {
         // one pass runs in place; otherwise ping-pong buf -> tmp -> buf ...

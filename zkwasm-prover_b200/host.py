@@ -331,6 +331,22 @@ def ntt_batch(buf, tmp, omegas, log_n: int, ncols: int, scale=None, stream=None)
     return tmp if res.value else buf
 
 
+def ntt_default_plan(log_n: int) -> list:
+    rad = (ctypes.c_int * 4)()
+    k = lib().zkp_ntt_default_plan(log_n, ctypes.addressof(rad))
+    return [rad[i] for i in range(k)]
+
+
+def ntt_batch_plan(buf, tmp, omegas, log_n: int, ncols: int, radices, scale=None, stream=None):
+    """zkp_ntt_batch with the pass radices given (log2 each)."""
+    rad = (ctypes.c_int * len(radices))(*[int(r) for r in radices])
+    res = ctypes.c_int(0)
+    abi.check(lib().zkp_ntt_batch_plan(ptr(buf), ptr(tmp), ptr(omegas), ptr(scale), log_n, ncols, 1 << log_n,
+                                       ctypes.addressof(rad), len(radices), ctypes.addressof(res),
+                                       stream_handle(stream)), "zkp_ntt_batch_plan")
+    return tmp if res.value else buf
+
+
 def scan_scratch(n: int) -> torch.Tensor:
     return empty_fr(max(1, lib().zkp_scan_scratch_elems(n)))
 

@@ -189,6 +189,65 @@ class Model:
         return c
 
 
+# ------------------------------------------------------------------ NTT radices
+
+
+_R_MOD = 0x30644E72E131A029B85045B68181585D2833E84879B9709143E1F593F0000001
+
+
+def _root_of_unity_mont(log_n: int):
+    """A primitive 2^log_n-th root of unity of Fr (from the generator 7) in
+    Montgomery form, as 4 u64 limbs."""
+    w = pow(7, (_R_MOD - 1) >> log_n, _R_MOD)
+    v = w * (1 << 256) % _R_MOD
+    return np.array([(v >> (64 * i)) & 0xFFFFFFFFFFFFFFFF for i in range(4)], np.uint64)
+
+
+def ntt_splits(log_n: int, lo: int = 6, hi: int = 12, max_passes: int = 3) -> list:
+    """Every ordered split of log_n into 2..max_passes pass radices in [lo, hi]."""
+    out = []
+
+    def rec(left, parts):
+        if left == 0 and len(parts) >= 2:
+            out.append(list(parts))
+            return
+        if len(parts) == max_passes:
+            return
+        for r in range(lo, min(hi, left) + 1):
+            rec(left - r, parts + [r])
+
+    rec(log_n, [])
+    return out
+
+
+def autotune_ntt(log_n: int, ncols: int = 1, reps: int = 3, omegas=None):
+    """Exhaustive search over the pass splits of a batched NTT of ncols columns
+    of 2^log_n points (zkp_ntt_batch_plan on seeded device data); returns
+    (best split, {split: ms}).  Results do not depend on the split (the tests
+    check that), only the time does."""
+    n = 1 << log_n
+    g = torch.Generator(device="cuda")
+    g.manual_seed(log_n)
+    buf = torch.randint(-(2 ** 63), 2 ** 63 - 1, (ncols * n, 4), dtype=torch.int64, device="cuda", generator=g)
+    buf[:, 3] &= (1 << 61) - 1
+    tmp = torch.empty_like(buf)
+    if omegas is None:
+        omegas = H.generate_omega_buffers(_root_of_unity_mont(log_n), log_n, False)
+    times = {}
+    for split in ntt_splits(log_n):
+        H.ntt_batch_plan(buf, tmp, omegas, log_n, ncols, split)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(reps):
+            H.ntt_batch_plan(buf, tmp, omegas, log_n, ncols, split)
+        b.record()
+        b.synchronize()
+        times[tuple(split)] = a.elapsed_time(b) / reps
+    best = min(times, key=times.get)
+    return list(best), times
+
+
 # ------------------------------------------------------------------ dataset / evaluation
 
 
