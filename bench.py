@@ -193,7 +193,7 @@ class ExtendPhase:
         return [c * half, c * (half + n), c * E * (half + n), c * E * half]
 
     def launches_per_step(self):
-        return (self.C // self.chunk) * 4
+        return (self.C // self.chunk) * (3 if self.fused() else 4)
 
     def run_chunk(self, c0, events=None, stream=None, lag=None, coeff=None):
         n, E = self.n, self.E
@@ -901,7 +901,9 @@ def run_ours(args):
             "graph": {"ms_per_step": round(graph_ms, 3),
                       "value": round(total_bytes / (graph_ms / 1e3) / 1e9, 3), "unit": "GB/s",
                       "launches_per_step": 1},
-            "gpu_launches": launches * 4,
+            # kernels per chunk: inverse pass 1, the fused stage and coset
+            # pass 2 (four separate passes without the fused stage)
+            "gpu_launches": launches * (3 if ph.fused() else 4),
             "roofline": {
                 "bound": "hbm", "achieved": round(achieved, 2), "peak": peak_hbm, "unit": "GB/s",
                 "frac": round(achieved / peak_hbm, 4), "traffic": traffic,
