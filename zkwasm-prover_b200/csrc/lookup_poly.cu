@@ -104,12 +104,17 @@ __global__ void horner_level_kernel(const Fr* in, Fr* out, const Fr* x, uint32_t
     for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < count; j += gridDim.x * blockDim.x) {
         const Fr xx = ld_elem<FrCfg>(x);
         const size_t base = (size_t)j * C * stride;
+        // lazily reduced in [0, 2r) until the store
         Fr acc = ld_elem<FrCfg>(in + base + (size_t)(C - 1) * stride);
         for (int i = (int)C - 2; i >= 0; i--)
-            acc = fe_add<FrCfg>(fe_mul<FrCfg>(acc, xx), ld_elem<FrCfg>(in + base + (size_t)i * stride));
-        st_elem<FrCfg>(out + base, acc);
+            acc = fe_add_lazy<FrCfg>(fe_mul_lazy<FrCfg>(acc, xx), ld_elem<FrCfg>(in + base + (size_t)i * stride));
+        st_elem<FrCfg>(out + base, fe_canon<FrCfg>(acc));
     }
 }
+
+#ifndef POLY_EVAL_LOG_CHUNK
+#define POLY_EVAL_LOG_CHUNK 4  // Horner chunks of 16 coefficients
+#endif
 
 cudaError_t poly_eval(const Fr* p, Fr* res, const Fr* x_table, uint32_t n, cudaStream_t s) {
     if (n == 0) return cudaErrorInvalidValue;
@@ -122,7 +127,7 @@ cudaError_t poly_eval(const Fr* p, Fr* res, const Fr* x_table, uint32_t n, cudaS
     const Fr* src = p;
     while (remain > 1) {
         int d = log_n - done;
-        if (d > 4) d = 4;
+        if (d > POLY_EVAL_LOG_CHUNK) d = POLY_EVAL_LOG_CHUNK;
         const uint32_t C = 1u << d;
         const uint32_t count = remain / C;
         horner_level_kernel<<<grid_rows(count), 256, 0, s>>>(src, res, x_table + done, count, C, 1u << done);
