@@ -119,3 +119,10 @@ def test_autotune_picks_fastest_and_is_exact(O, gpu):
         out = H.msm(bases, s, n=n, window_bits=c)
         torch.cuda.synchronize()
         assert (O.g1_jac_to_aff(H.to_host(out).reshape(1, 12)) == exp).all()
+
+
+def test_autotune_extend_small(gpu):
+    # the extend-phase search covers both table layouts and the chunk sizes
+    best, times = gpu.schedule.autotune_extend(14, 2, 4, chunks=(2, 4), reps=1)
+    assert set(times) == {("montgomery", 2), ("pairs", 2), ("montgomery", 4), ("pairs", 4)}
+    assert best in times

@@ -248,6 +248,57 @@ def autotune_ntt(log_n: int, ncols: int = 1, reps: int = 3, omegas=None):
     return list(best), times
 
 
+def autotune_extend(log_n: int, ext_bits: int, ncols: int, chunks=(2, 4, 8, 16), shift: int = 7, reps: int = 2):
+    """Exhaustive search over the run-time choices of the extended-domain phase
+    for ncols columns of 2^log_n points: the multiplier-table layout
+    (zkp_extend_batch over Montgomery tables, or zkp_extend_batch_tables over
+    (w, w') pairs) and the columns per launch.  Returns (best (layout, chunk),
+    {(layout, chunk): ms for the whole phase}).  The outputs do not depend on
+    either choice (the parity tests run both layouts)."""
+    n, E = 1 << log_n, 1 << ext_bits
+    w = pow(7, (_R_MOD - 1) >> log_n, _R_MOD)
+    mont = lambda v: np.array([((v * (1 << 256) % _R_MOD) >> (64 * i)) & 0xFFFFFFFFFFFFFFFF for i in range(4)],
+                              np.uint64)
+    tw = H.generate_omega_buffers(mont(w), log_n, False)
+    tw_inv = H.generate_omega_buffers(mont(pow(w, -1, _R_MOD)), log_n, False)
+    n_inv = H.to_device(mont(pow(n, -1, _R_MOD)).reshape(1, 4))
+    w_ext = pow(7, (_R_MOD - 1) >> (log_n + ext_bits), _R_MOD)
+    twist = H.twist_tables(mont(shift), mont(w_ext), log_n, ext_bits, tw)
+    tables = H.extend_tables(tw, tw_inv, n_inv, mont(shift), mont(w_ext), log_n, ext_bits)
+    g = torch.Generator(device="cuda")
+    g.manual_seed(log_n)
+    lag = torch.randint(-(2 ** 63), 2 ** 63 - 1, (ncols * n, 4), dtype=torch.int64, device="cuda", generator=g)
+    lag[:, 3] &= (1 << 61) - 1
+    coeff = torch.empty_like(lag)
+    ext = torch.empty((ncols * E * n, 4), dtype=torch.int64, device="cuda")
+    times = {}
+    for chunk in chunks:
+        if chunk > ncols or ncols % chunk:
+            continue
+        scratch = torch.empty((chunk * E * n, 4), dtype=torch.int64, device="cuda")
+        for layout in ("montgomery", "pairs"):
+            def phase():
+                for c0 in range(0, ncols, chunk):
+                    if layout == "pairs":
+                        H.extend_batch_tables(ext[c0 * E * n:], coeff[c0 * n:], lag[c0 * n:], chunk, log_n, ext_bits,
+                                              tables, scratch)
+                    else:
+                        H.extend_batch(ext[c0 * E * n:], coeff[c0 * n:], lag[c0 * n:], chunk, log_n, ext_bits,
+                                       tw_inv, n_inv, tw, twist, scratch)
+            phase()
+            torch.cuda.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            for _ in range(reps):
+                phase()
+            b.record()
+            b.synchronize()
+            times[(layout, chunk)] = a.elapsed_time(b) / reps
+        del scratch
+    best = min(times, key=times.get)
+    return best, times
+
+
 # ------------------------------------------------------------------ dataset / evaluation
 
 
