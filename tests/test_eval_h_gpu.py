@@ -97,6 +97,29 @@ def test_field_op_batch_mul_sum(env):
     assert (_get(e, res) == O.field_op_batch_mul_sum(res0, terms, N)).all()
 
 
+def test_field_op_batch_mul_sum_many_groups(env):
+    # the term lists of many gate groups in one call: 75 terms of two columns,
+    # 300 list entries, more than the kernel stages in shared memory
+    e, O = env, env.O
+    res0, res = _res(e, 6)
+    coeffs = O.rand_fr(75, 6)
+    rng = np.random.default_rng(7)
+    terms, v, rot = [], [], []
+    for t in range(75):
+        cs = [(e.cols[int(rng.integers(0, 8))], int(rng.integers(-3, 4))) for _ in range(2)]
+        terms.append((coeffs[t:t + 1], cs))
+        v.append(e.dev(coeffs[t:t + 1]).data_ptr())
+        for col, r in cs:
+            v.append(e.dev(col).data_ptr())
+            rot.append(r)
+        v.append(0)
+    assert len(v) == 300
+    vd = torch.tensor(v, dtype=torch.int64, device="cuda")
+    rd = torch.tensor(rot, dtype=torch.int32, device="cuda")
+    assert e.L.field_op_batch_mul_sum(P(res), P(vd), P(rd), len(v), N, e.st) == 0
+    assert (_get(e, res) == O.field_op_batch_mul_sum(res0, terms, N)).all()
+
+
 def test_permutation_eval_h(env):
     e, O = env, env.O
     l0, ll = e.cols[6], e.cols[7]
