@@ -439,26 +439,17 @@ static int windows_for(int c, bool glv) { return glv ? (128 + c - 1) / c : (254 
 // j directly into the one bucket set of |d|: the sum over windows needs no
 // doublings, and the bucket reduction runs once instead of once per window.
 
-// (X / ZZ, Y / ZZZ) with one inversion: 1 / ZZ = ZZZ / (ZZ ZZZ), 1 / ZZZ = ZZ / (ZZ ZZZ)
-__device__ __forceinline__ Aff xyzz_to_aff(const Xyzz& p) {
-    Aff r;
-    if (xyzz_is_id(p)) {
-        r.x = fe_zero<FqCfg>();
-        r.y = fe_zero<FqCfg>();
-        return r;
-    }
-    const Fq inv = fe_inv<FqCfg>(cmul(p.zz, p.zzz));
-    r.x = cmul(p.x, cmul(inv, p.zzz));
-    r.y = cmul(p.y, cmul(inv, p.zz));
-    return r;
-}
-
 __device__ __forceinline__ void st_aff(Aff* p, const Aff& a) {
     st_elem<FqCfg>(&p->x, a.x);
     st_elem<FqCfg>(&p->y, a.y);
 }
 
-// one thread per base: W windows of c doublings each
+// One thread per base: W windows of c doublings each.  The W - 1 affine
+// conversions share one field inversion (Montgomery's trick over the base's
+// own windows): window j's XYZZ form is parked in its two table slots (X, Y in
+// the base's slot, ZZ, ZZZ in the image's), the product of the ZZ ZZZ is
+// inverted once, and the windows are converted from the last back.  An
+// inversion is about 36 us of one thread, so W - 1 of them dominated the build.
 __global__ void __launch_bounds__(128) msm_table_kernel(Aff* __restrict__ table, const Aff* __restrict__ bases,
                                                         uint32_t nsrs, int c, int W) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -468,11 +459,41 @@ __global__ void __launch_bounds__(128) msm_table_kernel(Aff* __restrict__ table,
     st_aff(table + i, a);
     st_aff(table + nsrs + i, glv_phi(a));
     Xyzz acc = xyzz_from_aff(a);
+    Fq pre[32];  // pre[j] = product of d_1 .. d_{j-1}, d_j = ZZ_j ZZZ_j (1 for the identity); W <= 32
+    Fq run = fe_one<FqCfg>();
     for (int j = 1; j < W; j++) {
         for (int k = 0; k < c; k++) acc = xyzz_dbl(acc);
-        a = xyzz_to_aff(acc);
-        st_aff(table + j * stride + i, a);
-        st_aff(table + j * stride + nsrs + i, glv_phi(a));
+        Aff* slot = table + j * stride + i;
+        Aff* islot = table + j * stride + nsrs + i;
+        st_elem<FqCfg>(&slot->x, acc.x);
+        st_elem<FqCfg>(&slot->y, acc.y);
+        st_elem<FqCfg>(&islot->x, acc.zz);
+        st_elem<FqCfg>(&islot->y, acc.zzz);
+        pre[j] = run;
+        if (!xyzz_is_id(acc)) run = cmul(run, cmul(acc.zz, acc.zzz));
+    }
+    Fq inv = fe_inv<FqCfg>(run);  // 1 / (d_1 ... d_{W-1})
+    for (int j = W - 1; j >= 1; j--) {
+        Aff* slot = table + j * stride + i;
+        Aff* islot = table + j * stride + nsrs + i;
+        Xyzz p;
+        p.x = ld_elem<FqCfg>(&slot->x);
+        p.y = ld_elem<FqCfg>(&slot->y);
+        p.zz = ld_elem<FqCfg>(&islot->x);
+        p.zzz = ld_elem<FqCfg>(&islot->y);
+        Aff r;
+        if (xyzz_is_id(p)) {
+            r.x = fe_zero<FqCfg>();
+            r.y = fe_zero<FqCfg>();
+        } else {
+            const Fq dj = cmul(p.zz, p.zzz);
+            const Fq inv_dj = cmul(inv, pre[j]);  // 1 / d_j
+            inv = cmul(inv, dj);                  // 1 / (d_1 ... d_{j-1})
+            r.x = cmul(p.x, cmul(inv_dj, p.zzz));  // X / ZZ
+            r.y = cmul(p.y, cmul(inv_dj, p.zz));   // Y / ZZZ
+        }
+        st_aff(slot, r);
+        st_aff(islot, glv_phi(r));
     }
 }
 
