@@ -855,6 +855,17 @@ def run_ours(args):
     peak_hbm, peak_kind = load_peaks()
     total_bytes = ws * ph.C * ph.bytes_per_column()
     value = total_bytes / (ms / 1e3) / 1e9
+    # end to end through the C ABI with host buffers, on every rank at once:
+    # the whole-job figure is all ranks' bytes over the slowest rank's time
+    barrier(ws)
+    e2e = run_e2e(ph, max(1, min(args.steps, 3)))
+    e2e_ms = max_over_ranks(e2e["ms_per_step"], ws)
+    e2e.update({"ms_per_step": e2e_ms, "value": ws * ph.C * ph.bytes_per_column() / (e2e_ms / 1e3) / 1e9})
+    # every collective is behind this point: rank 0's remaining work (rates,
+    # the CPU baseline, MSMs, rows) waits on no other rank, and with more than
+    # one rank it is skipped so that the N-GPU run holds its GPUs only for the
+    # phase itself
+    extras = ws == 1
     out = None
     if rank == 0:
         mont_rate = calib_mont_rate(zkp, device)
@@ -862,7 +873,6 @@ def run_ours(args):
         # the phase multiplies by table factors: its product form is the one
         # of its tables
         prod_rate = mont_rate if args.montgomery_tables else shoup_rate
-        e2e = run_e2e(ph, max(1, min(args.steps, 3)))
         sb, sm = ph.stage_bytes()[dom], ph.stage_mults()[dom]
         achieved = sb / (stage_ms[dom] / 1e3) / 1e9
         traffic = None
@@ -870,13 +880,15 @@ def run_ours(args):
         if os.path.exists(prof):
             with open(prof) as f:
                 traffic = json.load(f).get("stage_traffic_bytes", [None] * 4)[dom]
-        cpu = cpu_baseline_port(args.log_n, args.ext_bits) if not args.no_cpu_baseline else None
-        msm = run_msm(zkp, device) if not args.no_msm else None
-        msm_batch = run_msm_batch(zkp, device) if not args.no_msm else None
+        cpu = cpu_baseline_port(args.log_n, args.ext_bits) if extras and not args.no_cpu_baseline else None
+        do_msm = extras and not args.no_msm
+        do_rows = extras and not args.no_rows
+        msm = run_msm(zkp, device) if do_msm else None
+        msm_batch = run_msm_batch(zkp, device) if do_msm else None
         msm_columns = ([run_msm_columns(zkp, device), run_msm_columns(zkp, device, count=8, log_n=22, reps=2)]
-                       if not args.no_msm else None)
-        rows = run_rows(zkp.load_library(), device, mont_rate, peak_hbm) if not args.no_rows else None
-        staging = run_staging(zkp, device) if not args.no_rows else None
+                       if do_msm else None)
+        rows = run_rows(zkp.load_library(), device, mont_rate, peak_hbm) if do_rows else None
+        staging = run_staging(zkp, device) if do_rows else None
         out = {
             "metric": f"NTT HBM GB/s: batched iNTT 2^{args.log_n} -> coset NTT 2^{args.log_n + args.ext_bits}, "
                       f"{args.columns} columns",
