@@ -120,6 +120,66 @@ def test_field_op_batch_mul_sum_many_groups(env):
     assert (_get(e, res) == O.field_op_batch_mul_sum(res0, terms, N)).all()
 
 
+@pytest.mark.parametrize("yv", [0, 1, "m-1"])
+def test_known_factor_edges(env, yv):
+    # the challenge (y, beta) and the gate coefficients enter the products as
+    # known factors: 0, 1 and m - 1, against columns that hold 0 and m - 1
+    e, O = env, env.O
+    yv = O.R_MOD - 1 if yv == "m-1" else yv
+    y = O.fr_vec([yv])
+    c = [x.copy() for x in e.cols]
+    for k in range(8):
+        c[k][k] = O.fr_vec([0])[0]
+        c[k][k + 1] = O.fr_vec([O.R_MOD - 1])[0]
+    res0, res = _res(e, 40)
+    assert e.L.permutation_eval_h_p1(P(res), P(e.dev(c[0])), P(e.dev(c[1])), P(e.dev(c[6])), P(e.dev(c[7])),
+                                     P(e.dev(y)), N) == 0
+    assert (_get(e, res) == O.permutation_eval_h_p1(res0, c[0], c[1], c[6], c[7], y)).all()
+    res0, res = _res(e, 41)
+    assert e.L.permutation_eval_h_p2(P(res), P(e.arr([e.dev(s) for s in c[:4]])), P(e.dev(c[6])), P(e.dev(c[7])),
+                                     P(e.dev(y)), 4, 3, N) == 0
+    assert (_get(e, res) == O.permutation_eval_h_p2(res0, c[:4], c[6], c[7], y, 3)).all()
+    res0, res = _res(e, 42)
+    assert e.L.permutation_eval_h_l(P(res), P(e.dev(y)), P(e.dev(e.gamma)), P(e.dev(c[2])), N, e.st) == 0
+    assert (_get(e, res) == O.permutation_eval_h_l(res0, y, e.gamma, c[2])).all()
+    res0, res = _res(e, 43)
+    assert e.L.logup_eval_h(P(res), *[P(e.dev(x)) for x in c[:8]], P(e.dev(c[0])), P(e.dev(y)), -2, N,
+                            e.st) == 0
+    exp = O.logup_eval_h(res0, c[0], c[1], c[2], c[3], c[4], c[5], c[6], c[7], c[0], y, -2)
+    assert (_get(e, res) == exp).all()
+    res0, res = _res(e, 44)
+    assert e.L.logup_eval_h_extra_inputs(P(res), P(e.dev(c[1])), P(e.dev(c[2])), P(e.dev(c[3])), P(e.dev(c[4])),
+                                         P(e.dev(y)), 1, N, e.st) == 0
+    assert (_get(e, res) == O.logup_eval_h_extra_inputs(res0, c[1], c[2], c[3], c[4], y, 1)).all()
+    res0, res = _res(e, 45)
+    assert e.L.shuffle_eval_h(P(res), *[P(e.dev(x)) for x in c[:6]], P(e.dev(y)), 1, N) == 0
+    assert (_get(e, res) == O.shuffle_eval_h(res0, c[0], c[1], c[2], c[3], c[4], c[5], y, 1)).all()
+    res0, res = _res(e, 46)
+    betas = O.fr_vec([yv, 5, O.R_MOD - 1])
+    assert e.L.shuffle_eval_h_v2(P(res), P(e.arr([e.dev(x) for x in c[:3]])), P(e.arr([e.dev(x) for x in c[3:6]])),
+                                 P(e.dev(betas)), 3, P(e.dev(c[6])), P(e.dev(c[7])), P(e.dev(c[0])),
+                                 P(e.dev(c[1])), P(e.dev(y)), 1, N) == 0
+    exp = O.shuffle_eval_h_v2(res0, c[:3], c[3:6], betas, c[6], c[7], c[0], c[1], y, 1)
+    assert (_get(e, res) == exp).all()
+    # gate terms whose coefficients are the edge value, with a term of no
+    # columns (its coefficient alone) in the middle of the list
+    res0, res = _res(e, 47)
+    coeffs = O.fr_vec([yv, O.R_MOD - 1, yv, 7])
+    terms = [(coeffs[0:1], [(c[0], 0), (c[1], 1)]), (coeffs[1:2], []), (coeffs[2:3], [(c[2], -1)]),
+             (coeffs[3:4], [(c[3], 2), (c[4], 0), (c[5], -2)])]
+    v, rot = [], []
+    for cf, fs in terms:
+        v.append(e.dev(cf).data_ptr())
+        for col, r in fs:
+            v.append(e.dev(col).data_ptr())
+            rot.append(r)
+        v.append(0)
+    vd = torch.tensor(v, dtype=torch.int64, device="cuda")
+    rd = torch.tensor(rot, dtype=torch.int32, device="cuda")
+    assert e.L.field_op_batch_mul_sum(P(res), P(vd), P(rd), len(v), N, e.st) == 0
+    assert (_get(e, res) == O.field_op_batch_mul_sum(res0, terms, N)).all()
+
+
 def test_permutation_eval_h(env):
     e, O = env, env.O
     l0, ll = e.cols[6], e.cols[7]

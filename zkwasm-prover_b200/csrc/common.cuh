@@ -47,6 +47,30 @@ __device__ __forceinline__ void st_factor(Fr* t, size_t i, const Fr& wm) {
     }
 }
 
+// A factor fixed for a whole launch (a challenge such as y or beta, a gate
+// coefficient) in the pair form of fe_mul_shoup, built once from its
+// Montgomery form: every product by it then costs 207 multiply-adds instead of
+// 264 and lands in [0, 2r) like fe_mul_lazy.
+struct KnownFr {
+    Fr w, wp;
+};
+
+__device__ __forceinline__ KnownFr known_fr(const Fr& wm) {
+    const Fr c = fe_canon<FrCfg>(wm);
+    return {fe_from_mont<FrCfg>(c), fe_shoup_companion<FrCfg>(c)};
+}
+
+__device__ __forceinline__ Fr mul_known(const Fr& a, const KnownFr& k) { return fe_mul_shoup<FrCfg>(a, k.w, k.wp); }
+
+// known_fr of the factor at p, built once per block by thread 0 (every thread
+// of the block must call it)
+__device__ __forceinline__ KnownFr block_known(const Fr* p) {
+    __shared__ KnownFr k;
+    if (threadIdx.x == 0) k = known_fr(ld_elem<FrCfg>(p));
+    __syncthreads();
+    return k;
+}
+
 }  // namespace zk
 
 #define ZK_CHECK(x)                           \

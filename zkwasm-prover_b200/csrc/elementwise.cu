@@ -85,42 +85,72 @@ cudaError_t field_op(Fr* res, const Fr* l, int l_rot, const Fr* l_c, const Fr* r
 // device pointers), rot = rotation per non-coefficient entry.
 
 // The term list (pointers and rotations) is staged in shared memory once per
-// block when it fits (every row walks it), and each term's product is kept
-// lazily reduced in [0, 2r) until the row's sum is stored.
+// block when it fits (every row walks it), together with each term's
+// coefficient in the pair form of a known factor, so that a term's first
+// product (coefficient x first column) is a product by a known factor.  Each
+// term's product is kept lazily reduced in [0, 2r) until the row's sum is
+// stored.
 static constexpr int BMS_SMEM_ENTRIES = 256;
+// a term takes at least two entries (its coefficient and its null)
+static constexpr int BMS_SMEM_TERMS = BMS_SMEM_ENTRIES / 2;
 
 __global__ void batch_mul_sum_kernel(Fr* res, Fr* const* v, const int* rot, int n_v, uint32_t n) {
     __shared__ const Fr* sv[BMS_SMEM_ENTRIES];
     __shared__ int srot[BMS_SMEM_ENTRIES];
-    const bool staged = n_v <= BMS_SMEM_ENTRIES;
-    if (staged) {
-        // rotations are indexed by the non-null, non-coefficient entries, at
-        // most n_v of them
+    __shared__ KnownFr scoef[BMS_SMEM_TERMS];
+    if (n_v <= BMS_SMEM_ENTRIES) {
         for (int k = threadIdx.x; k < n_v; k += blockDim.x) sv[k] = v[k];
-        int nrot = 0;
+        __syncthreads();
+        // rotations are indexed by the non-null, non-coefficient entries (at
+        // most n_v of them); term k's coefficient pair is built by thread k
+        int nrot = 0, nterm = 0;
         {
             int vi = 0;
             while (vi < n_v) {
+                if (nterm == (int)threadIdx.x) scoef[nterm] = known_fr(ld_elem<FrCfg>(sv[vi]));
                 vi++;
-                while (vi < n_v && v[vi]) {
+                while (vi < n_v && sv[vi]) {
                     vi++;
                     nrot++;
                 }
                 vi++;
+                nterm++;
             }
         }
         for (int k = threadIdx.x; k < nrot; k += blockDim.x) srot[k] = rot[k];
         __syncthreads();
+        ZK_GRID_LOOP(i, n) {
+            Fr acc = fe_zero<FrCfg>();
+            int vi = 0, ri = 0, tk = 0;
+            while (vi < n_v) {
+                Fr t;
+                if (vi + 1 < n_v && sv[vi + 1]) {
+                    t = mul_known(ld_elem<FrCfg>(sv[vi + 1] + rot_pow2(i, srot[ri], n)), scoef[tk]);
+                    vi += 2;
+                    ri++;
+                } else {
+                    t = ld_elem<FrCfg>(sv[vi++]);  // a term without columns
+                }
+                while (vi < n_v && sv[vi]) {
+                    t = fe_mul_lazy<FrCfg>(t, ld_elem<FrCfg>(sv[vi] + rot_pow2(i, srot[ri], n)));
+                    vi++;
+                    ri++;
+                }
+                acc = fe_add_lazy<FrCfg>(acc, t);
+                vi++;
+                tk++;
+            }
+            st_elem<FrCfg>(res + i, fe_add<FrCfg>(ld_elem<FrCfg>(res + i), fe_canon<FrCfg>(acc)));
+        }
+        return;
     }
-    Fr* const* vv = staged ? const_cast<Fr* const*>(reinterpret_cast<const Fr* const*>(sv)) : v;
-    const int* rr = staged ? srot : rot;
     ZK_GRID_LOOP(i, n) {
         Fr acc = fe_zero<FrCfg>();
         int vi = 0, ri = 0;
         while (vi < n_v) {
-            Fr t = ld_elem<FrCfg>(vv[vi++]);
-            while (vi < n_v && vv[vi]) {
-                t = fe_mul_lazy<FrCfg>(t, ld_elem<FrCfg>(vv[vi] + rot_pow2(i, rr[ri], n)));
+            Fr t = ld_elem<FrCfg>(v[vi++]);
+            while (vi < n_v && v[vi]) {
+                t = fe_mul_lazy<FrCfg>(t, ld_elem<FrCfg>(v[vi] + rot_pow2(i, rot[ri], n)));
                 vi++;
                 ri++;
             }
@@ -164,15 +194,15 @@ cudaError_t extended_prepare(Fr* s, const Fr* coset_powers, uint32_t cpn, uint32
 
 __global__ void perm_p1_kernel(Fr* res, const Fr* first, const Fr* last, const Fr* l0, const Fr* l_last,
                                const Fr* y, uint32_t n) {
-    const Fr yy = ld_elem<FrCfg>(y);
+    const KnownFr ky = block_known(y);
     const Fr one = fe_one<FrCfg>();
     ZK_GRID_LOOP(i, n) {
-        Fr t1 = fe_mul<FrCfg>(ld_elem<FrCfg>(res + i), yy);
-        Fr t2 = fe_mul<FrCfg>(fe_sub<FrCfg>(one, ld_elem<FrCfg>(first + i)), ld_elem<FrCfg>(l0 + i));
-        t1 = fe_mul<FrCfg>(fe_add<FrCfg>(t1, t2), yy);
+        Fr t1 = mul_known(ld_elem<FrCfg>(res + i), ky);
+        Fr t2 = fe_mul_lazy<FrCfg>(fe_sub_lazy<FrCfg>(one, ld_elem<FrCfg>(first + i)), ld_elem<FrCfg>(l0 + i));
+        t1 = mul_known(fe_add_lazy<FrCfg>(t1, t2), ky);
         Fr z = ld_elem<FrCfg>(last + i);
-        t2 = fe_mul<FrCfg>(fe_sub<FrCfg>(fe_sqr<FrCfg>(z), z), ld_elem<FrCfg>(l_last + i));
-        st_elem<FrCfg>(res + i, fe_add<FrCfg>(t1, t2));
+        t2 = fe_mul_lazy<FrCfg>(fe_sub_lazy<FrCfg>(fe_mul_lazy<FrCfg>(z, z), z), ld_elem<FrCfg>(l_last + i));
+        st_elem<FrCfg>(res + i, fe_canon<FrCfg>(fe_add_lazy<FrCfg>(t1, t2)));
     }
 }
 
@@ -183,20 +213,32 @@ cudaError_t permutation_eval_h_p1(Fr* res, const Fr* first_set, const Fr* last_s
     return cudaGetLastError();
 }
 
-__global__ void perm_p2_kernel(Fr* res, const Fr* const* set, const Fr* l0, const Fr* y, int n_set, int rot,
-                               uint32_t n) {
-    const Fr yy = ld_elem<FrCfg>(y);
+// The reference's chain t = t y + (set_j[i] - set_{j-1}[i + rot]) l0 over
+// j = 1 .. k-1 (k = n_set) equals res y^(k-1) + l0 u with
+// u = sum_j y^(k-1-j) (set_j[i] - set_{j-1}[i + rot]) by Horner: k - 1 products
+// by the known factors y and y^(k-1) and one by l0, instead of k - 1 of each.
+__global__ void __launch_bounds__(256, 4) perm_p2_kernel(Fr* res, const Fr* const* set, const Fr* l0, const Fr* y,
+                                                          int n_set, int rot, uint32_t n) {
+    __shared__ KnownFr sk[2];
+    if (threadIdx.x == 0) {
+        const Fr yy = ld_elem<FrCfg>(y);
+        Fr yk = yy;
+        for (int j = 2; j < n_set; j++) yk = fe_mul<FrCfg>(yk, yy);
+        sk[0] = known_fr(yy);
+        sk[1] = known_fr(yk);
+    }
+    __syncthreads();
+    const KnownFr &ky = sk[0], &kyk = sk[1];
     ZK_GRID_LOOP(i, n) {
         const uint32_t rp = rot_pow2(i, rot, n);
-        Fr t1 = ld_elem<FrCfg>(res + i);
-        const Fr l = ld_elem<FrCfg>(l0 + i);
         // lazily reduced in [0, 2r) until the store
-        for (int j = 1; j < n_set; j++) {
-            t1 = fe_mul_lazy<FrCfg>(t1, yy);
-            Fr t2 = fe_sub_lazy<FrCfg>(ld_elem<FrCfg>(set[j] + i), ld_elem<FrCfg>(set[j - 1] + rp));
-            t1 = fe_add_lazy<FrCfg>(t1, fe_mul_lazy<FrCfg>(t2, l));
-        }
-        st_elem<FrCfg>(res + i, fe_canon<FrCfg>(t1));
+        Fr u = fe_sub_lazy<FrCfg>(ld_elem<FrCfg>(set[1] + i), ld_elem<FrCfg>(set[0] + rp));
+        for (int j = 2; j < n_set; j++)
+            u = fe_add_lazy<FrCfg>(mul_known(u, ky),
+                                   fe_sub_lazy<FrCfg>(ld_elem<FrCfg>(set[j] + i), ld_elem<FrCfg>(set[j - 1] + rp)));
+        const Fr t = fe_add_lazy<FrCfg>(mul_known(ld_elem<FrCfg>(res + i), kyk),
+                                        fe_mul_lazy<FrCfg>(u, ld_elem<FrCfg>(l0 + i)));
+        st_elem<FrCfg>(res + i, fe_canon<FrCfg>(t));
     }
 }
 
@@ -208,11 +250,11 @@ cudaError_t permutation_eval_h_p2(Fr* res, const Fr* const* set, const Fr* l0, c
 }
 
 __global__ void perm_l_kernel(Fr* res, const Fr* beta, const Fr* gamma, const Fr* p, uint32_t n) {
-    const Fr b = ld_elem<FrCfg>(beta);
+    const KnownFr kb = block_known(beta);
     ZK_GRID_LOOP(i, n) {
-        Fr t = fe_mul<FrCfg>(ld_elem<FrCfg>(p + i), b);
-        if (i == 0) t = fe_add<FrCfg>(t, ld_elem<FrCfg>(gamma));
-        st_elem<FrCfg>(res + i, fe_add<FrCfg>(ld_elem<FrCfg>(res + i), t));
+        Fr t = mul_known(ld_elem<FrCfg>(p + i), kb);
+        if (i == 0) t = fe_add_lazy<FrCfg>(t, ld_elem<FrCfg>(gamma));
+        st_elem<FrCfg>(res + i, fe_canon<FrCfg>(fe_add_lazy<FrCfg>(ld_elem<FrCfg>(res + i), t)));
     }
 }
 
@@ -228,29 +270,31 @@ cudaError_t permutation_eval_h_l(Fr* res, const Fr* beta, const Fr* gamma, const
 __global__ void lookup_kernel(Fr* res, const Fr* input, const Fr* table, const Fr* pin, const Fr* ptab,
                               const Fr* z, const Fr* l0, const Fr* l_last, const Fr* l_act, const Fr* y,
                               const Fr* beta, const Fr* gamma, int rot, uint32_t n) {
-    const Fr yy = ld_elem<FrCfg>(y), bb = ld_elem<FrCfg>(beta), gg = ld_elem<FrCfg>(gamma);
+    const KnownFr ky = block_known(y);
+    const Fr bb = ld_elem<FrCfg>(beta), gg = ld_elem<FrCfg>(gamma);
     const Fr one = fe_one<FrCfg>();
     ZK_GRID_LOOP(i, n) {
         const uint32_t rn = rot_pow2(i, rot, n), rp = rot_pow2(i, -rot, n);
         const Fr zi = ld_elem<FrCfg>(z + i);
-        Fr t = fe_mul<FrCfg>(ld_elem<FrCfg>(res + i), yy);
-        t = fe_add<FrCfg>(t, fe_mul<FrCfg>(ld_elem<FrCfg>(l0 + i), fe_sub<FrCfg>(one, zi)));
-        t = fe_mul<FrCfg>(t, yy);
-        t = fe_add<FrCfg>(t, fe_mul<FrCfg>(ld_elem<FrCfg>(l_last + i), fe_sub<FrCfg>(fe_sqr<FrCfg>(zi), zi)));
-        t = fe_mul<FrCfg>(t, yy);
+        Fr t = mul_known(ld_elem<FrCfg>(res + i), ky);
+        t = fe_add_lazy<FrCfg>(t, fe_mul_lazy<FrCfg>(ld_elem<FrCfg>(l0 + i), fe_sub_lazy<FrCfg>(one, zi)));
+        t = mul_known(t, ky);
+        t = fe_add_lazy<FrCfg>(t, fe_mul_lazy<FrCfg>(ld_elem<FrCfg>(l_last + i),
+                                                     fe_sub_lazy<FrCfg>(fe_mul_lazy<FrCfg>(zi, zi), zi)));
+        t = mul_known(t, ky);
         const Fr a = ld_elem<FrCfg>(pin + i), sv = ld_elem<FrCfg>(ptab + i);
-        Fr u = fe_mul<FrCfg>(fe_add<FrCfg>(a, bb), fe_add<FrCfg>(sv, gg));
-        u = fe_mul<FrCfg>(u, ld_elem<FrCfg>(z + rn));
-        Fr x = fe_mul<FrCfg>(ld_elem<FrCfg>(input + i), ld_elem<FrCfg>(table + i));
-        u = fe_sub<FrCfg>(u, fe_mul<FrCfg>(zi, x));
-        t = fe_add<FrCfg>(t, fe_mul<FrCfg>(u, ld_elem<FrCfg>(l_act + i)));
-        t = fe_mul<FrCfg>(t, yy);
-        const Fr p = fe_sub<FrCfg>(a, sv);
-        t = fe_add<FrCfg>(t, fe_mul<FrCfg>(ld_elem<FrCfg>(l0 + i), p));
-        t = fe_mul<FrCfg>(t, yy);
-        u = fe_mul<FrCfg>(fe_sub<FrCfg>(a, ld_elem<FrCfg>(pin + rp)), p);
-        t = fe_add<FrCfg>(t, fe_mul<FrCfg>(u, ld_elem<FrCfg>(l_act + i)));
-        st_elem<FrCfg>(res + i, t);
+        Fr u = fe_mul_lazy<FrCfg>(fe_add_lazy<FrCfg>(a, bb), fe_add_lazy<FrCfg>(sv, gg));
+        u = fe_mul_lazy<FrCfg>(u, ld_elem<FrCfg>(z + rn));
+        Fr x = fe_mul_lazy<FrCfg>(ld_elem<FrCfg>(input + i), ld_elem<FrCfg>(table + i));
+        u = fe_sub_lazy<FrCfg>(u, fe_mul_lazy<FrCfg>(zi, x));
+        t = fe_add_lazy<FrCfg>(t, fe_mul_lazy<FrCfg>(u, ld_elem<FrCfg>(l_act + i)));
+        t = mul_known(t, ky);
+        const Fr p = fe_sub_lazy<FrCfg>(a, sv);
+        t = fe_add_lazy<FrCfg>(t, fe_mul_lazy<FrCfg>(ld_elem<FrCfg>(l0 + i), p));
+        t = mul_known(t, ky);
+        u = fe_mul_lazy<FrCfg>(fe_sub_lazy<FrCfg>(a, ld_elem<FrCfg>(pin + rp)), p);
+        t = fe_add_lazy<FrCfg>(t, fe_mul_lazy<FrCfg>(u, ld_elem<FrCfg>(l_act + i)));
+        st_elem<FrCfg>(res + i, fe_canon<FrCfg>(t));
     }
 }
 
@@ -269,22 +313,22 @@ cudaError_t lookup_eval_h(Fr* res, const Fr* input, const Fr* table, const Fr* p
 __global__ void logup_kernel(Fr* res, const Fr* ip, const Fr* ips, const Fr* table, const Fr* m, const Fr* zf,
                              const Fr* zl, const Fr* l0, const Fr* l_last, const Fr* l_act, const Fr* y, int rot,
                              uint32_t n) {
-    const Fr yy = ld_elem<FrCfg>(y);
+    const KnownFr ky = block_known(y);
     ZK_GRID_LOOP(i, n) {
         const uint32_t rn = rot_pow2(i, rot, n);
         const Fr z = ld_elem<FrCfg>(zf + i);
-        Fr t = fe_mul<FrCfg>(ld_elem<FrCfg>(res + i), yy);
-        t = fe_add<FrCfg>(t, fe_mul<FrCfg>(ld_elem<FrCfg>(l0 + i), z));
-        t = fe_mul<FrCfg>(t, yy);
-        t = fe_add<FrCfg>(t, fe_mul<FrCfg>(ld_elem<FrCfg>(l_last + i), ld_elem<FrCfg>(zl + i)));
-        t = fe_mul<FrCfg>(t, yy);
+        Fr t = mul_known(ld_elem<FrCfg>(res + i), ky);
+        t = fe_add_lazy<FrCfg>(t, fe_mul_lazy<FrCfg>(ld_elem<FrCfg>(l0 + i), z));
+        t = mul_known(t, ky);
+        t = fe_add_lazy<FrCfg>(t, fe_mul_lazy<FrCfg>(ld_elem<FrCfg>(l_last + i), ld_elem<FrCfg>(zl + i)));
+        t = mul_known(t, ky);
         const Fr tab = ld_elem<FrCfg>(table + i);
-        Fr u = fe_mul<FrCfg>(fe_sub<FrCfg>(ld_elem<FrCfg>(zf + rn), z), tab);
-        u = fe_add<FrCfg>(u, ld_elem<FrCfg>(m + i));
-        u = fe_mul<FrCfg>(u, ld_elem<FrCfg>(ip + i));
-        u = fe_sub<FrCfg>(u, fe_mul<FrCfg>(tab, ld_elem<FrCfg>(ips + i)));
-        t = fe_add<FrCfg>(t, fe_mul<FrCfg>(u, ld_elem<FrCfg>(l_act + i)));
-        st_elem<FrCfg>(res + i, t);
+        Fr u = fe_mul_lazy<FrCfg>(fe_sub_lazy<FrCfg>(ld_elem<FrCfg>(zf + rn), z), tab);
+        u = fe_add_lazy<FrCfg>(u, ld_elem<FrCfg>(m + i));
+        u = fe_mul_lazy<FrCfg>(u, ld_elem<FrCfg>(ip + i));
+        u = fe_sub_lazy<FrCfg>(u, fe_mul_lazy<FrCfg>(tab, ld_elem<FrCfg>(ips + i)));
+        t = fe_add_lazy<FrCfg>(t, fe_mul_lazy<FrCfg>(u, ld_elem<FrCfg>(l_act + i)));
+        st_elem<FrCfg>(res + i, fe_canon<FrCfg>(t));
     }
 }
 
@@ -299,15 +343,15 @@ cudaError_t logup_eval_h(Fr* res, const Fr* input_product, const Fr* input_produ
 
 __global__ void logup_extra_kernel(Fr* res, const Fr* ip, const Fr* ips, const Fr* z, const Fr* l_act,
                                    const Fr* y, int rot, uint32_t n) {
-    const Fr yy = ld_elem<FrCfg>(y);
+    const KnownFr ky = block_known(y);
     ZK_GRID_LOOP(i, n) {
         const uint32_t rn = rot_pow2(i, rot, n);
-        Fr t = fe_mul<FrCfg>(ld_elem<FrCfg>(res + i), yy);
-        Fr u = fe_sub<FrCfg>(ld_elem<FrCfg>(z + rn), ld_elem<FrCfg>(z + i));
-        u = fe_mul<FrCfg>(u, ld_elem<FrCfg>(ip + i));
-        u = fe_sub<FrCfg>(u, ld_elem<FrCfg>(ips + i));
-        t = fe_add<FrCfg>(t, fe_mul<FrCfg>(u, ld_elem<FrCfg>(l_act + i)));
-        st_elem<FrCfg>(res + i, t);
+        Fr t = mul_known(ld_elem<FrCfg>(res + i), ky);
+        Fr u = fe_sub_lazy<FrCfg>(ld_elem<FrCfg>(z + rn), ld_elem<FrCfg>(z + i));
+        u = fe_mul_lazy<FrCfg>(u, ld_elem<FrCfg>(ip + i));
+        u = fe_sub_lazy<FrCfg>(u, ld_elem<FrCfg>(ips + i));
+        t = fe_add_lazy<FrCfg>(t, fe_mul_lazy<FrCfg>(u, ld_elem<FrCfg>(l_act + i)));
+        st_elem<FrCfg>(res + i, fe_canon<FrCfg>(t));
     }
 }
 
@@ -327,11 +371,11 @@ __global__ void inputs_product_sum_kernel(Fr* prod, Fr* psum, const Fr* const* s
         // running: sum_{j<k} prod_{l<=k, l!=j} a_l  updated as sum = sum * a_k + p_{k-1}
         for (int k = 0; k < n_set; k++) {
             const Fr a = ld_elem<FrCfg>(set[k] + i);
-            sum = fe_add<FrCfg>(fe_mul<FrCfg>(sum, a), p);
-            p = fe_mul<FrCfg>(p, a);
+            sum = fe_add_lazy<FrCfg>(fe_mul_lazy<FrCfg>(sum, a), p);
+            p = fe_mul_lazy<FrCfg>(p, a);
         }
-        st_elem<FrCfg>(prod + i, p);
-        st_elem<FrCfg>(psum + i, sum);
+        st_elem<FrCfg>(prod + i, fe_canon<FrCfg>(p));
+        st_elem<FrCfg>(psum + i, fe_canon<FrCfg>(sum));
     }
 }
 
@@ -344,24 +388,25 @@ cudaError_t logup_eval_h_inputs_product_sum(Fr* product, Fr* product_sum, const 
 
 // -------------------------------------------------------------------- shuffle
 
-__device__ __forceinline__ Fr shuffle_tail(Fr t, const Fr& yy, const Fr& zi, const Fr& zn, const Fr& l0,
+// lhs, rhs lazily reduced; the result canonical
+__device__ __forceinline__ Fr shuffle_tail(Fr t, const KnownFr& ky, const Fr& zi, const Fr& zn, const Fr& l0,
                                            const Fr& ll, const Fr& la, const Fr& lhs, const Fr& rhs) {
     const Fr one = fe_one<FrCfg>();
-    t = fe_mul<FrCfg>(t, yy);
-    t = fe_add<FrCfg>(t, fe_mul<FrCfg>(l0, fe_sub<FrCfg>(one, zi)));
-    t = fe_mul<FrCfg>(t, yy);
-    t = fe_add<FrCfg>(t, fe_mul<FrCfg>(ll, fe_sub<FrCfg>(fe_sqr<FrCfg>(zi), zi)));
-    t = fe_mul<FrCfg>(t, yy);
-    Fr u = fe_sub<FrCfg>(fe_mul<FrCfg>(rhs, zn), fe_mul<FrCfg>(lhs, zi));
-    return fe_add<FrCfg>(t, fe_mul<FrCfg>(u, la));
+    t = mul_known(t, ky);
+    t = fe_add_lazy<FrCfg>(t, fe_mul_lazy<FrCfg>(l0, fe_sub_lazy<FrCfg>(one, zi)));
+    t = mul_known(t, ky);
+    t = fe_add_lazy<FrCfg>(t, fe_mul_lazy<FrCfg>(ll, fe_sub_lazy<FrCfg>(fe_mul_lazy<FrCfg>(zi, zi), zi)));
+    t = mul_known(t, ky);
+    Fr u = fe_sub_lazy<FrCfg>(fe_mul_lazy<FrCfg>(rhs, zn), fe_mul_lazy<FrCfg>(lhs, zi));
+    return fe_canon<FrCfg>(fe_add_lazy<FrCfg>(t, fe_mul_lazy<FrCfg>(u, la)));
 }
 
 __global__ void shuffle_kernel(Fr* res, const Fr* input, const Fr* table, const Fr* z, const Fr* l0,
                                const Fr* l_last, const Fr* l_act, const Fr* y, int rot, uint32_t n) {
-    const Fr yy = ld_elem<FrCfg>(y);
+    const KnownFr ky = block_known(y);
     ZK_GRID_LOOP(i, n) {
         const uint32_t rn = rot_pow2(i, rot, n);
-        Fr t = shuffle_tail(ld_elem<FrCfg>(res + i), yy, ld_elem<FrCfg>(z + i), ld_elem<FrCfg>(z + rn),
+        Fr t = shuffle_tail(ld_elem<FrCfg>(res + i), ky, ld_elem<FrCfg>(z + i), ld_elem<FrCfg>(z + rn),
                             ld_elem<FrCfg>(l0 + i), ld_elem<FrCfg>(l_last + i), ld_elem<FrCfg>(l_act + i),
                             ld_elem<FrCfg>(input + i), ld_elem<FrCfg>(table + i));
         st_elem<FrCfg>(res + i, t);
@@ -378,18 +423,18 @@ cudaError_t shuffle_eval_h(Fr* res, const Fr* input, const Fr* table, const Fr* 
 __global__ void shuffle_v2_kernel(Fr* res, const Fr* const* inputs, const Fr* const* tables, const Fr* betas,
                                   int group_len, const Fr* z, const Fr* l0, const Fr* l_last, const Fr* l_act,
                                   const Fr* y, int rot, uint32_t n) {
-    const Fr yy = ld_elem<FrCfg>(y);
+    const KnownFr ky = block_known(y);
     ZK_GRID_LOOP(i, n) {
         const uint32_t rn = rot_pow2(i, rot, n);
         Fr b = ld_elem<FrCfg>(betas);
-        Fr l = fe_add<FrCfg>(ld_elem<FrCfg>(inputs[0] + i), b);
-        Fr r = fe_add<FrCfg>(ld_elem<FrCfg>(tables[0] + i), b);
+        Fr l = fe_add_lazy<FrCfg>(ld_elem<FrCfg>(inputs[0] + i), b);
+        Fr r = fe_add_lazy<FrCfg>(ld_elem<FrCfg>(tables[0] + i), b);
         for (int j = 1; j < group_len; j++) {
             b = ld_elem<FrCfg>(betas + j);
-            l = fe_mul<FrCfg>(l, fe_add<FrCfg>(ld_elem<FrCfg>(inputs[j] + i), b));
-            r = fe_mul<FrCfg>(r, fe_add<FrCfg>(ld_elem<FrCfg>(tables[j] + i), b));
+            l = fe_mul_lazy<FrCfg>(l, fe_add_lazy<FrCfg>(ld_elem<FrCfg>(inputs[j] + i), b));
+            r = fe_mul_lazy<FrCfg>(r, fe_add_lazy<FrCfg>(ld_elem<FrCfg>(tables[j] + i), b));
         }
-        Fr t = shuffle_tail(ld_elem<FrCfg>(res + i), yy, ld_elem<FrCfg>(z + i), ld_elem<FrCfg>(z + rn),
+        Fr t = shuffle_tail(ld_elem<FrCfg>(res + i), ky, ld_elem<FrCfg>(z + i), ld_elem<FrCfg>(z + rn),
                             ld_elem<FrCfg>(l0 + i), ld_elem<FrCfg>(l_last + i), ld_elem<FrCfg>(l_act + i), l, r);
         st_elem<FrCfg>(res + i, t);
     }
