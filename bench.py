@@ -311,9 +311,13 @@ def run_msm(zkp, device, sizes=(1 << 18, 1 << 22), reps=5):
         line = {"n": n, "ms": round(ms, 4), "mpts_per_s": round(n / ms / 1e3, 2), "window_bits": c}
         # the same MSM over a table of pre-multiplied bases (the bases stay
         # resident across MSMs, as an SRS does); the one-time build is timed
-        # apart
+        # apart, into a buffer allocated before the timed region
+        lib = zkp.load_library()
+        tc = lib.zkp_msm_table_default_window(n)
+        table = torch.empty(lib.zkp_msm_table_bytes(n, tc) // 8, dtype=torch.int64, device=device)
+        torch.cuda.synchronize()
         a.record()
-        table, tc = H.msm_table_build(bases, n)
+        H.msm_table_build(bases, n, tc, table=table)
         b.record()
         b.synchronize()
         build_ms = a.elapsed_time(b)
@@ -664,8 +668,10 @@ def run_msm_batch(zkp, device, count=32, lo=14, hi=20, seed=2024, reps=3, refere
     n_arr = (ctypes.c_uint32 * count)(*ns)
     tc = zkp.load_library().zkp_msm_batch_table_default_window(ctypes.addressof(n_arr), count)
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    table = torch.empty(zkp.load_library().zkp_msm_table_bytes(nmax, tc) // 8, dtype=torch.int64, device=device)
+    torch.cuda.synchronize()
     a.record()
-    table, tc = H.msm_table_build(bases, nmax, tc)
+    H.msm_table_build(bases, nmax, tc, table=table)
     b.record()
     b.synchronize()
     res["table_window_bits"], res["table_build_ms"] = tc, round(a.elapsed_time(b), 2)
@@ -818,6 +824,28 @@ def run_msm_only(args):
     sizes = tuple(1 << int(x) for x in args.msm_log_sizes.split(","))
     print(json.dumps({"metric": "MSM Mpts/s", "msm": run_msm(zkp, torch.device("cuda", 0), sizes=sizes,
                                                             reps=max(1, args.steps))}))
+
+
+def run_rows_only(args):
+    """The per-row kernel timings alone (one JSON line), of this library or,
+    with --impl reference, of the reference's kernels rebuilt for sm_100a;
+    used for profiling those kernels on their own."""
+    torch.cuda.set_device(0)
+    device = torch.device("cuda", 0)
+    zkp = importlib.import_module("zkwasm-prover_b200")
+    lib = zkp.load_library()
+    peak_hbm, _ = load_peaks()
+    mont_rate = calib_mont_rate(zkp, device)
+    reps = max(1, args.steps)
+    if args.impl == "reference":
+        path = os.path.join(ROOT, "oracle", "_ref", "libzkwasm_prover_kernel_ref.so")
+        if not os.path.exists(path):
+            print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built"}))
+            return
+        rows = run_rows(ctypes.CDLL(path), device, mont_rate, peak_hbm, ours=False, reps=reps)
+    else:
+        rows = run_rows(lib, device, mont_rate, peak_hbm, reps=reps)
+    print(json.dumps({"impl": args.impl, "rows": rows}))
 
 
 def run_ours(args):
@@ -1168,8 +1196,12 @@ def main():
     ap.add_argument("--msm-only", action="store_true", help="time only single MSMs (sizes from --msm-log-sizes)")
     ap.add_argument("--msm-log-sizes", default="18,22")
     ap.add_argument("--msm-config-c", action="store_true", help="256 uneven MSMs 2^14..2^22 (about a minute)")
+    ap.add_argument("--rows-only", action="store_true",
+                    help="time only the per-row kernels (with --impl reference: the reference's kernels)")
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.rows_only:
+        run_rows_only(args)
+    elif args.impl == "reference":
         run_reference(args)
     elif args.msm_only:
         run_msm_only(args)

@@ -198,17 +198,21 @@ def msm(points_buf, scalars_buf, n: int | None = None, window_bits: int = 0, scr
     return out
 
 
-def msm_table_build(bases_buf, nsrs: int | None = None, window_bits: int = 0, stream=None):
+def msm_table_build(bases_buf, nsrs: int | None = None, window_bits: int = 0, stream=None, table=None):
     """zkp_msm_table_build: the table of pre-multiplied bases (and their
     endomorphism images) for MSMs over the resident bases_buf[:nsrs];
-    window_bits 0 picks the library's width for nsrs points.  Returns
+    window_bits 0 picks the library's width for nsrs points; table, if
+    given, is a device buffer of at least zkp_msm_table_bytes.  Returns
     (table, window_bits)."""
     nsrs = bases_buf.shape[0] if nsrs is None else nsrs
     c = window_bits or lib().zkp_msm_table_default_window(nsrs)
     nbytes = lib().zkp_msm_table_bytes(nsrs, c)
     if nbytes == 0:
         raise ValueError(f"unsupported table window width {c}")
-    table = torch.empty(nbytes // 8, dtype=torch.int64, device="cuda")
+    if table is None:
+        table = torch.empty(nbytes // 8, dtype=torch.int64, device="cuda")
+    elif table.numel() * table.element_size() < nbytes:
+        raise ValueError(f"table buffer holds {table.numel() * table.element_size()} bytes, {nbytes} needed")
     abi.check(lib().zkp_msm_table_build(ptr(table), ptr(bases_buf), nsrs, c, stream_handle(stream)),
               "zkp_msm_table_build")
     return table, c
