@@ -387,6 +387,11 @@ def run_rows(lib, device, mont_rate, peak_hbm, ours=True, log_n=22, log_ext=24, 
                        cols[2].data_ptr(), 0, cptr[2], cols[3].data_ptr(), cols[4].data_ptr(),
                        cols[5].data_ptr(), 0], dtype=torch.int64, device=device)
     rd = torch.tensor([0, 1, -1, 2, 0, -2], dtype=torch.int32, device=device)
+    # field_sum: sum_j v_j[i] omega^((n + rot_j) i) c_j, one column without
+    # its constant
+    sum_v = ptrs(small[:3])
+    sum_c = torch.tensor([gate_c.data_ptr(), 0, beta.data_ptr()], dtype=torch.int64, device=device)
+    sum_rot = torch.tensor([0, 1, -1], dtype=torch.int32, device=device)
     sets4, ins2, tabs2 = ptrs(cols[:4]), ptrs(small[:2]), ptrs(small[2:4])
     pc, ps = ptrs(small[:4]), ptrs(small[4:8])
     betas2, betas4, xt = fr(2, 909), fr(4, 910), fr(log_n, 911)
@@ -413,6 +418,23 @@ def run_rows(lib, device, mont_rate, peak_hbm, ours=True, log_n=22, log_ext=24, 
          [(P, res)] + [(P, c) for c in cols[:8]] + [(P, cols[0]), (P, y), (I, 4), (I, N), (S, st)], True),
         ("a13 shuffle_eval_h (2^24)", (6 + 2) * N * E, 9 * N, "shuffle_eval_h",
          [(P, res)] + [(P, c) for c in cols[:6]] + [(P, y), (I, 4), (I, N)], True),
+        ("a13 lookup_eval_h (2^24)", (9 + 1) * N * E, 16 * N, "lookup_eval_h",
+         [(P, res)] + [(P, c) for c in cols[:8]] + [(P, y), (P, beta), (P, gamma), (I, 1), (I, N), (S, st)],
+         True),
+        ("a13 field_op (l[i+1] c_l * r[i-1] c_r, 2^24)", 3 * N * E, 3 * N, "field_op",
+         [(P, res), (P, cols[0]), (I, 1), (P, gate_c), (P, cols[1]), (I, -1), (P, beta), (I, N), (I, 1), (S, st)],
+         True),
+        ("a13 field_mul_zip (3 coset powers, 2^24)", 2 * N * E, N, "field_mul_zip",
+         [(P, res), (P, coset), (I, 3), (I, N)], True),
+        ("f2 shplonk_h_x_merge (3 points, 2^22)", 4 * n * E, 4 * n, "shplonk_h_x_merge",
+         [(P, out_n), (P, y), (P, small[6]), (P, small[7]), (P, coset), (I, 3), (I, n)], True),
+        # values / prod_j (w_i - p_j): 4 products, then one batch inversion
+        # (3 products per element) and the quotient (1); the reference
+        # inverts twice per element instead
+        ("f2 shplonk_h_x_div_points (4 points, 2^22)", 3 * n * E, 8 * n, "shplonk_h_x_div_points",
+         [(P, small[4]), (P, small[7]), (P, betas4), (I, 4), (I, n)], True),
+        ("f2 field_sum (3 columns, omega^(rot i), 2^22)", 4 * n * E, 5 * n, "field_sum",
+         [(P, out_n), (P, sum_v), (P, sum_c), (P, sum_rot), (P, small[7]), (I, 3), (I, n)], True),
         ("f1 poly_eval (Horner levels in place, 2^22)", 2 * n * E, n, "poly_eval",
          [(P, small[5]), (P, out_n), (P, xt), (I, n), (S, st)], True),
         ("a9 zkp_batch_inverse (2^22)", 2 * n * E, 3 * n, "zkp_batch_inverse",

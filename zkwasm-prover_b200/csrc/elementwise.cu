@@ -38,19 +38,27 @@ static inline unsigned grid_for(uint32_t n, unsigned tb = 256) {
 
 // ------------------------------------------------------------------ field_op
 
+// a column times its constant is a product by a known factor; operands stay
+// lazily reduced until the store
 __global__ void field_op_kernel(Fr* res, const Fr* l, int l_rot, const Fr* l_c, const Fr* r, int r_rot,
                                 const Fr* r_c, uint32_t n, int op) {
+    __shared__ KnownFr kl, kr;
+    if (threadIdx.x == 0) {
+        if (l && l_c) kl = known_fr(ld_elem<FrCfg>(l_c));
+        if (r && r_c) kr = known_fr(ld_elem<FrCfg>(r_c));
+    }
+    __syncthreads();
     ZK_GRID_LOOP(i, n) {
         Fr fl, fr_;
         if (l) {
             fl = ld_elem<FrCfg>(l + rot_idx(i, l_rot, n));
-            if (l_c) fl = fe_mul<FrCfg>(fl, ld_elem<FrCfg>(l_c));
+            if (l_c) fl = mul_known(fl, kl);
         } else {
             fl = ld_elem<FrCfg>(l_c);
         }
         if (r) {
             fr_ = ld_elem<FrCfg>(r + rot_idx(i, r_rot, n));
-            if (r_c) fr_ = fe_mul<FrCfg>(fr_, ld_elem<FrCfg>(r_c));
+            if (r_c) fr_ = mul_known(fr_, kr);
         } else if (r_c) {
             fr_ = ld_elem<FrCfg>(r_c);
         } else {
@@ -58,13 +66,13 @@ __global__ void field_op_kernel(Fr* res, const Fr* l, int l_rot, const Fr* l_c, 
         }
         Fr out;
         if (op == 0)
-            out = fe_add<FrCfg>(fl, fr_);
+            out = fe_canon<FrCfg>(fe_add_lazy<FrCfg>(fl, fr_));
         else if (op == 1)
             out = fe_mul<FrCfg>(fl, fr_);
         else if (op == 2)
-            out = fl;
+            out = fe_canon<FrCfg>(fl);
         else
-            out = fe_sub<FrCfg>(fl, fr_);
+            out = fe_canon<FrCfg>(fe_sub_lazy<FrCfg>(fl, fr_));
         st_elem<FrCfg>(res + i, out);
     }
 }
@@ -451,7 +459,18 @@ cudaError_t shuffle_eval_h_v2(Fr* res, const Fr* const* inputs, const Fr* const*
 
 // --------------------------------------------------------------- small maps
 
+// up to ZIP_KNOWN coefficients (the coset powers the quotient cycles through)
+// are staged per block as known factors
+static constexpr uint32_t ZIP_KNOWN = 64;
+
 __global__ void mul_zip_kernel(Fr* buf, const Fr* coeff, uint32_t coeff_n, uint32_t n) {
+    __shared__ KnownFr sk[ZIP_KNOWN];
+    if (coeff_n <= ZIP_KNOWN) {
+        for (uint32_t k = threadIdx.x; k < coeff_n; k += blockDim.x) sk[k] = known_fr(ld_elem<FrCfg>(coeff + k));
+        __syncthreads();
+        ZK_GRID_LOOP(i, n) st_elem<FrCfg>(buf + i, fe_canon<FrCfg>(mul_known(ld_elem<FrCfg>(buf + i), sk[i % coeff_n])));
+        return;
+    }
     ZK_GRID_LOOP(i, n) {
         st_elem<FrCfg>(buf + i, fe_mul<FrCfg>(ld_elem<FrCfg>(buf + i), ld_elem<FrCfg>(coeff + i % coeff_n)));
     }
@@ -464,17 +483,28 @@ cudaError_t field_mul_zip(Fr* buf, const Fr* coeff, uint32_t coeff_n, uint32_t n
     return cudaGetLastError();
 }
 
+// the constants c_j of up to SUM_KNOWN columns are staged per block as known
+// factors; the sum stays lazily reduced until the store
+static constexpr int SUM_KNOWN = 64;
+
 __global__ void field_sum_kernel(Fr* res, Fr* const* v, Fr* const* v_c, const int* v_rot, const Fr* omegas,
                                  int v_n, uint32_t n) {
+    __shared__ KnownFr sk[SUM_KNOWN];
+    const bool staged = v_n <= SUM_KNOWN;
+    if (staged) {
+        for (int j = threadIdx.x; j < v_n; j += blockDim.x)
+            if (v_c[j]) sk[j] = known_fr(ld_elem<FrCfg>(v_c[j]));
+        __syncthreads();
+    }
     ZK_GRID_LOOP(i, n) {
         Fr acc = fe_zero<FrCfg>();
         for (int j = 0; j < v_n; j++) {
             const uint32_t e = (uint32_t)(((long long)((int)n + v_rot[j]) * (long long)i) & (long long)(n - 1));
-            Fr t = fe_mul<FrCfg>(ld_elem<FrCfg>(v[j] + i), ld_elem<FrCfg>(omegas + e));
-            if (v_c[j]) t = fe_mul<FrCfg>(t, ld_elem<FrCfg>(v_c[j]));
-            acc = (j == 0) ? t : fe_add<FrCfg>(acc, t);
+            Fr t = fe_mul_lazy<FrCfg>(ld_elem<FrCfg>(v[j] + i), ld_elem<FrCfg>(omegas + e));
+            if (v_c[j]) t = staged ? mul_known(t, sk[j]) : fe_mul_lazy<FrCfg>(t, ld_elem<FrCfg>(v_c[j]));
+            acc = fe_add_lazy<FrCfg>(acc, t);
         }
-        st_elem<FrCfg>(res + i, acc);
+        st_elem<FrCfg>(res + i, fe_canon<FrCfg>(acc));
     }
 }
 
@@ -487,12 +517,12 @@ cudaError_t field_sum(Fr* res, Fr* const* v, Fr* const* v_c, const int* v_rot, c
 
 __global__ void shplonk_merge_kernel(Fr* res, const Fr* v, const Fr* values, const Fr* omegas, const Fr* diff,
                                      int nd, uint32_t n) {
-    const Fr vv = ld_elem<FrCfg>(v);
+    const KnownFr kv = block_known(v);
     ZK_GRID_LOOP(i, n) {
         Fr t = ld_elem<FrCfg>(values + i);
         const Fr w = ld_elem<FrCfg>(omegas + i);
-        for (int j = 0; j < nd; j++) t = fe_mul<FrCfg>(t, fe_sub<FrCfg>(w, ld_elem<FrCfg>(diff + j)));
-        st_elem<FrCfg>(res + i, fe_add<FrCfg>(fe_mul<FrCfg>(ld_elem<FrCfg>(res + i), vv), t));
+        for (int j = 0; j < nd; j++) t = fe_mul_lazy<FrCfg>(t, fe_sub_lazy<FrCfg>(w, ld_elem<FrCfg>(diff + j)));
+        st_elem<FrCfg>(res + i, fe_canon<FrCfg>(fe_add_lazy<FrCfg>(mul_known(ld_elem<FrCfg>(res + i), kv), t)));
     }
 }
 
