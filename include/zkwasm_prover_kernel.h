@@ -369,9 +369,8 @@ cudaError_t zkp_shuffle_z(void *z, const void *inputs, const void *tables, const
 
 /* No counterpart in the reference.  zkp_msm without caller-supplied scratch,
  * for callers that cannot allocate device memory: a host whose device memory
- * is all owned by its own pool, code running during CUDA-graph capture, or a
- * latency-critical path that cannot afford cudaMalloc's implicit device
- * synchronisation.  out (96-byte Jacobian) = sum_i [scalars_i] bases_i for
+ * is all owned by its own pool, or a latency-critical path that cannot afford
+ * cudaMalloc's implicit device synchronisation.  out (96-byte Jacobian) = sum_i [scalars_i] bases_i for
  * n <= 16384 points; larger n returns cudaErrorInvalidValue without launching.
  * The scratch is a 9 MiB __device__ array inside the library (one per GPU
  * that loads it, held until exit) shared by every call: calls that overlap on

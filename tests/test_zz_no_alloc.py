@@ -1,7 +1,7 @@
 """zkp_msm_static: the MSM entry point for callers that cannot allocate device
-memory (a host whose device memory is all owned by its own pool, code inside
-CUDA-graph capture, latency-critical paths that cannot take cudaMalloc's
-implicit synchronisation).  Its scratch is a fixed array inside the library,
+memory (a host whose device memory is all owned by its own pool, or a
+latency-critical path that cannot take cudaMalloc's implicit
+synchronisation).  Its scratch is a fixed array inside the library,
 so this file checks, through the C ABI, that two calls in a row (the second
 sees the first call's leftovers in that array) return the same points as the
 existing zkp_msm entry point, and that oversized inputs are refused.

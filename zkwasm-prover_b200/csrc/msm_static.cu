@@ -1,9 +1,8 @@
 // MSM entry point that allocates nothing, for callers that cannot call
 // cudaMalloc: a host whose device memory is entirely owned by its own pool
 // (the prover reserves one pool up front and a stray allocation either fails
-// or fragments it), code running while a stream is being captured into a CUDA
-// graph, and latency-critical paths that must not pay cudaMalloc's implicit
-// device synchronisation.  Such callers cannot size and hand over the scratch
+// or fragments it), and latency-critical paths that must not pay cudaMalloc's
+// implicit device synchronisation.  Such callers cannot size and hand over the scratch
 // that zkp_msm takes either, so this variant keeps its scratch in a fixed
 // device array inside the library.
 //
