@@ -63,12 +63,15 @@ __device__ __forceinline__ KnownFr known_fr(const Fr& wm) {
 __device__ __forceinline__ Fr mul_known(const Fr& a, const KnownFr& k) { return fe_mul_shoup<FrCfg>(a, k.w, k.wp); }
 
 // known_fr of the factor at p, built once per block by thread 0 (every thread
-// of the block must call it)
+// of the block must call it); the second barrier lets a kernel call it again
+// without thread 0 overwriting the slot before every thread has read it
 __device__ __forceinline__ KnownFr block_known(const Fr* p) {
     __shared__ KnownFr k;
     if (threadIdx.x == 0) k = known_fr(ld_elem<FrCfg>(p));
     __syncthreads();
-    return k;
+    const KnownFr r = k;
+    __syncthreads();
+    return r;
 }
 
 }  // namespace zk

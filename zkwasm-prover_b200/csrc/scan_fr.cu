@@ -366,31 +366,43 @@ cudaError_t logup_z_compose(Fr* z, const Fr* sum, const Fr* table, const Fr* m, 
 
 __global__ void perm_den_kernel(Fr* den, const Fr* const* cols, const Fr* const* sig, int ncols, const Fr* beta,
                                 const Fr* gamma, uint32_t n) {
-    const Fr b = ld_elem<FrCfg>(beta), g = ld_elem<FrCfg>(gamma);
+    // beta is a known factor; the product stays lazily reduced until the store
+    const KnownFr kb = block_known(beta);
+    const Fr g = ld_elem<FrCfg>(gamma);
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         Fr acc = fe_one<FrCfg>();
         for (int c = 0; c < ncols; c++) {
-            Fr t = fe_add<FrCfg>(fe_add<FrCfg>(fe_mul<FrCfg>(ld_elem<FrCfg>(sig[c] + i), b), g),
-                                 ld_elem<FrCfg>(cols[c] + i));
-            acc = fe_mul<FrCfg>(acc, t);
+            const Fr t = fe_add_lazy<FrCfg>(fe_add_lazy<FrCfg>(mul_known(ld_elem<FrCfg>(sig[c] + i), kb), g),
+                                            ld_elem<FrCfg>(cols[c] + i));
+            acc = c ? fe_mul_lazy<FrCfg>(acc, t) : t;
         }
-        st_elem<FrCfg>(den + i, acc);
+        st_elem<FrCfg>(den + i, fe_canon<FrCfg>(acc));
     }
 }
 
-// d[i] = inv_den[i] * prod_c (v_c[i] + beta*delta^c*w^i + gamma); omega table w^i
+// d[i] = inv_den[i] * prod_c (v_c[i] + beta*delta^c*w^i + gamma); omega table
+// w^i.  The beta delta^c of up to PERM_KNOWN columns are staged per block as
+// known factors; the product stays lazily reduced until the store.
+static constexpr int PERM_KNOWN = 64;
+
 __global__ void perm_num_kernel(Fr* d, const Fr* const* cols, const Fr* dbeta, int ncols, const Fr* gamma,
                                 const Fr* omegas, uint32_t n) {
+    __shared__ KnownFr sk[PERM_KNOWN];
+    const bool staged = ncols <= PERM_KNOWN;
+    if (staged) {
+        for (int c = threadIdx.x; c < ncols; c += blockDim.x) sk[c] = known_fr(ld_elem<FrCfg>(dbeta + c));
+        __syncthreads();
+    }
     const Fr g = ld_elem<FrCfg>(gamma);
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const Fr w = ld_elem<FrCfg>(omegas + i);
         Fr acc = ld_elem<FrCfg>(d + i);
         for (int c = 0; c < ncols; c++) {
-            Fr t = fe_add<FrCfg>(fe_add<FrCfg>(fe_mul<FrCfg>(w, ld_elem<FrCfg>(dbeta + c)), g),
-                                 ld_elem<FrCfg>(cols[c] + i));
-            acc = fe_mul<FrCfg>(acc, t);
+            const Fr wb = staged ? mul_known(w, sk[c]) : fe_mul_lazy<FrCfg>(w, ld_elem<FrCfg>(dbeta + c));
+            const Fr t = fe_add_lazy<FrCfg>(fe_add_lazy<FrCfg>(wb, g), ld_elem<FrCfg>(cols[c] + i));
+            acc = fe_mul_lazy<FrCfg>(acc, t);
         }
-        st_elem<FrCfg>(d + i, acc);
+        st_elem<FrCfg>(d + i, fe_canon<FrCfg>(acc));
     }
 }
 
@@ -418,14 +430,15 @@ cudaError_t permutation_chunk_z(Fr* z, const Fr* const* cols, const Fr* const* s
 __global__ void shuffle_terms_kernel(Fr* den, Fr* num, const Fr* const* inputs, const Fr* const* tables,
                                      const Fr* betas, int groups, uint32_t n) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        // lazily reduced until the stores
         Fr a = fe_one<FrCfg>(), b = fe_one<FrCfg>();
         for (int g = 0; g < groups; g++) {
             const Fr bg = ld_elem<FrCfg>(betas + g);
-            a = fe_mul<FrCfg>(a, fe_add<FrCfg>(ld_elem<FrCfg>(inputs[g] + i), bg));
-            b = fe_mul<FrCfg>(b, fe_add<FrCfg>(ld_elem<FrCfg>(tables[g] + i), bg));
+            a = fe_mul_lazy<FrCfg>(a, fe_add_lazy<FrCfg>(ld_elem<FrCfg>(inputs[g] + i), bg));
+            b = fe_mul_lazy<FrCfg>(b, fe_add_lazy<FrCfg>(ld_elem<FrCfg>(tables[g] + i), bg));
         }
-        st_elem<FrCfg>(num + i, a);
-        st_elem<FrCfg>(den + i, b);
+        st_elem<FrCfg>(num + i, fe_canon<FrCfg>(a));
+        st_elem<FrCfg>(den + i, fe_canon<FrCfg>(b));
     }
 }
 
