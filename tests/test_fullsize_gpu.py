@@ -9,6 +9,8 @@ first chunk and the last column of the last chunk with the oracle's coset DFT.
 The MSMs use the reference's known-discrete-log identity
 (src/cuda/msm.rs:501-512): with bases P_i = [d_i]G, sum_i [s_i] P_i equals
 [sum_i s_i d_i] G, which the oracle evaluates in O(n) at any size."""
+import ctypes
+
 import numpy as np
 import pytest
 import torch
@@ -55,12 +57,12 @@ def msm_2p22(O):
     n = 1 << 22
     d = O.rand_fr(n, 5151)
     s = O.rand_fr(n, 5152)
-    return n, O.g1_gen_bases(d), s, O.msm_known_dlog(d, s)
+    return n, O.g1_gen_bases(d), s, O.msm_known_dlog(d, s), d
 
 
 def test_msm_2p22_known_dlog(O, gpu, msm_2p22):
     H = gpu.host
-    n, bases, s, exp = msm_2p22
+    n, bases, s, exp, _ = msm_2p22
     out = H.msm(H.to_device(bases), H.to_device(s), n=n)
     torch.cuda.synchronize()
     assert (O.g1_jac_to_aff(H.to_host(out).reshape(1, 12)) == exp).all()
@@ -68,9 +70,43 @@ def test_msm_2p22_known_dlog(O, gpu, msm_2p22):
 
 def test_msm_table_2p22_known_dlog(O, gpu, msm_2p22):
     H = gpu.host
-    n, bases, s, exp = msm_2p22
+    n, bases, s, exp, _ = msm_2p22
     table, c = H.msm_table_build(H.to_device(bases), n)
     for _ in range(2):  # the second call runs on the first call's scratch contents
         out = H.msm_table(table, n, c, H.to_device(s), n=n)
         torch.cuda.synchronize()
         assert (O.g1_jac_to_aff(H.to_host(out).reshape(1, 12)) == exp).all()
+
+
+def test_msm_batch_uneven_over_one_srs(O, gpu, msm_2p22):
+    """24 MSMs over prefixes of one 2^22-point SRS, sizes 2^14..2^22 (one of
+    each end), uniform, witness-like (< 2^20), sparse and mixed scalars: one
+    pipeline with the library's windows, one with the learned windows, and one
+    over a table of the SRS, each against the known-discrete-log identity."""
+    import importlib
+
+    H = gpu.host
+    S = importlib.import_module("zkwasm-prover_b200.schedule")
+    nsrs, bases, _, _, d = msm_2p22
+    rng = np.random.default_rng(77)
+    logs = [14, 22] + [int(x) for x in rng.integers(14, 23, 22)]
+    mixes = ["uniform", "small", "sparse", "mixed"]
+    ns = [1 << lg for lg in logs]
+    cols = [S.scalars(n, mixes[i % 4], 600 + i) for i, n in enumerate(ns)]
+    exp = [O.msm_known_dlog(d[:n], H.to_host(c)) for n, c in zip(ns, cols)]
+    bases_dev = H.to_device(bases)
+
+    def check(out):
+        torch.cuda.synchronize()
+        got = H.to_host(out)
+        for i in range(len(ns)):
+            assert (O.g1_jac_to_aff(got[i].reshape(1, 12)) == exp[i]).all(), f"MSM {i} (2^{logs[i]})"
+
+    check(H.msm_batch(bases_dev, cols, ns))
+    model = S.Model.load()
+    learned = [model.pick(S.shape_features(n, len(ns), S.histogram(c))) for n, c in zip(ns, cols)]
+    check(H.msm_batch(bases_dev, cols, ns, learned))
+    n_arr = (ctypes.c_uint32 * len(ns))(*ns)
+    c = gpu.load_library().zkp_msm_batch_table_default_window(ctypes.addressof(n_arr), len(ns))
+    table, c = H.msm_table_build(bases_dev, nsrs, c)
+    check(H.msm_batch_table(table, nsrs, c, cols, ns))
