@@ -201,8 +201,8 @@ size_t batch_inv_scratch_elems(uint32_t n) {
 // inversion at the top), (3) every block unwound with its product's inverse.
 // Otherwise each block inverts its own product (binary extended Euclid, about
 // 30 us of one thread while the block waits): measured on B200 this is the
-// faster form up to 2^22 elements (0.078 against 0.136 ms at 2^16, 0.651
-// against 0.686 ms at 2^22), the extra pass of the three-phase form costing
+// faster form up to 2^22 elements (0.078 against 0.136 ms at 2^16, 0.57
+// against 0.64 ms at 2^22), the extra pass of the three-phase form costing
 // more than the inversion stalls that other resident blocks partly hide.
 static constexpr uint32_t BATCH_INV_THREE_PHASE_ABOVE = 1u << 22;
 
