@@ -376,7 +376,8 @@ cudaError_t zkp_shuffle_z(void *z, const void *inputs, const void *tables, const
  * that loads it, held until exit) shared by every call: calls that overlap on
  * the GPU race, so order them on one stream.  The first call on a device looks
  * up the array's address (cudaGetSymbolAddress) and should come before any
- * stream capture.  Calls cudaMalloc, cudaFree or no allocating routine. */
+ * stream capture.  It calls no allocating routine: no cudaMalloc, no
+ * cudaFree, no cudaMallocAsync. */
 cudaError_t zkp_msm_static(void *out, const void *bases, const void *scalars, uint32_t n, cudaStream_t stream);
 
 /* ----------------------------------------------------------------------
@@ -453,7 +454,8 @@ void zkp_host_pool_destroy(void *pool);
 
 /* Bounded asynchronous copy queue on `device` (src/async_copy_queue.rs): at
  * most max_in_flight copies in flight, each on its own stream.  NULL on
- * failure.  One owner thread. */
+ * failure.  The caller's current device is unchanged on return.  One owner
+ * thread. */
 void *zkp_copy_queue_create(int max_in_flight, int device);
 /* one cudaMemcpyAsync of `bytes` (kind: a cudaMemcpyKind value), ordered
  * after the work already queued on `after`; when max_in_flight copies are in

@@ -1,8 +1,12 @@
-"""Generates tests/golden/reference_kernels.npz from the reference's own CUDA
+"""Writes tests/golden/reference_kernels.json from the reference's own CUDA
 kernels (cuda/bn254.cu + cuda/msm.cu rebuilt for sm_100a by `make -C oracle
-ref` into oracle/_ref/).  Needs a GPU; run once on the B200 box:
+ref` into oracle/_ref/).  Needs a GPU:
 
-    python tests/golden/make_golden.py gpurun_out/reference_kernels.npz
+    python tests/golden/make_golden.py [OUT_DIR]
+
+writes OUT_DIR/reference_kernels.json (default: this directory, where the
+committed copy lives; on a machine whose results must be carried back, give a
+directory that is copied back and copy the file here).
 
 Inputs come from the oracle's seeded generators.  Each reference entry point
 is called the way the reference's Rust host calls it:
@@ -10,6 +14,9 @@ is called the way the reference's Rust host calls it:
   msm + batch_msm_collect     src/cuda/msm.rs:239-455 (batch of one)
   logup_sum_input_inv         src/lib.rs:643 (n >= 32768)
   eval_logup_z_compose        src/lib.rs:662
+and every case of tests/ref_cases.py (the quotient, multi-open, coset and
+lookup symbols) at n = 2^12 and 2^16, recorded as SHA-256 hashes of each
+output under "kernels" (key "<case>@<n>").
 """
 import ctypes
 import json
@@ -21,7 +28,10 @@ import torch
 
 ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+sys.path.insert(0, ROOT)
 import oracle as O  # noqa: E402
+import ref_cases as RC  # noqa: E402
 
 REF = os.path.join(ROOT, "oracle", "_ref", "libzkwasm_prover_kernel_ref.so")
 
@@ -93,6 +103,7 @@ def ref_msm(L, bases, scalars):
 
 
 def main(out):
+    os.makedirs(out, exist_ok=True)
     L = ctypes.CDLL(REF)
     g = {}
     for k in (10, 13):
@@ -124,9 +135,14 @@ def main(out):
     assert L.eval_logup_z_compose(p(z), p(s2), p(table_d), p(m_d), p(beta_d), p(last), n - 17, n, None) == 0
     torch.cuda.synchronize()
     g["logup_table"], g["logup_m"], g["logup_z"], g["logup_last_z"] = table, m, host(z), host(last)
-    np.savez_compressed(out, **g)
-    write_json(g, os.path.join(os.path.dirname(out), "reference_kernels.json"))
-    print("wrote", out, sorted(g))
+    kernels = {}
+    LR = RC.load_ref()
+    for n in (1 << 12, 1 << 16):
+        for case in RC.cases_for(n):
+            kernels[f"{case.name}@{n}"] = {k: sha(v) for k, v in case.run(LR, RC.Dev(), n).items()}
+    path = os.path.join(out, "reference_kernels.json")
+    write_json(g, kernels, path)
+    print("wrote", path, len(kernels), "kernel cases")
 
 
 def sha(a):
@@ -135,7 +151,7 @@ def sha(a):
     return hashlib.sha256(np.ascontiguousarray(a, np.uint64).tobytes()).hexdigest()
 
 
-def write_json(g, path):
+def write_json(g, kernels, path):
     """Compact fixture: seeds of the inputs, hashes of large outputs, small
     outputs in full."""
     out = {"generator": "tests/golden/make_golden.py on a B200 (reference cuda/bn254.cu + cuda/msm.cu rebuilt "
@@ -152,9 +168,10 @@ def write_json(g, path):
     out["logup"] = {"n": n, "input_seed": 10001, "beta_seed": 10002, "table_seed": 10003, "m": "i % 5",
                     "last_z_index": n - 17, "sum_sha256": sha(g["logup_sum"]), "z_sha256": sha(g["logup_z"]),
                     "last_z": [int(x) for x in g["logup_last_z"].reshape(-1)]}
+    out["kernels"] = kernels
     with open(path, "w") as f:
         json.dump(out, f, indent=1)
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else os.path.join(ROOT, "gpurun_out", "reference_kernels.npz"))
+    main(sys.argv[1] if len(sys.argv) > 1 else os.path.dirname(os.path.abspath(__file__)))

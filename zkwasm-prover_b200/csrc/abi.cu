@@ -7,7 +7,18 @@
 
 using namespace zk;
 
+#include <initializer_list>
+
 static inline Fr* F(void* p) { return reinterpret_cast<Fr*>(p); }
+
+// Argument checks of the reference-compatible symbols: every pointer a kernel
+// dereferences must be set once there is work (n > 0).  A failed check
+// returns cudaErrorInvalidValue before anything is enqueued.
+static inline bool all_set(std::initializer_list<const void*> ps) {
+    for (const void* q : ps)
+        if (!q) return false;
+    return true;
+}
 static inline const Fr* CF(const void* p) { return reinterpret_cast<const Fr*>(p); }
 
 // ------------------------------------------------------------------ kernels used only here
@@ -87,43 +98,50 @@ cudaError_t ntt(void* buf, void* tmp, void* pq, void* omega, void* n_inv, int ar
 
 cudaError_t field_op(void* res, void* l, int l_rot, void* l_c, void* r, int r_rot, void* r_c, int size, int op,
                      cudaStream_t stream) {
-    if (size < 0) return cudaErrorInvalidValue;
+    if (size < 0 || op < 0 || op > 3) return cudaErrorInvalidValue;
+    // L is l (times l_c) or l_c alone; R likewise, and unused by op 2
+    if (size > 0 && (!res || (!l && !l_c) || (op != 2 && !r && !r_c))) return cudaErrorInvalidValue;
     return zk::field_op(F(res), CF(l), l_rot, CF(l_c), CF(r), r_rot, CF(r_c), (uint32_t)size, op, stream);
 }
 
 cudaError_t extended_prepare(void* s, void* coset_powers, int coset_powers_n, int size, int extended_size,
                              int to_coset, cudaStream_t stream) {
     if (size < 0 || extended_size < 0 || coset_powers_n <= 0) return cudaErrorInvalidValue;
+    if (!to_coset && size > extended_size) return cudaErrorInvalidValue;
+    if ((to_coset ? extended_size : (extended_size > size ? extended_size : size)) > 0 &&
+        (!s || (coset_powers_n > 1 && !coset_powers)))
+        return cudaErrorInvalidValue;
     return zk::extended_prepare(F(s), CF(coset_powers), (uint32_t)coset_powers_n, (uint32_t)size,
                                 (uint32_t)extended_size, to_coset, stream);
 }
 
 cudaError_t permutation_eval_h_p1(void* res, void* first_set, void* last_set, void* l0, void* l_last, void* y,
                                   int n) {
-    if (n < 0) return cudaErrorInvalidValue;
+    if (n < 0 || (n > 0 && !all_set({res, first_set, last_set, l0, l_last, y}))) return cudaErrorInvalidValue;
     return zk::permutation_eval_h_p1(F(res), CF(first_set), CF(last_set), CF(l0), CF(l_last), CF(y), (uint32_t)n, 0);
 }
 
 cudaError_t permutation_eval_h_p2(void* res, void* set, void* l0, void* l_last, void* y, int n_set, int rot, int n) {
     (void)l_last;
-    if (n < 0) return cudaErrorInvalidValue;
+    if (n < 0 || n_set < 0 || (n > 0 && n_set > 1 && !all_set({res, set, l0, y}))) return cudaErrorInvalidValue;
     return zk::permutation_eval_h_p2(F(res), reinterpret_cast<const Fr* const*>(set), CF(l0), CF(y), n_set, rot,
                                      (uint32_t)n, 0);
 }
 
 cudaError_t permutation_eval_h_l(void* res, void* beta, void* gamma, void* p, int n, cudaStream_t stream) {
-    if (n < 0) return cudaErrorInvalidValue;
+    if (n < 0 || (n > 0 && !all_set({res, beta, gamma, p}))) return cudaErrorInvalidValue;
     return zk::permutation_eval_h_l(F(res), CF(beta), CF(gamma), CF(p), (uint32_t)n, stream);
 }
 
 cudaError_t field_sum(void* res, void* v, void* v_c, void* v_rot, void* omegas, int v_n, int n) {
-    if (n < 0) return cudaErrorInvalidValue;
+    if (n < 0 || v_n < 0 || (n > 0 && (!res || (v_n > 0 && !all_set({v, v_c, v_rot, omegas})))))
+        return cudaErrorInvalidValue;
     return zk::field_sum(F(res), reinterpret_cast<Fr* const*>(v), reinterpret_cast<Fr* const*>(v_c),
                          reinterpret_cast<const int*>(v_rot), CF(omegas), v_n, (uint32_t)n, 0);
 }
 
 cudaError_t field_op_batch_mul_sum(void* res, void* v, void* rot, int v_n, int n, cudaStream_t stream) {
-    if (n < 0) return cudaErrorInvalidValue;
+    if (n < 0 || v_n < 0 || (n > 0 && v_n > 0 && !all_set({res, v, rot}))) return cudaErrorInvalidValue;
     return zk::field_op_batch_mul_sum(F(res), reinterpret_cast<Fr* const*>(v), reinterpret_cast<const int*>(rot),
                                       v_n, (uint32_t)n, stream);
 }
@@ -131,7 +149,9 @@ cudaError_t field_op_batch_mul_sum(void* res, void* v, void* rot, int v_n, int n
 cudaError_t lookup_eval_h(void* res, void* input, void* table, void* permuted_input, void* permuted_table, void* z,
                           void* l0, void* l_last, void* l_active_row, void* y, void* beta, void* gamma, int rot,
                           int n, cudaStream_t stream) {
-    if (n < 0) return cudaErrorInvalidValue;
+    if (n < 0 || (n > 0 && !all_set({res, input, table, permuted_input, permuted_table, z, l0, l_last, l_active_row, y,
+                                      beta, gamma})))
+        return cudaErrorInvalidValue;
     return zk::lookup_eval_h(F(res), CF(input), CF(table), CF(permuted_input), CF(permuted_table), CF(z), CF(l0),
                              CF(l_last), CF(l_active_row), CF(y), CF(beta), CF(gamma), rot, (uint32_t)n, stream);
 }
@@ -139,7 +159,9 @@ cudaError_t lookup_eval_h(void* res, void* input, void* table, void* permuted_in
 cudaError_t logup_eval_h(void* res, void* input_product, void* input_product_sum, void* table, void* multiplicity,
                          void* z_first, void* z_last, void* l0, void* l_last, void* l_active_row, void* y, int rot,
                          int n, cudaStream_t stream) {
-    if (n < 0) return cudaErrorInvalidValue;
+    if (n < 0 || (n > 0 && !all_set({res, input_product, input_product_sum, table, multiplicity, z_first, z_last, l0,
+                                      l_last, l_active_row, y})))
+        return cudaErrorInvalidValue;
     return zk::logup_eval_h(F(res), CF(input_product), CF(input_product_sum), CF(table), CF(multiplicity),
                             CF(z_first), CF(z_last), CF(l0), CF(l_last), CF(l_active_row), CF(y), rot, (uint32_t)n,
                             stream);
@@ -147,7 +169,8 @@ cudaError_t logup_eval_h(void* res, void* input_product, void* input_product_sum
 
 cudaError_t logup_eval_h_extra_inputs(void* res, void* input_product, void* input_product_sum, void* z,
                                       void* l_active_row, void* y, int rot, int n, cudaStream_t stream) {
-    if (n < 0) return cudaErrorInvalidValue;
+    if (n < 0 || (n > 0 && !all_set({res, input_product, input_product_sum, z, l_active_row, y})))
+        return cudaErrorInvalidValue;
     return zk::logup_eval_h_extra_inputs(F(res), CF(input_product), CF(input_product_sum), CF(z), CF(l_active_row),
                                          CF(y), rot, (uint32_t)n, stream);
 }
@@ -155,14 +178,14 @@ cudaError_t logup_eval_h_extra_inputs(void* res, void* input_product, void* inpu
 cudaError_t logup_eval_h_z_set(void* res, void* set, void* l0, void* l_last, void* y, int n_set, int rot, int n,
                                cudaStream_t stream) {
     (void)l_last;
-    if (n < 0) return cudaErrorInvalidValue;
+    if (n < 0 || n_set < 0 || (n > 0 && n_set > 1 && !all_set({res, set, l0, y}))) return cudaErrorInvalidValue;
     return zk::permutation_eval_h_p2(F(res), reinterpret_cast<const Fr* const*>(set), CF(l0), CF(y), n_set, rot,
                                      (uint32_t)n, stream);
 }
 
 cudaError_t logup_sum_input_inv(void* sum, void* input, void* temp, void* beta, int init, int n,
                                 cudaStream_t stream) {
-    if (n < 0) return cudaErrorInvalidValue;
+    if (n < 0 || (n > 0 && !all_set({sum, input, beta}))) return cudaErrorInvalidValue;
     // temp: the host's n-element buffer (src/lib.rs:596), scratch of the
     // three-phase inversion
     return zk::batch_inverse(F(sum), CF(input), CF(beta), (uint32_t)n, init != 0, F(temp), temp ? (size_t)n : 0,
@@ -171,21 +194,23 @@ cudaError_t logup_sum_input_inv(void* sum, void* input, void* temp, void* beta, 
 
 cudaError_t logup_eval_h_inputs_product_sum(void* product, void* product_sum, void* sets, int n_set, int n,
                                             cudaStream_t stream) {
-    if (n < 0) return cudaErrorInvalidValue;
+    if (n < 0 || n_set < 1 || (n > 0 && !all_set({product, product_sum, sets}))) return cudaErrorInvalidValue;
     return zk::logup_eval_h_inputs_product_sum(F(product), F(product_sum), reinterpret_cast<const Fr* const*>(sets),
                                                n_set, (uint32_t)n, stream);
 }
 
 cudaError_t shuffle_eval_h(void* res, void* input, void* table, void* z, void* l0, void* l_last, void* l_active_row,
                            void* y, int rot, int n) {
-    if (n < 0) return cudaErrorInvalidValue;
+    if (n < 0 || (n > 0 && !all_set({res, input, table, z, l0, l_last, l_active_row, y}))) return cudaErrorInvalidValue;
     return zk::shuffle_eval_h(F(res), CF(input), CF(table), CF(z), CF(l0), CF(l_last), CF(l_active_row), CF(y), rot,
                               (uint32_t)n, 0);
 }
 
 cudaError_t shuffle_eval_h_v2(void* res, void* inputs, void* tables, void* betas, int group_len, void* z, void* l0,
                               void* l_last, void* l_active_row, void* y, int rot, int n) {
-    if (n < 0) return cudaErrorInvalidValue;
+    if (n < 0 || group_len < 1 ||
+        (n > 0 && !all_set({res, inputs, tables, betas, z, l0, l_last, l_active_row, y})))
+        return cudaErrorInvalidValue;
     return zk::shuffle_eval_h_v2(F(res), reinterpret_cast<const Fr* const*>(inputs),
                                  reinterpret_cast<const Fr* const*>(tables), CF(betas), group_len, CF(z), CF(l0),
                                  CF(l_last), CF(l_active_row), CF(y), rot, (uint32_t)n, 0);
@@ -193,35 +218,39 @@ cudaError_t shuffle_eval_h_v2(void* res, void* inputs, void* tables, void* betas
 
 cudaError_t expand_omega_buffer(void* buf, int n, int may_bit_reversed) {
     (void)may_bit_reversed;
-    if (n < 0 || n > 30) return cudaErrorInvalidValue;
+    if (n < 0 || n > 30 || !buf) return cudaErrorInvalidValue;
     return zk::expand_powers(F(buf), 1u << n, 0);
 }
 
 cudaError_t field_mul_zip(void* buf, void* coeff, int coeff_n, int n) {
-    if (n < 0 || coeff_n <= 0) return cudaErrorInvalidValue;
+    if (n < 0 || coeff_n <= 0 || (n > 0 && !all_set({buf, coeff}))) return cudaErrorInvalidValue;
     return zk::field_mul_zip(F(buf), CF(coeff), (uint32_t)coeff_n, (uint32_t)n, 0);
 }
 
 cudaError_t poly_eval(void* p, void* res, void* x, int n, cudaStream_t stream) {
-    if (n <= 0) return cudaErrorInvalidValue;
+    if (n <= 0 || (n & (n - 1)) != 0 || !all_set({p, res, x})) return cudaErrorInvalidValue;
     return zk::poly_eval(CF(p), F(res), CF(x), (uint32_t)n, stream);
 }
 
 cudaError_t shplonk_h_x_merge(void* res, void* v, void* values, void* omegas, void* diff_points, int diff_points_n,
                               int n) {
-    if (n < 0) return cudaErrorInvalidValue;
+    if (n < 0 || diff_points_n < 0 ||
+        (n > 0 && (!all_set({res, v, values, omegas}) || (diff_points_n > 0 && !diff_points))))
+        return cudaErrorInvalidValue;
     return zk::shplonk_h_x_merge(F(res), CF(v), CF(values), CF(omegas), CF(diff_points), diff_points_n, (uint32_t)n,
                                  0);
 }
 
 cudaError_t shplonk_h_x_div_points(void* values, void* omegas, void* points, int points_n, int n) {
-    if (n < 0) return cudaErrorInvalidValue;
+    if (n < 0 || points_n < 0 || (n > 0 && (!all_set({values, omegas}) || (points_n > 0 && !points))))
+        return cudaErrorInvalidValue;
     return zk::div_by_point_diffs(F(values), CF(omegas), CF(points), points_n, (uint32_t)n, nullptr, 0, 0);
 }
 
 cudaError_t eval_logup_z_compose(void* z, void* input, void* table, void* multiplicity, void* beta, void* last_z,
                                  int last_z_index, int n, cudaStream_t stream) {
-    if (n <= 0) return cudaErrorInvalidValue;
+    if (n <= 0 || last_z_index < 0 || last_z_index >= n || !all_set({z, input, table, multiplicity, beta, last_z}))
+        return cudaErrorInvalidValue;
     return zk::logup_z_compose(F(z), CF(input), CF(table), CF(multiplicity), CF(beta), F(last_z), last_z_index,
                                (uint32_t)n, F(table), stream);
 }
@@ -229,7 +258,7 @@ cudaError_t eval_logup_z_compose(void* z, void* input, void* table, void* multip
 cudaError_t eval_logup_z_pure(void* z, void* input, void* table, void* last_z, int last_z_index, int n,
                               cudaStream_t stream) {
     (void)input;
-    if (n <= 0) return cudaErrorInvalidValue;
+    if (n <= 0 || last_z_index < 0 || last_z_index >= n || !all_set({z, table, last_z})) return cudaErrorInvalidValue;
     return zk::logup_z_scan(F(z), F(last_z), last_z_index, (uint32_t)n, F(table), stream);
 }
 
@@ -247,9 +276,9 @@ cudaError_t batch_msm_collect(void* remain_indices, void* remain_acc, void* next
     (void)workers;
     (void)windows;
     (void)window_bits;
+    if (batch_size > 0 && !buckets) return cudaErrorInvalidValue;
     ZK_CHECK(cudaGetLastError());  // errors of earlier msm() launches surface here, as in the reference
     if (batch_size == 0) return cudaSuccess;
-    if (!buckets) return cudaErrorInvalidValue;
     // buckets: device array of the per-MSM regions msm() parked its window sums in
     return msm_collect(reinterpret_cast<char* const*>(buckets), batch_size, MSM_NOTE_OFF, stream);
 }
@@ -268,6 +297,7 @@ cudaError_t msm(void* res, void* p, void* s, void* indices_buf0, void* indices_b
     (void)skip_zero;
     if (array_len < 0 || windows <= 0 || window_bits <= 0 || window_bits > 24 || workers < 0 || !res || !sort_buf)
         return cudaErrorInvalidValue;
+    if (array_len > 0 && (!p || !s)) return cudaErrorInvalidValue;
     const uint32_t n = (uint32_t)array_len;
     // scratch the reference host allocates for this call (src/cuda/msm.rs:297-317)
     const size_t words_avail = (size_t)3 * n * (size_t)windows;
@@ -312,7 +342,7 @@ cudaError_t prepare_table_lookup(void* table, void* table_lowest_u32, void* sort
     (void)sorted_index;
     (void)candidate_sort_temp_storage;
     (void)candidate_sort_temp_storage_bytes;
-    if (k > 27 || unusable_rows_start > (1u << k)) return cudaErrorInvalidValue;
+    if (k > 27 || unusable_rows_start > (1u << k) || !all_set({table, start_offset})) return cudaErrorInvalidValue;
     // start_offset spans n Fr = 2^(k+3) u32: 2^(k+2) slots keep the load <= 1/4
     return zk::lookup_table_build(CF(table), unusable_rows_start, reinterpret_cast<uint32_t*>(start_offset), k + 2,
                                   stream);
@@ -326,7 +356,8 @@ cudaError_t calc_m(void* m, void* table, void* input, void* sorted_index, void* 
     (void)sorted_matched_index;
     (void)candidate_sort_temp_storage;
     (void)candidate_sort_temp_storage_bytes;
-    if (k > 27 || unusable_rows_start > (1u << k)) return cudaErrorInvalidValue;
+    if (k > 27 || unusable_rows_start > (1u << k) || !all_set({m, table, input, start_offset, matched_index}))
+        return cudaErrorInvalidValue;
     return zk::lookup_count(F(m), CF(table), CF(input), 1u << k, unusable_rows_start,
                             reinterpret_cast<const uint32_t*>(start_offset), k + 2,
                             reinterpret_cast<uint32_t*>(matched_index), stream);

@@ -2,6 +2,10 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <stddef.h>
+#include <stdint.h>
+
+#include <mutex>
+
 #include "field.cuh"
 
 namespace zk {
@@ -81,3 +85,28 @@ __device__ __forceinline__ KnownFr block_known(const Fr* p) {
         cudaError_t err__ = (x);              \
         if (err__ != cudaSuccess) return err__; \
     } while (0)
+
+namespace zk {
+
+// Raises a kernel's dynamic shared-memory limit once per device: the
+// attribute belongs to the device that is current when it is set, so a flag
+// shared by all devices would leave a second GPU without it.  One instance per
+// launch site (a function-local static), safe to call from several threads.
+struct SmemOptIn {
+    std::mutex mu;
+    uint64_t done = 0;  // bit d: set on device d
+
+    template <class K>
+    cudaError_t ensure(K kernel, int bytes) {
+        int dev = 0;
+        ZK_CHECK(cudaGetDevice(&dev));
+        if (dev < 0 || dev >= 64) return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        std::lock_guard<std::mutex> lock(mu);
+        if ((done >> dev) & 1u) return cudaSuccess;
+        ZK_CHECK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+        done |= uint64_t(1) << dev;
+        return cudaSuccess;
+    }
+};
+
+}  // namespace zk

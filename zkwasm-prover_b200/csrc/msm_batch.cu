@@ -370,12 +370,8 @@ cudaError_t msm_batch_run(Jac* out, const Aff* bases, const Fr* const* scalars, 
     const uint32_t max_parts = L.maxG < 128 ? 1u : L.maxG / 128u;
     uint32_t bd = 1;
     while (bd < max_parts && bd < 256) bd <<= 1;
-    static bool attr = false;
-    if (!attr) {
-        ZK_CHECK(cudaFuncSetAttribute(batch_window_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      512 * (int)sizeof(Xyzz)));
-        attr = true;
-    }
+    static SmemOptIn opt;
+    ZK_CHECK(opt.ensure(batch_window_kernel, 512 * (int)sizeof(Xyzz)));
     batch_window_kernel<<<L.win_total, bd, (size_t)bd * sizeof(Xyzz), st>>>(d, count, segsum, winsum);
     ZK_CHECK(cudaGetLastError());
     batch_final_kernel<<<count, COOP_THREADS, 0, st>>>(d, winsum, out);

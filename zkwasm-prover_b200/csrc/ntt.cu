@@ -493,12 +493,8 @@ template <int LOGR, class TW>
 static cudaError_t launch_fused(const FusedExtendArgs& a, unsigned ncols, cudaStream_t s) {
     constexpr int R = 1 << LOGR;
     const size_t smem = (size_t)(ZK_FUSED_ONE_TILE ? 1 : 2) * R * sizeof(Fr);
-    static bool attr_set = false;
-    if (!attr_set) {
-        ZK_CHECK(cudaFuncSetAttribute(ntt_fused_extend_kernel<LOGR, TW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)smem));
-        attr_set = true;
-    }
+    static SmemOptIn opt;
+    ZK_CHECK(opt.ensure(ntt_fused_extend_kernel<LOGR, TW>, (int)smem));
     dim3 grid(1u << (a.log_n - LOGR), ncols, 1);
     ntt_fused_extend_kernel<LOGR, TW><<<grid, R / 8, smem, s>>>(a);
     return cudaGetLastError();
@@ -599,12 +595,8 @@ static cudaError_t launch_pass(const NttPassArgs& a, unsigned ny, unsigned nz, c
     constexpr int R = 1 << LOGR;
     constexpr int T = (G * R) / 8;
     const size_t smem = (size_t)G * R * sizeof(Fr);
-    static bool attr_set = false;
-    if (!attr_set) {
-        ZK_CHECK(cudaFuncSetAttribute(ntt_pass_kernel<LOGR, G, TW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)smem));
-        attr_set = true;
-    }
+    static SmemOptIn opt;
+    ZK_CHECK(opt.ensure(ntt_pass_kernel<LOGR, G, TW>, (int)smem));
     const unsigned items = 1u << (a.log_n - LOGR);
     dim3 grid(items / G, ny, nz);
     ntt_pass_kernel<LOGR, G, TW><<<grid, T, smem, s>>>(a);

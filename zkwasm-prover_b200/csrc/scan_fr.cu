@@ -209,12 +209,8 @@ static constexpr uint32_t BATCH_INV_THREE_PHASE_ABOVE = 1u << 22;
 template <class Src, class Dst>
 static cudaError_t launch_batch_inv(Src src, Dst dst, uint32_t n, Fr* scratch, size_t scratch_elems, cudaStream_t s) {
     if (n == 0) return cudaSuccess;
-    static bool attr = false;
-    if (!attr) {
-        ZK_CHECK(cudaFuncSetAttribute(batch_inv_kernel<Src, Dst>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)BATCH_INV_SMEM));
-        attr = true;
-    }
+    static SmemOptIn opt;
+    ZK_CHECK(opt.ensure(batch_inv_kernel<Src, Dst>, (int)BATCH_INV_SMEM));
     const uint32_t nb = (n + SBLK - 1) / SBLK;
     if (n > BATCH_INV_THREE_PHASE_ABOVE && scratch && scratch_elems >= batch_inv_scratch_elems(n)) {
         Fr* tot = scratch;

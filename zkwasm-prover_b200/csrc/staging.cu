@@ -29,10 +29,25 @@ namespace {
 
 struct HostBlock {
     char* base;
-    size_t bytes;
+    size_t bytes;   // length of the mapping (a whole number of huge pages for MAP_HUGETLB)
     bool mapped;    // mmap'ed (else operator new)
     bool pinned;    // cudaHostRegister'ed
 };
+
+// MAP_HUGETLB mappings are made in whole huge pages; munmap must be given the
+// rounded length or it fails with EINVAL and the block leaks.  2 MiB is the
+// default huge-page size on x86-64 and aarch64 hosts.
+constexpr size_t HUGE_PAGE_BYTES = size_t(2) << 20;
+
+void release_block(const HostBlock& b) {
+    if (b.pinned) cudaHostUnregister(b.base);
+    if (b.mapped) {
+        // a failed munmap leaves the mapping in place; there is nothing more to do here than not crash
+        (void)munmap(b.base, b.bytes);
+    } else {
+        ::operator delete(b.base, std::align_val_t(4096));
+    }
+}
 
 struct HostPool {
     size_t chunk = 0;
@@ -52,9 +67,11 @@ bool pool_grow(HostPool* p) {
     HostBlock b{nullptr, bytes, false, false};
     if (p->flags & POOL_HUGE) {
 #ifdef MAP_HUGETLB
-        void* m = mmap(nullptr, bytes, PROT_READ | PROT_WRITE, MAP_PRIVATE | MAP_ANONYMOUS | MAP_HUGETLB, -1, 0);
+        const size_t huge_bytes = (bytes + HUGE_PAGE_BYTES - 1) / HUGE_PAGE_BYTES * HUGE_PAGE_BYTES;
+        void* m = mmap(nullptr, huge_bytes, PROT_READ | PROT_WRITE, MAP_PRIVATE | MAP_ANONYMOUS | MAP_HUGETLB, -1, 0);
         if (m != MAP_FAILED) {
             b.base = static_cast<char*>(m);
+            b.bytes = huge_bytes;
             b.mapped = true;
         }
 #endif
@@ -72,12 +89,9 @@ bool pool_grow(HostPool* p) {
         if (!b.base) return false;
     }
     if (p->flags & POOL_PIN) {
-        if (cudaHostRegister(b.base, bytes, cudaHostRegisterDefault) != cudaSuccess) {
+        if (cudaHostRegister(b.base, b.bytes, cudaHostRegisterDefault) != cudaSuccess) {
             cudaGetLastError();
-            if (b.mapped)
-                munmap(b.base, bytes);
-            else
-                ::operator delete(b.base, std::align_val_t(4096));
+            release_block(b);
             return false;
         }
         b.pinned = true;
@@ -128,7 +142,7 @@ int zkp_host_pool_free(void* pool, void* ptr) {
     char* c = static_cast<char*>(ptr);
     std::lock_guard<std::mutex> lock(p->mu);
     for (const HostBlock& b : p->blocks) {
-        if (c >= b.base && c < b.base + b.bytes) {
+        if (c >= b.base && c < b.base + p->chunk * (size_t)p->per_block) {
             if ((size_t)(c - b.base) % p->chunk != 0) return -1;
             for (char* f : p->free_chunks)
                 if (f == c) return -1;  // double free
@@ -152,13 +166,7 @@ void zkp_host_pool_stats(void* pool, size_t* blocks, size_t* used_chunks) {
 void zkp_host_pool_destroy(void* pool) {
     HostPool* p = static_cast<HostPool*>(pool);
     if (!p) return;
-    for (const HostBlock& b : p->blocks) {
-        if (b.pinned) cudaHostUnregister(b.base);
-        if (b.mapped)
-            munmap(b.base, b.bytes);
-        else
-            ::operator delete(b.base, std::align_val_t(4096));
-    }
+    for (const HostBlock& b : p->blocks) release_block(b);
     delete p;
 }
 
@@ -168,7 +176,11 @@ void* zkp_copy_queue_create(int max_in_flight, int device) {
     if (!q) return nullptr;
     q->max = max_in_flight;
     q->device = device;
-    if (cudaSetDevice(device) != cudaSuccess) {
+    // the streams and events belong to `device`; the caller's current device
+    // is put back before returning, on success and on failure
+    int prev_device = 0;
+    if (cudaGetDevice(&prev_device) != cudaSuccess || cudaSetDevice(device) != cudaSuccess) {
+        cudaGetLastError();
         delete q;
         return nullptr;
     }
@@ -187,8 +199,10 @@ void* zkp_copy_queue_create(int max_in_flight, int device) {
         for (cudaEvent_t e : q->done) cudaEventDestroy(e);
         if (q->order) cudaEventDestroy(q->order);
         delete q;
+        cudaSetDevice(prev_device);
         return nullptr;
     }
+    cudaSetDevice(prev_device);
     return q;
 }
 
