@@ -367,6 +367,91 @@ cudaError_t zkp_permutation_z(void *z, const void *cols, const void *sigmas, int
 cudaError_t zkp_shuffle_z(void *z, const void *inputs, const void *tables, const void *betas, int groups, uint32_t n,
                           void *scratch, cudaStream_t stream);
 
+/* ----------------------------------------------------------------------
+ * Quotient over cosets of the extended domain, and multi-open helpers
+ * (csrc/quotient.cu).  They replace the per-column 2^(k+e) extension and the
+ * per-family kernels of src/eval_h.rs:410-1199 with per-coset work, and the
+ * host-side divisions of src/multiopen.rs:145-159, 543-553.
+ * ------------------------------------------------------------------ */
+
+/* NTT of ncols columns from `in` (stride in_stride) into `out` (stride
+ * out_stride, out != in): out_c = NTT(in_c[k] * in_mul[k]) (in_mul may be
+ * NULL), every output times *scale when scale is non-NULL.  With in_mul[k] =
+ * (zeta w_N^j)^k it gives coset j of the extended domain zeta <w_N>
+ * (N = E n) from coefficients.  tmp: n * ncols elements (unused for one-pass
+ * sizes). */
+cudaError_t zkp_ntt_batch_twisted(void *out, const void *in, void *tmp, const void *omegas, const void *in_mul,
+                                  const void *scale, int log_n, uint32_t ncols, size_t in_stride, size_t out_stride,
+                                  cudaStream_t stream);
+
+/* Arguments of zkp_eval_h_fused.  Every pointer is a device pointer; `T**`
+ * fields are device arrays of device pointers.  Row i of every column is row
+ * i of one coset (rot_scale 1) or of the whole extended domain (rot_scale E);
+ * a rotation r reads row (i + r * rot_scale) mod n. */
+typedef struct zkp_eval_h_args {
+    uint32_t n;
+    int rot_scale;
+    const void *y;             /* the challenge y */
+    /* gates: [coeff, col, col, ..., NULL, coeff, ...] as field_op_batch_mul_sum
+     * takes them, coefficients carrying their powers of y; one rotation per
+     * column entry */
+    const void *gate_terms;
+    const void *gate_rots;
+    int gate_terms_n;
+    const void *l0, *l_last, *l_active;
+    const void *x;             /* the point X of each row (permutation only) */
+    const void *beta, *gamma;
+    /* permutation: perm_chunks products z_j over chunks of perm_chunk_len of
+     * the perm_cols_n columns; perm_dbeta[c] = beta * delta^c (Fr array);
+     * perm_last_rot = -(blinding factors + 1) links the chunks */
+    int perm_chunks, perm_chunk_len, perm_cols_n, perm_last_rot;
+    const void *perm_z, *perm_cols, *perm_sigmas, *perm_dbeta;
+    /* logup lookups with one input per set: 4 pointers each, input, table,
+     * multiplicity, z */
+    int lookups;
+    const void *lookup_cols;
+    /* shuffles: per shuffle z, then shuffle_group_len[s] (input, table)
+     * pairs; shuffle_betas[g] = beta^(g + 1) */
+    int shuffles;
+    const void *shuffle_cols, *shuffle_group_len, *shuffle_betas;
+    const void *scale;         /* optional factor of every output (1 / Z_H on a coset) */
+} zkp_eval_h_args;
+
+/* The constraint expression of the prover's quotient over n rows, in one pass
+ * that reads each column once and writes h once: the gate terms, then with
+ * Horner steps in y the permutation (l_0 (1 - z_0), l_last (z_last^2 -
+ * z_last), the chunk links, the chunk products), every logup lookup and every
+ * shuffle, exactly the chain that src/eval_h.rs:588-1199 builds with
+ * field_op_batch_mul_sum, permutation_eval_h_p1 / p2, field_op, logup_eval_h
+ * and shuffle_eval_h_v2 (cuda/bn254.cu:664-1071). */
+cudaError_t zkp_eval_h_fused(void *h, const zkp_eval_h_args *args, cudaStream_t stream);
+
+/* From the E = 2^ext_bits coset iNTTs g_j (g_j = iNTT_n of h on coset
+ * zeta w_N^j <w_n>, scaled by 1/n; stride g_stride) to the N = E n
+ * coefficients of h, with h's values first multiplied by t_j on coset j:
+ * out[r + n s] = zeta^-(r+ns) / E * sum_j w_E^-(j s) t_j w_N^-(j r) g_j[r].
+ * winv[r] = w_N^-r (n entries); consts = t_0..t_{E-1}, w_E^-k (k < E),
+ * zeta^-k / E (k < 3).  ext_bits 1..3.  Equals src/eval_h.rs:463-510
+ * (field_mul_zip by t_evaluations, iNTT of 2^(k+e), extended_prepare with
+ * to_coset). */
+cudaError_t zkp_coset_combine(void *out, const void *g, size_t g_stride, const void *winv, const void *consts,
+                              int log_n, int ext_bits, cudaStream_t stream);
+
+/* q = (a(X) - a(z)) / (X - z) for n coefficients: q_i = sum_{j>i} a_j z^(j-i-1),
+ * q_{n-1} = 0, the layout src/multiopen.rs:145-159 leaves.  z is a HOST
+ * pointer to one Fr (Montgomery form); scratch:
+ * zkp_poly_divide_scratch_elems(n) elements; q must not alias a. */
+size_t zkp_poly_divide_scratch_elems(uint32_t n);
+cudaError_t zkp_poly_divide_linear(void *q, const void *a, const void *z, uint32_t n, void *scratch,
+                                   cudaStream_t stream);
+
+/* out[p] = sum_i polys[p][i] * powers[i] for count polynomials of n
+ * coefficients (powers: x^i, i < n, from zkp_powers); scratch:
+ * zkp_poly_eval_batch_scratch_elems(count) elements. */
+size_t zkp_poly_eval_batch_scratch_elems(uint32_t count);
+cudaError_t zkp_poly_eval_batch(void *out, const void *polys, uint32_t count, const void *powers, uint32_t n,
+                                void *scratch, cudaStream_t stream);
+
 /* No counterpart in the reference.  zkp_msm without caller-supplied scratch,
  * for callers that cannot allocate device memory: a host whose device memory
  * is all owned by its own pool, or a latency-critical path that cannot afford
