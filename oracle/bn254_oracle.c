@@ -351,6 +351,23 @@ void or_intt(u64 *a, int log_n, const u64 *omega) {
 }
 
 /* out[i] = base^i for i < n (Montgomery in and out) */
+/* The division the reference runs on the host after the multi-open batching
+ * (src/multiopen.rs:145-159 GWC, 543-553 SHPLONK), step by step: tmp = a[n-1],
+ * a[n-1] = 0, then for i = n-2 .. 1: p = a[i] + tmp z, a[i] = tmp, tmp = p;
+ * a[0] = tmp.  In place on n Montgomery-form coefficients (n >= 2). */
+void or_poly_divide_linear(u64 *a, const u64 *z, long n) {
+    u64 tmp[4], p[4], t[4];
+    memcpy(tmp, a + 4 * (n - 1), 32);
+    memset(a + 4 * (n - 1), 0, 32);
+    for (long i = n - 2; i >= 1; i--) {
+        f_mul(&FR, t, tmp, z);
+        f_add(&FR, p, a + 4 * i, t);
+        memcpy(a + 4 * i, tmp, 32);
+        memcpy(tmp, p, 32);
+    }
+    memcpy(a, tmp, 32);
+}
+
 void or_powers(u64 *out, const u64 *base, long n) {
     or_init();
     const fdesc *f = &FR;

@@ -68,6 +68,7 @@ def lib():
         "or_intt": [P, ci, P],
         "or_dft_naive": [P, P, ci, P],
         "or_powers": [P, P, i64],
+        "or_poly_divide_linear": [P, P, i64],
         "or_coset_extend": [P, P, ci, ci, P, P],
         "or_g1_generator": [P],
         "or_g1_is_on_curve": [P],
@@ -734,6 +735,14 @@ def field_sum(vs, v_cs, v_rots, omegas, n):
             t = mul(t, c)
         acc = t if acc is None else add(acc, t)
     return acc
+
+
+def poly_divide_linear(a, z: int):
+    """src/multiopen.rs:145-159: the quotient of a(X) - a(z) by X - z with the
+    reference's layout (last coefficient 0), by its own recurrence."""
+    out = np.array(_arr(a), copy=True)
+    lib().or_poly_divide_linear(_p(out), _p(fr(z)), out.shape[0])
+    return out
 
 
 def poly_eval(p, x: int):

@@ -1,0 +1,102 @@
+"""The proof hot path (zkwasm-prover_b200/prover.py) on small circuits of the
+benchmark's two shapes: the plain schedule (reference-compatible symbols, one
+kernel per column), the batched schedule (phase pipelines, per-coset fused
+quotient) and the plain schedule through the reference's own kernels (with the
+CPU steps through the oracle, as the reference's host runs them) give the same
+commitments and evaluations, bit for bit; the witness satisfies the circuit,
+so the quotient's coefficients past its degree bound are zero; commitments
+match the known-discrete-log identity of the SRS."""
+import importlib
+import os
+
+import numpy as np
+import pytest
+import torch
+
+import ref_cases as RC
+
+pytestmark = pytest.mark.gpu
+
+
+def _shapes(P, k=10):
+    return {
+        "gwc_deg4": P.Shape(k=k, advice=16, fixed=6, lookups=3, shuffles=1, perm=10, degree=4, multiopen="gwc"),
+        "shplonk_deg9": P.Shape(k=k, advice=16, fixed=6, lookups=3, shuffles=1, perm=10, degree=9,
+                                multiopen="shplonk"),
+    }
+
+
+@pytest.fixture(scope="module")
+def P(gpu):
+    return importlib.import_module("zkwasm-prover_b200.prover")
+
+
+def _run(P, shape, schedule, symbols=None, host_work=None, seed=3):
+    c = P.Circuit(shape, seed=seed)
+    hp = P.HotPath(c, schedule, symbols=symbols, host_work=host_work)
+    return hp, hp.prove()
+
+
+@pytest.mark.parametrize("name", ["gwc_deg4", "shplonk_deg9"])
+def test_plain_and_batched_agree(P, name):
+    shape = _shapes(P)[name]
+    hp_p, proof_p = _run(P, shape, "plain")
+    hp_b, proof_b = _run(P, shape, "batched")
+    assert proof_p["challenges"] == proof_b["challenges"]
+    for (na, a), (nb, b) in zip(proof_p["commitments"], proof_b["commitments"]):
+        assert na == nb and a == b, na
+    assert proof_p["evals"] == proof_b["evals"]
+    assert torch.equal(hp_p.h_coeff, hp_b.h_coeff)
+
+
+@pytest.mark.parametrize("name", ["gwc_deg4", "shplonk_deg9"])
+def test_quotient_vanishes_past_degree_bound(P, name):
+    """With a witness that satisfies every constraint, h = C / Z_H has degree
+    at most degree (n - 1) - n; any wrong value anywhere makes the top
+    coefficients nonzero."""
+    shape = _shapes(P)[name]
+    hp, _ = _run(P, shape, "batched")
+    n = shape.n
+    bound = shape.degree * (n - 1) - n
+    top = hp.h_coeff[bound + 1:]
+    assert top.shape[0] > 0
+    assert not top.any(), f"{int((top != 0).any(dim=1).sum())} coefficients past {bound} are nonzero"
+    # and a deliberately broken witness (one gate output changed) does not vanish
+    c = P.Circuit(shape, seed=3)
+    g = c.gate_cols[0]
+    row = int(torch.nonzero(c.fixed[c.selector_cols[0], :c.u, 0]).flatten()[0])
+    c.advice[g[4], row] = P.fr_tensor([12345])[0]
+    hp2 = P.HotPath(c, "batched")
+    hp2.prove()
+    assert hp2.h_coeff[bound + 1:].any()
+
+
+@pytest.mark.parametrize("name", ["gwc_deg4", "shplonk_deg9"])
+def test_plain_through_reference_kernels(P, name):
+    if not os.path.exists(RC.REF_LIB):
+        pytest.skip("reference kernels not built (make -C oracle ref)")
+    from host_work import OracleHostWork
+
+    # k = 15: the reference's logup kernels need n >= 32768 (cuda/bn254.cu:1914-1934)
+    shape = _shapes(P, k=15)[name]
+    _, proof_b = _run(P, shape, "batched")
+    _, proof_r = _run(P, shape, "plain", symbols=RC.load_ref(), host_work=OracleHostWork())
+    for (na, a), (nb, b) in zip(proof_b["commitments"], proof_r["commitments"]):
+        assert na == nb and a == b, na
+    assert proof_b["evals"] == proof_r["evals"]
+
+
+def test_commitments_match_known_dlogs(O, P):
+    """An advice commitment over the Lagrange SRS equals [sum_i a_i k_i] G."""
+    shape = _shapes(P)["gwc_deg4"]
+    c = P.Circuit(shape, seed=5)
+    hp = P.HotPath(c, "batched")
+    proof = hp.prove()
+    adv = dict(proof["commitments"])["advice"]
+    kl = hp.srs_k[1].cpu().numpy().view(np.uint64)
+    dl = O.fr_vec([int(x) for x in kl])
+    for i in (0, shape.advice - 1):
+        a = c.advice[i].cpu().numpy().view(np.uint64)
+        exp = O.msm_known_dlog(dl, a)
+        ex = [O.fq_ints(exp[:, :4])[0], O.fq_ints(exp[:, 4:])[0]]
+        assert tuple(ex) == adv[i]
