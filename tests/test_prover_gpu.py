@@ -49,13 +49,14 @@ def test_plain_and_batched_agree(P, name):
     assert torch.equal(hp_p.h_coeff, hp_b.h_coeff)
 
 
+@pytest.mark.parametrize("schedule", ["plain", "batched"])
 @pytest.mark.parametrize("name", ["gwc_deg4", "shplonk_deg9"])
-def test_quotient_vanishes_past_degree_bound(P, name):
+def test_quotient_vanishes_past_degree_bound(P, name, schedule):
     """With a witness that satisfies every constraint, h = C / Z_H has degree
     at most degree (n - 1) - n; any wrong value anywhere makes the top
     coefficients nonzero."""
     shape = _shapes(P)[name]
-    hp, _ = _run(P, shape, "batched")
+    hp, _ = _run(P, shape, schedule)
     n = shape.n
     bound = shape.degree * (n - 1) - n
     top = hp.h_coeff[bound + 1:]
@@ -66,7 +67,7 @@ def test_quotient_vanishes_past_degree_bound(P, name):
     g = c.gate_cols[0]
     row = int(torch.nonzero(c.fixed[c.selector_cols[0], :c.u, 0]).flatten()[0])
     c.advice[g[4], row] = P.fr_tensor([12345])[0]
-    hp2 = P.HotPath(c, "batched")
+    hp2 = P.HotPath(c, schedule)
     hp2.prove()
     assert hp2.h_coeff[bound + 1:].any()
 

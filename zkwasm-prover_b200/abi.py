@@ -91,6 +91,13 @@ SIGNATURES = {
     "zkp_mlp_grad": [P, P, P, P, U, P, P, P, S],
     "zkp_mlp_train_step": [P, P, P, P, P, P, P, U, ctypes.c_float, I, P, P, S],
     "zkp_msm_schedule_predict": ([P, P, I, I, P, S], I),
+    "zkp_ntt_batch_twisted": [P, P, P, P, P, P, I, U, SZ, SZ, S],
+    "zkp_eval_h_fused": [P, P, S],
+    "zkp_coset_combine": [P, P, SZ, P, P, I, I, S],
+    "zkp_poly_divide_scratch_elems": ([U], SZ),
+    "zkp_poly_divide_linear": [P, P, P, U, P, S],
+    "zkp_poly_eval_batch_scratch_elems": ([U], SZ),
+    "zkp_poly_eval_batch": [P, P, U, P, U, P, S],
     "zkp_calib_mont_rate": [P, U, U, S],
     "zkp_calib_shoup_rate": [P, P, U, U, S],
     # Part 4: host staging (csrc/staging.cu)

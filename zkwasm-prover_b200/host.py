@@ -147,9 +147,21 @@ class ReferenceMsmBatch:
         self.sort_buf = torch.empty(max(1, single * 3), dtype=torch.int32, device="cuda")
         self.idx = [torch.empty(max(1, single), dtype=torch.int32, device="cuda") for _ in range(4)]
         self.acc_idx = [torch.empty(max(1, self.worker * 2), dtype=torch.int32, device="cuda") for _ in range(count)]
-        # device array of the per-MSM region pointers (src/cuda/msm.rs:387-420)
-        self.regions = torch.tensor([self.curve_buf.data_ptr() + i * self.region * 96 for i in range(count)],
-                                    dtype=torch.int64, device="cuda")
+        # device arrays of the per-MSM region pointers and of the worker
+        # remainders inside each region (src/cuda/msm.rs:387-420): this
+        # library's batch_msm_collect reads the regions only, the reference's
+        # kernels all five
+        base = self.curve_buf.data_ptr()
+        bucket = windows << c
+
+        def ptrs(xs):
+            return torch.tensor(xs, dtype=torch.int64, device="cuda")
+
+        self.regions = ptrs([base + i * self.region * 96 for i in range(count)])
+        self.remain = (ptrs([a.data_ptr() for a in self.acc_idx]),
+                       ptrs([base + (i * self.region + bucket) * 96 for i in range(count)]),
+                       ptrs([a.data_ptr() + self.worker * 4 for a in self.acc_idx]),
+                       ptrs([base + (i * self.region + bucket + self.worker) * 96 for i in range(count)]))
         self.stream = stream
 
     def enqueue(self):
@@ -161,8 +173,9 @@ class ReferenceMsmBatch:
                             ptr(self.sort_buf), ptr(self.acc_idx[i]), self.length, self.windows, self.c,
                             self.threads, self.worker, self.sort_buf.numel() * 4, 1, st)
             abi.check(err, "msm")
-        abi.check(lib().batch_msm_collect(None, None, None, None, ptr(self.regions), self.worker, self.windows,
-                                          self.c, self.count, st), "batch_msm_collect")
+        r = self.remain
+        abi.check(lib().batch_msm_collect(ptr(r[0]), ptr(r[1]), ptr(r[2]), ptr(r[3]), ptr(self.regions), self.worker,
+                                          self.windows, self.c, self.count, st), "batch_msm_collect")
 
     def results(self):
         """Jacobian results as a numpy (count, 12) uint64 array (synchronises)."""

@@ -45,6 +45,7 @@ from __future__ import annotations
 import ctypes
 import hashlib
 import math
+import time
 from dataclasses import dataclass
 
 import numpy as np
@@ -464,11 +465,14 @@ class DeviceHostWork:
         L = lib()
         scratch = H.empty_fr(n + L.zkp_scan_scratch_elems(n))
         zs = []
+        betas = fr_tensor([beta])
         for inp, tab in pairs:
-            betas = fr_tensor([beta])
             z = torch.empty((n, 4), dtype=torch.int64, device="cuda")
-            abi.check(L.zkp_shuffle_z(z.data_ptr(), ptr_array([inp.data_ptr()]).data_ptr(),
-                                      ptr_array([tab.data_ptr()]).data_ptr(), betas.data_ptr(), 1, n,
+            # the pointer arrays stay referenced until the call returns: a
+            # temporary freed inside the argument list can be handed out again
+            # to the next one before the kernel reads it
+            pi, pt = ptr_array([inp.data_ptr()]), ptr_array([tab.data_ptr()])
+            abi.check(L.zkp_shuffle_z(z.data_ptr(), pi.data_ptr(), pt.data_ptr(), betas.data_ptr(), 1, n,
                                       scratch.data_ptr(), _st()), "zkp_shuffle_z")
             zs.append(z)
         return zs
@@ -561,7 +565,9 @@ class HotPath:
         wE_inv = pow(pow(wN, n, R_MOD), -1, R_MOD)
         einv = pow(E, -1, R_MOD)
         zinv = pow(ZETA, -1, R_MOD)
-        self.combine_consts = fr_tensor(self.t_inv + [pow(wE_inv, kk, R_MOD) for kk in range(E)] +
+        # the fused pass already divides each coset's values by Z_H (its
+        # `scale`), so the combine's per-coset factors are 1
+        self.combine_consts = fr_tensor([1] * E + [pow(wE_inv, kk, R_MOD) for kk in range(E)] +
                                         [pow(zinv, kk, R_MOD) * einv % R_MOD for kk in range(3)])
         self.t_inv_dev = fr_tensor(self.t_inv)
 
@@ -611,10 +617,19 @@ class HotPath:
         s, c, n, u = self.shape, self.c, self.n, self.u
         tr = Transcript(self.seed)
         proof = {"commitments": [], "evals": []}
+        self.phase_s = {}
+        t0 = [time.perf_counter()]
 
         def absorb(name, pts):
             tr.points(pts)
             proof["commitments"].append((name, pts))
+
+        def mark(phase):
+            # wall time of each phase (the transcript synchronises at every challenge)
+            torch.cuda.synchronize()
+            t = time.perf_counter()
+            self.phase_s[phase] = t - t0[0]
+            t0[0] = t
 
         # 1. advice and instance
         adv = [c.advice[i] for i in range(s.advice)]
@@ -633,6 +648,7 @@ class HotPath:
         absorb("instance", com[s.advice:])
         absorb("advice", com[:s.advice])
         theta = tr.challenge()
+        mark("1 advice commit + iNTT")
 
         # 2. lookup multiplicities
         self.m = torch.zeros((s.lookups, n, 4), dtype=torch.int64, device="cuda")
@@ -640,6 +656,7 @@ class HotPath:
         absorb("lookup_m", self.commit(True, [self.m[i] for i in range(s.lookups)]))
         beta, gamma = tr.challenge(), tr.challenge()
         self.beta, self.gamma, self.theta = beta, gamma, theta
+        mark("2 lookup m")
 
         # 3. logup z, permutation and shuffle products
         self._logup_z(beta)
@@ -659,6 +676,7 @@ class HotPath:
         absorb("random", lz_com[-1:])
         y = tr.challenge()
         self.y = y
+        mark("3 grand products + commits")
 
         # 4. quotient
         if self.schedule == "plain":
@@ -670,9 +688,11 @@ class HotPath:
         # witness h has degree below degree (n - 1) - n, so the coefficients
         # past the pieces are zero
         pieces = [h_coeff[i * n:(i + 1) * n] for i in range(s.degree - 1)]
+        mark("4a quotient h")
         absorb("h_pieces", self.commit(False, pieces))
         x = tr.challenge()
         self.x = x
+        mark("4b h commits")
 
         # 5. evaluations
         xn = pow(x, n, R_MOD)
@@ -685,13 +705,14 @@ class HotPath:
         evals = self._evaluate(queries)
         tr.scalars(evals)
         proof["evals"] = evals
+        mark("5 evaluations")
 
         # 6. multi-open
         if s.multiopen == "shplonk":
             absorb("multiopen", self._shplonk(tr, queries, evals))
         else:
             absorb("multiopen", self._gwc(tr, queries, evals))
-        torch.cuda.synchronize()
+        mark("6 multiopen")
         proof["challenges"] = {"theta": theta, "beta": beta, "gamma": gamma, "y": y, "x": x}
         return proof
 
@@ -918,7 +939,7 @@ class HotPath:
         for name, _, cnt in wit:
             off[name] = base
             base += cnt
-        tmp = torch.empty((max(w[2] for w in wit) * n, 4), dtype=torch.int64, device="cuda")
+        tmp = torch.empty((min(NTT_CHUNK, max(w[2] for w in wit)) * n, 4), dtype=torch.int64, device="cuda")
 
         def col(name, i):
             return ev[off[name] + i]
@@ -1207,5 +1228,7 @@ class _RefMsm(H.ReferenceMsmBatch):
                                self.length, self.windows, self.c, self.threads, self.worker,
                                self.sort_buf.numel() * 4, 1, st)
             abi.check(err, "msm")
-        abi.check(self.sym.batch_msm_collect(None, None, None, None, self.regions.data_ptr(), self.worker,
-                                             self.windows, self.c, self.count, st), "batch_msm_collect")
+        r = self.remain
+        abi.check(self.sym.batch_msm_collect(r[0].data_ptr(), r[1].data_ptr(), r[2].data_ptr(), r[3].data_ptr(),
+                                             self.regions.data_ptr(), self.worker, self.windows, self.c, self.count,
+                                             st), "batch_msm_collect")
