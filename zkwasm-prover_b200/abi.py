@@ -126,17 +126,22 @@ class _Strict:
 
     def __init__(self, cdll):
         self._cdll = cdll
+        # per-entry-point call counts while counting is on (benchmark
+        # instrumentation: each call of a compute entry point launches one or
+        # more kernels)
+        self.calls = None
         for name, sig in SIGNATURES.items():
             fn = getattr(cdll, name)
             argtypes, restype = sig if isinstance(sig, tuple) else (sig, E)
             fn.argtypes, fn.restype = argtypes, restype
             setattr(self, name, self._wrap(name, fn, len(argtypes)))
 
-    @staticmethod
-    def _wrap(name, fn, arity):
+    def _wrap(self, name, fn, arity):
         def call(*args):
             if len(args) != arity:
                 raise TypeError(f"{name} takes {arity} arguments, got {len(args)}")
+            if self.calls is not None:
+                self.calls[name] = self.calls.get(name, 0) + 1
             return fn(*args)
 
         call.__name__ = name

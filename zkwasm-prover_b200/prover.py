@@ -295,10 +295,11 @@ def ntt_cols(buf, tables: Tables, ncols: int, inverse: bool, tmp=None, stream=No
 NTT_CHUNK = 32
 
 
-def ntt_into(out, src, tables: Tables, ncols: int, inverse: bool, in_mul=None, tmp=None, stream=None):
+def ntt_into(out, src, tables: Tables, ncols: int, inverse: bool, in_mul=None, tmp=None, stream=None, events=None):
     """Out-of-place batched transform of ncols contiguous columns, NTT_CHUNK
     columns per launch: out = NTT(src * in_mul) (or iNTT scaled by n^-1);
-    tables from this library (natural order)."""
+    tables from this library (natural order).  events: optional list that
+    receives (start, end, columns) CUDA events around each launch group."""
     n = 1 << tables.log_n
     step = min(ncols, NTT_CHUNK)
     tmp = torch.empty((step * n, 4), dtype=torch.int64, device="cuda") if tmp is None else tmp
@@ -306,10 +307,16 @@ def ntt_into(out, src, tables: Tables, ncols: int, inverse: bool, in_mul=None, t
     sr = src.reshape(-1, 4)
     for c0 in range(0, ncols, step):
         cnt = min(step, ncols - c0)
+        if events is not None:
+            ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True), cnt)
+            ev[0].record(stream)
         abi.check(lib().zkp_ntt_batch_twisted(o[c0 * n:].data_ptr(), sr[c0 * n:].data_ptr(), tmp.data_ptr(),
                                               (tables.tw_inv if inverse else tables.tw).data_ptr(), _p(in_mul),
                                               tables.n_inv.data_ptr() if inverse else 0, tables.log_n, cnt, n, n,
                                               _st(stream)), "zkp_ntt_batch_twisted")
+        if events is not None:
+            ev[1].record(stream)
+            events.append(ev)
 
 
 def powers(base: int, w: int, n: int, out=None) -> torch.Tensor:
@@ -508,6 +515,9 @@ class HotPath:
         self.sym = symbols or lib()
         self.hw = host_work or DeviceHostWork()
         self.seed = seed
+        # when set to a list, the batched quotient's coset transforms append
+        # (start, end, columns) CUDA events to it (benchmark instrumentation)
+        self.ntt_events = None
         s = self.shape
         self.E = 1 << s.ext_bits
         self.ek = self.k + s.ext_bits
@@ -608,6 +618,17 @@ class HotPath:
         else:
             for c in cols:
                 ntt_cols(c, self.tab_n, 1, True)
+
+    def counts(self):
+        """Work units of one proof in this schedule: MSMs of n points, NTTs of
+        n points (batched) or of n and 2^(k+e) points (plain), and the
+        polynomials whose coset values the quotient needs."""
+        s = self.shape
+        msm = (s.advice + 1) + s.lookups + (s.perm_chunks + s.shuffles) + (s.lookups + 1) + (s.degree - 1)
+        msm += 2 if s.multiopen == "shplonk" else 3
+        cols = s.advice + 1 + s.perm_chunks + 2 * s.lookups + s.shuffles + s.fixed + s.perm + 3
+        return {"msm": msm, "quotient_columns": cols, "cosets": self.E,
+                "ntt_n": (s.advice + 1) + 2 * s.lookups + s.perm_chunks + s.shuffles + cols * self.E + self.E + 2}
 
     # ------------------------------------------------------------ the proof
 
@@ -995,7 +1016,8 @@ class HotPath:
         for j in range(E):
             tw = self.coset_twist[j]
             for name, src, cnt in wit:
-                ntt_into(ev[off[name]:off[name] + cnt], src, self.tab_n, cnt, False, in_mul=tw, tmp=tmp)
+                ntt_into(ev[off[name]:off[name] + cnt], src, self.tab_n, cnt, False, in_mul=tw, tmp=tmp,
+                         events=self.ntt_events)
             args.x = self.coset_x[j].data_ptr()
             args.scale = self.t_inv_dev[j].data_ptr()
             abi.check(L.zkp_eval_h_fused(hc[j].data_ptr(), ctypes.byref(args), st), "zkp_eval_h_fused")
