@@ -31,7 +31,11 @@ import subprocess
 import sys
 import time
 
-import torch
+# the proof's buffers come and go in sizes of 0.1-30 GiB: growable segments
+# keep the caching allocator from fragmenting HBM between the schedules
+os.environ.setdefault("PYTORCH_CUDA_ALLOC_CONF", "expandable_segments:True")
+
+import torch  # noqa: E402
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)

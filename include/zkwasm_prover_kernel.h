@@ -379,10 +379,15 @@ cudaError_t zkp_shuffle_z(void *z, const void *inputs, const void *tables, const
  * NULL), every output times *scale when scale is non-NULL.  With in_mul[k] =
  * (zeta w_N^j)^k it gives coset j of the extended domain zeta <w_N>
  * (N = E n) from coefficients.  tmp: n * ncols elements (unused for one-pass
- * sizes). */
+ * sizes).  pairs != 0: omegas, in_mul and scale hold (w, w') known-factor
+ * pairs (zkp_shoup_pairs), 2 elements an entry. */
 cudaError_t zkp_ntt_batch_twisted(void *out, const void *in, void *tmp, const void *omegas, const void *in_mul,
                                   const void *scale, int log_n, uint32_t ncols, size_t in_stride, size_t out_stride,
-                                  cudaStream_t stream);
+                                  int pairs, cudaStream_t stream);
+
+/* out[2i], out[2i+1] = (w, w' = floor(w 2^256 / r)) for the Montgomery-form
+ * factors in[i], i < n: the table form of products by a known factor. */
+cudaError_t zkp_shoup_pairs(void *out, const void *in, uint32_t n, cudaStream_t stream);
 
 /* Arguments of zkp_eval_h_fused.  Every pointer is a device pointer; `T**`
  * fields are device arrays of device pointers.  Row i of every column is row

@@ -31,17 +31,27 @@ def P(gpu):
     return importlib.import_module("zkwasm-prover_b200.prover")
 
 
-def _run(P, shape, schedule, symbols=None, host_work=None, seed=3):
+def _run(P, shape, schedule, symbols=None, host_work=None, seed=3, **kw):
     c = P.Circuit(shape, seed=seed)
-    hp = P.HotPath(c, schedule, symbols=symbols, host_work=host_work)
+    hp = P.HotPath(c, schedule, symbols=symbols, host_work=host_work, **kw)
     return hp, hp.prove()
 
 
+# the batched schedule with (w, w') pair tables and every proving-key coset
+# cached, with Montgomery tables and nothing cached, and with the cache holding
+# only part of the cosets (the rest transformed per proof)
+BATCHED = {"pairs_cached": {}, "montgomery_uncached": {"pair_tables": False, "pk_cache_gib": 0},
+           "partly_cached": {"pk_cache_gib": 0.0003}}
+
+
+@pytest.mark.parametrize("variant", sorted(BATCHED))
 @pytest.mark.parametrize("name", ["gwc_deg4", "shplonk_deg9"])
-def test_plain_and_batched_agree(P, name):
+def test_plain_and_batched_agree(P, name, variant):
     shape = _shapes(P)[name]
     hp_p, proof_p = _run(P, shape, "plain")
-    hp_b, proof_b = _run(P, shape, "batched")
+    hp_b, proof_b = _run(P, shape, "batched", **BATCHED[variant])
+    if variant == "partly_cached":
+        assert 0 < len(hp_b.pk_cos) < 3 * hp_b.E
     assert proof_p["challenges"] == proof_b["challenges"]
     for (na, a), (nb, b) in zip(proof_p["commitments"], proof_b["commitments"]):
         assert na == nb and a == b, na

@@ -91,7 +91,8 @@ SIGNATURES = {
     "zkp_mlp_grad": [P, P, P, P, U, P, P, P, S],
     "zkp_mlp_train_step": [P, P, P, P, P, P, P, U, ctypes.c_float, I, P, P, S],
     "zkp_msm_schedule_predict": ([P, P, I, I, P, S], I),
-    "zkp_ntt_batch_twisted": [P, P, P, P, P, P, I, U, SZ, SZ, S],
+    "zkp_ntt_batch_twisted": [P, P, P, P, P, P, I, U, SZ, SZ, I, S],
+    "zkp_shoup_pairs": [P, P, U, S],
     "zkp_eval_h_fused": [P, P, S],
     "zkp_coset_combine": [P, P, SZ, P, P, I, I, S],
     "zkp_poly_divide_scratch_elems": ([U], SZ),

@@ -301,7 +301,7 @@ extern "C" {
 
 cudaError_t zkp_ntt_batch_twisted(void* out, const void* in, void* tmp, const void* omegas, const void* in_mul,
                                   const void* scale, int log_n, uint32_t ncols, size_t in_stride, size_t out_stride,
-                                  cudaStream_t stream) {
+                                  int pairs, cudaStream_t stream) {
     if (log_n < 1 || log_n > 28 || !out || !in || !omegas || ncols == 0 || ncols > 65535) return cudaErrorInvalidValue;
     const size_t n = (size_t)1 << log_n;
     if (in_stride < n || out_stride < n || out == in) return cudaErrorInvalidValue;
@@ -325,6 +325,7 @@ cudaError_t zkp_ntt_batch_twisted(void* out, const void* in, void* tmp, const vo
         a.scale = p == np - 1 ? reinterpret_cast<const Fr*>(scale) : nullptr;
         a.src_ys = src_stride;
         a.dst_ys = to_out ? out_stride : n;
+        a.pairs = pairs ? 1 : 0;
         ZK_CHECK(ntt_pass(a, rad[p], ncols, 1, stream));
         src = dst;
         src_stride = a.dst_ys;
@@ -397,6 +398,12 @@ cudaError_t zkp_coset_combine(void* out, const void* g, size_t g_stride, const v
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
+}
+
+cudaError_t zkp_shoup_pairs(void* out, const void* in, uint32_t n, cudaStream_t stream) {
+    if (n == 0) return cudaSuccess;
+    if (!out || !in || out == in) return cudaErrorInvalidValue;
+    return shoup_pairs(reinterpret_cast<Fr*>(out), CFr(in), n, stream);
 }
 
 size_t zkp_poly_divide_scratch_elems(uint32_t n) { return 4 * (size_t)n + fr_scan_tmp_elems(n); }

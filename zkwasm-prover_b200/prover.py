@@ -313,7 +313,26 @@ def ntt_into(out, src, tables: Tables, ncols: int, inverse: bool, in_mul=None, t
         abi.check(lib().zkp_ntt_batch_twisted(o[c0 * n:].data_ptr(), sr[c0 * n:].data_ptr(), tmp.data_ptr(),
                                               (tables.tw_inv if inverse else tables.tw).data_ptr(), _p(in_mul),
                                               tables.n_inv.data_ptr() if inverse else 0, tables.log_n, cnt, n, n,
-                                              _st(stream)), "zkp_ntt_batch_twisted")
+                                              0, _st(stream)), "zkp_ntt_batch_twisted")
+        if events is not None:
+            ev[1].record(stream)
+            events.append(ev)
+
+
+def _ntt_into_pairs(out, src, tw_pairs, in_mul_pairs, ncols: int, log_n: int, tmp, events=None, stream=None):
+    """ntt_into's forward transform over (w, w') pair tables."""
+    n = 1 << log_n
+    step = min(ncols, NTT_CHUNK)
+    o = out.reshape(-1, 4)
+    sr = src.reshape(-1, 4)
+    for c0 in range(0, ncols, step):
+        cnt = min(step, ncols - c0)
+        if events is not None:
+            ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True), cnt)
+            ev[0].record(stream)
+        abi.check(lib().zkp_ntt_batch_twisted(o[c0 * n:].data_ptr(), sr[c0 * n:].data_ptr(), tmp.data_ptr(),
+                                              tw_pairs.data_ptr(), in_mul_pairs.data_ptr(), 0, log_n, cnt, n, n,
+                                              1, _st(stream)), "zkp_ntt_batch_twisted")
         if events is not None:
             ev[1].record(stream)
             events.append(ev)
@@ -505,7 +524,8 @@ class HotPath:
     plain schedule calls (default: this one); ``host_work``: the CPU-side steps
     (default: DeviceHostWork)."""
 
-    def __init__(self, circuit: Circuit, schedule="batched", symbols=None, host_work=None, seed=7, srs_seed=11):
+    def __init__(self, circuit: Circuit, schedule="batched", symbols=None, host_work=None, seed=7, srs_seed=11,
+                 pair_tables=False, pk_cache_gib=None):
         if schedule not in ("plain", "batched"):
             raise ValueError(schedule)
         self.c = circuit
@@ -518,6 +538,14 @@ class HotPath:
         # when set to a list, the batched quotient's coset transforms append
         # (start, end, columns) CUDA events to it (benchmark instrumentation)
         self.ntt_events = None
+        # batched schedule: coset transforms over Montgomery tables, or over
+        # (w, w') known-factor tables (pair_tables; at 2^22 the radix-2^11
+        # passes run no faster with them: 1.028 against 0.994 ms a column);
+        # proving-key coset values cached up to pk_cache_gib (None: as much as
+        # the proof's memory leaves, 0: none)
+        self.pair_tables = pair_tables
+        self.pk_cache_gib = pk_cache_gib
+        self.pk_cos = {}
         s = self.shape
         self.E = 1 << s.ext_bits
         self.ek = self.k + s.ext_bits
@@ -580,6 +608,52 @@ class HotPath:
         self.combine_consts = fr_tensor([1] * E + [pow(wE_inv, kk, R_MOD) for kk in range(E)] +
                                         [pow(zinv, kk, R_MOD) * einv % R_MOD for kk in range(3)])
         self.t_inv_dev = fr_tensor(self.t_inv)
+        # known-factor (w, w') forms of the forward twiddles and the coset twists
+        if self.pair_tables:
+            self.tab_pairs = torch.empty((2 * n, 4), dtype=torch.int64, device="cuda")
+            abi.check(L.zkp_shoup_pairs(self.tab_pairs.data_ptr(), self.tab_n.tw.data_ptr(), n, _st()),
+                      "zkp_shoup_pairs")
+            self.coset_twist_pairs = torch.empty((E, 2 * n, 4), dtype=torch.int64, device="cuda")
+            for j in range(E):
+                abi.check(L.zkp_shoup_pairs(self.coset_twist_pairs[j].data_ptr(), self.coset_twist[j].data_ptr(), n,
+                                            _st()), "zkp_shoup_pairs")
+        self._cache_pk_cosets()
+
+    def _cache_pk_cosets(self):
+        """Coset values of the proving key's columns (fixed, then l_0 / l_last /
+        l_active, then sigma, one coset at a time), computed once and kept in
+        HBM as far as the memory a proof needs leaves room, as halo2's pk keeps
+        its fixed and permutation cosets; the quotient then transforms only the
+        witness's columns."""
+        s, n, E = self.shape, self.n, self.E
+        self.pk_cos = {}
+        if self.pk_cache_gib is not None:
+            budget = self.pk_cache_gib * (1 << 30)
+        else:
+            free, _ = torch.cuda.mem_get_info()
+            col = n * 32
+            # the proof's own peak: coefficient forms of the witness's columns,
+            # the per-coset workspace of the uncached columns, MSM scratch and
+            # transforms, with a margin
+            per_proof = col * (2 * (s.advice + 1) + 3 * s.lookups + 2 * (s.perm_chunks + s.shuffles) +
+                               (s.advice + 1 + s.perm_chunks + 2 * s.lookups + s.shuffles) + NTT_CHUNK + 3 * E)
+            per_proof += 8 << 30
+            budget = free - per_proof - (24 << 30)
+        tmp = torch.empty((NTT_CHUNK * n, 4), dtype=torch.int64, device="cuda")
+        order = [("fixed", self.fixed_coeff, s.fixed), ("l", self.l_coeff, 3), ("sigma", self.sigma_coeff, s.perm)]
+        used = 0
+        for name, src, cnt in order:
+            for j in range(E):
+                size = cnt * n * 32
+                if used + size > budget:
+                    break
+                t = torch.empty((cnt, n, 4), dtype=torch.int64, device="cuda")
+                self._coset_ntt(t, src, cnt, j, tmp)
+                self.pk_cos[(name, j)] = t
+                used += size
+        self.pk_cache_bytes = used
+        del tmp
+        torch.cuda.synchronize()
 
     # ------------------------------------------------------------ MSM helpers
 
@@ -947,80 +1021,89 @@ class HotPath:
         E = self.E
         L = lib()
         st = _st()
-        # every coefficient column the constraints read: witness and proving key
-        wit = [("adv", self.adv_coeff, s.advice), ("inst", self.inst_coeff, 1),
+        # every coefficient column the constraints read: the witness's, and the
+        # proving key's (fixed, sigma, l_0 / l_last / l_active) unless their
+        # coset values are cached (setup)
+        dyn = [("adv", self.adv_coeff, s.advice), ("inst", self.inst_coeff, 1),
                ("pz", torch.stack(self.perm_z), len(self.perm_z)), ("m", self.m_coeff, s.lookups),
                ("lz", self.lookup_z, s.lookups), ("sz", torch.stack(self.shuffle_z) if self.shuffle_z else None,
-                                                   len(self.shuffle_z)),
-               ("fixed", self.fixed_coeff, s.fixed), ("sigma", self.sigma_coeff, s.perm), ("l", self.l_coeff, 3)]
-        wit = [w for w in wit if w[2] > 0]
-        total = sum(w[2] for w in wit)
-        ev = torch.empty((total, n, 4), dtype=torch.int64, device="cuda")
+                                                   len(self.shuffle_z))]
+        pk = [("fixed", self.fixed_coeff, s.fixed), ("sigma", self.sigma_coeff, s.perm), ("l", self.l_coeff, 3)]
+        groups = [w for w in dyn + pk if w[2] > 0]
+        # rows of the per-coset workspace: every group that is not cached for all cosets
+        work = [w for w in groups if not all((w[0], j) in self.pk_cos for j in range(E))]
+        total = sum(w[2] for w in work)
+        ev = torch.empty((max(1, total), n, 4), dtype=torch.int64, device="cuda")
         off, base = {}, 0
-        for name, _, cnt in wit:
+        for name, _, cnt in work:
             off[name] = base
             base += cnt
-        tmp = torch.empty((min(NTT_CHUNK, max(w[2] for w in wit)) * n, 4), dtype=torch.int64, device="cuda")
-
-        def col(name, i):
-            return ev[off[name] + i]
-
-        # the argument block of zkp_eval_h_fused, rebuilt per coset for X
+        tmp = torch.empty((min(NTT_CHUNK, max(w[2] for w in groups)) * n, 4), dtype=torch.int64, device="cuda")
         yt, bt, gt = fr_tensor([y]), fr_tensor([beta]), fr_tensor([gamma])
         G = s.gates
-        v, rots, keep = [], [], []
-        for g in range(G):
-            co = pow(y, G - 1 - g, R_MOD)
-            q = col("fixed", c.selector_cols[g])
-            a, b, cc, d, e = [col("adv", x) for x in c.gate_cols[g]]
-            for coeff, fs in ((co, [q, a, b, cc]), (co, [q, d]), ((-co) % R_MOD, [q, e])):
-                ct = fr_tensor([coeff])
-                keep.append(ct)
-                v.append(ct.data_ptr())
-                v.extend(f.data_ptr() for f in fs)
-                rots.extend([0] * len(fs))
-                v.append(0)
-        gate_terms = ptr_array(v)
-        gate_rots = torch.tensor(rots, dtype=torch.int32, device="cuda")
-        kinds = {"advice": "adv", "fixed": "fixed", "instance": "inst"}
-        perm_cols = ptr_array([col(kinds[kd], i).data_ptr() for kd, i in c.perm_cols])
-        perm_sig = ptr_array([col("sigma", j).data_ptr() for j in range(s.perm)])
-        perm_z = ptr_array([col("pz", j).data_ptr() for j in range(len(self.perm_z))])
+        coeffs = fr_tensor([pow(y, G - 1 - g, R_MOD) if t < 2 else (-pow(y, G - 1 - g, R_MOD)) % R_MOD
+                            for g in range(G) for t in range(3)])
         dbeta = fr_tensor([beta * pow(DELTA, j, R_MOD) for j in range(s.perm)])
-        lk = []
-        for i, cl in enumerate(c.lookup_cols):
-            lk += [col("adv", cl).data_ptr(), col("fixed", c.table_col).data_ptr(), col("m", i).data_ptr(),
-                   col("lz", i).data_ptr()]
-        lookup_cols = ptr_array(lk) if lk else None
-        sh = []
-        for j, (a, b) in enumerate(c.shuffle_pairs):
-            sh += [col("sz", j).data_ptr(), col("adv", a).data_ptr(), col("adv", b).data_ptr()]
-        shuffle_cols = ptr_array(sh) if sh else None
-        shuffle_len = torch.ones(max(1, s.shuffles), dtype=torch.int32, device="cuda")
         betas = fr_tensor([pow(beta, i + 1, R_MOD) for i in range(16)])
+        shuffle_len = torch.ones(max(1, s.shuffles), dtype=torch.int32, device="cuda")
+        # one rotation (0) per column entry of the gate terms: 4 + 2 + 2 a gate
+        gate_rots = torch.zeros(max(1, 8 * G), dtype=torch.int32, device="cuda")
+        kinds = {"advice": "adv", "fixed": "fixed", "instance": "inst"}
         hc = torch.empty((E, n, 4), dtype=torch.int64, device="cuda")
-        args = _EvalHArgs()
-        args.n = n
-        args.rot_scale = 1
-        args.y = yt.data_ptr()
-        args.gate_terms, args.gate_rots, args.gate_terms_n = gate_terms.data_ptr(), gate_rots.data_ptr(), len(v)
-        args.l0, args.l_last, args.l_active = col("l", 0).data_ptr(), col("l", 1).data_ptr(), col("l", 2).data_ptr()
-        args.beta, args.gamma = bt.data_ptr(), gt.data_ptr()
-        args.perm_chunks, args.perm_chunk_len, args.perm_cols_n = len(self.perm_z), s.chunk_len, s.perm
-        args.perm_last_rot = -(s.blinding + 1)
-        args.perm_z, args.perm_cols, args.perm_sigmas = perm_z.data_ptr(), perm_cols.data_ptr(), perm_sig.data_ptr()
-        args.perm_dbeta = dbeta.data_ptr()
-        args.lookups, args.lookup_cols = s.lookups, _p(lookup_cols)
-        args.shuffles, args.shuffle_cols = s.shuffles, _p(shuffle_cols)
-        args.shuffle_group_len, args.shuffle_betas = shuffle_len.data_ptr(), betas.data_ptr()
         for j in range(E):
             tw = self.coset_twist[j]
-            for name, src, cnt in wit:
-                ntt_into(ev[off[name]:off[name] + cnt], src, self.tab_n, cnt, False, in_mul=tw, tmp=tmp,
-                         events=self.ntt_events)
+            # this coset's values of every column not cached
+            for name, src, cnt in work:
+                if (name, j) in self.pk_cos:
+                    continue
+                self._coset_ntt(ev[off[name]:off[name] + cnt], src, cnt, j, tmp)
+
+            def col(name, i, j=j):
+                cached = self.pk_cos.get((name, j))
+                return cached[i] if cached is not None else ev[off[name] + i]
+
+            # the argument block of zkp_eval_h_fused for this coset
+            v = []
+            for g in range(G):
+                q = col("fixed", c.selector_cols[g])
+                a, b, cc, d, e = [col("adv", x) for x in c.gate_cols[g]]
+                for t, fs in enumerate(([q, a, b, cc], [q, d], [q, e])):
+                    v.append(coeffs[3 * g + t].data_ptr())
+                    v.extend(f.data_ptr() for f in fs)
+                    v.append(0)
+            assert sum(1 for x in v if x) - 3 * G == 8 * G, "gate term layout"
+            gate_terms = ptr_array(v)
+            perm_cols = ptr_array([col(kinds[kd], i).data_ptr() for kd, i in c.perm_cols])
+            perm_sig = ptr_array([col("sigma", i).data_ptr() for i in range(s.perm)])
+            perm_z = ptr_array([col("pz", i).data_ptr() for i in range(len(self.perm_z))])
+            lk = []
+            for i, cl in enumerate(c.lookup_cols):
+                lk += [col("adv", cl).data_ptr(), col("fixed", c.table_col).data_ptr(), col("m", i).data_ptr(),
+                       col("lz", i).data_ptr()]
+            lookup_cols = ptr_array(lk) if lk else None
+            sh = []
+            for i, (a_, b_) in enumerate(c.shuffle_pairs):
+                sh += [col("sz", i).data_ptr(), col("adv", a_).data_ptr(), col("adv", b_).data_ptr()]
+            shuffle_cols = ptr_array(sh) if sh else None
+            args = _EvalHArgs()
+            args.n = n
+            args.rot_scale = 1
+            args.y = yt.data_ptr()
+            args.gate_terms, args.gate_rots, args.gate_terms_n = gate_terms.data_ptr(), gate_rots.data_ptr(), len(v)
+            args.l0, args.l_last, args.l_active = col("l", 0).data_ptr(), col("l", 1).data_ptr(), col("l", 2).data_ptr()
+            args.beta, args.gamma = bt.data_ptr(), gt.data_ptr()
+            args.perm_chunks, args.perm_chunk_len, args.perm_cols_n = len(self.perm_z), s.chunk_len, s.perm
+            args.perm_last_rot = -(s.blinding + 1)
+            args.perm_z, args.perm_cols, args.perm_sigmas = perm_z.data_ptr(), perm_cols.data_ptr(), perm_sig.data_ptr()
+            args.perm_dbeta = dbeta.data_ptr()
+            args.lookups, args.lookup_cols = s.lookups, _p(lookup_cols)
+            args.shuffles, args.shuffle_cols = s.shuffles, _p(shuffle_cols)
+            args.shuffle_group_len, args.shuffle_betas = shuffle_len.data_ptr(), betas.data_ptr()
             args.x = self.coset_x[j].data_ptr()
             args.scale = self.t_inv_dev[j].data_ptr()
             abi.check(L.zkp_eval_h_fused(hc[j].data_ptr(), ctypes.byref(args), st), "zkp_eval_h_fused")
+            # keep this coset's pointer arrays referenced until the kernel has read them
+            self._keep = (gate_terms, perm_cols, perm_sig, perm_z, lookup_cols, shuffle_cols)
         del ev, tmp
         # back to the 2^(k+e) coefficients of h
         g = torch.empty_like(hc)
@@ -1029,7 +1112,17 @@ class HotPath:
         abi.check(L.zkp_coset_combine(out.data_ptr(), g.data_ptr(), n, self.winv_N.data_ptr(),
                                       self.combine_consts.data_ptr(), self.k, s.ext_bits, st), "zkp_coset_combine")
         torch.cuda.synchronize()
+        self._keep = None
         return out
+
+    def _coset_ntt(self, out, src, cnt, j, tmp):
+        """Coset j of cnt coefficient columns: NTT_n of c_k (zeta w_N^j)^k, over
+        (w, w') pair tables when the schedule uses them."""
+        if self.pair_tables:
+            _ntt_into_pairs(out, src, self.tab_pairs, self.coset_twist_pairs[j], cnt, self.k, tmp,
+                            events=self.ntt_events)
+        else:
+            ntt_into(out, src, self.tab_n, cnt, False, in_mul=self.coset_twist[j], tmp=tmp, events=self.ntt_events)
 
     # ------------------------------------------------------------ phase 5
 
