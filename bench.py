@@ -1445,13 +1445,14 @@ def run_pipeline(args):
         print(json.dumps(out))
 
 
-# kernels each library entry point launches at the proof's sizes (2^22 and
-# the batched MSM pipeline over a table), from the ncu launch list of one
-# proof; entry points not listed launch one kernel
-KERNELS_PER_CALL = {"zkp_ntt_batch_twisted": 2, "zkp_ntt_batch": 2, "zkp_msm_batch_table": 9,
-                    "zkp_poly_divide_linear": 7, "zkp_poly_eval_batch": 2, "zkp_permutation_z": 5,
-                    "zkp_shuffle_z": 5, "eval_logup_z_compose": 4, "logup_sum_input_inv": 1,
-                    "prepare_table_lookup": 2, "calc_m": 2, "zkp_powers": 2, "shplonk_h_x_div_points": 1}
+# kernels each library entry point launches at the proof's sizes (2^22, the
+# batched MSM pipeline over a table), counted from the ncu launch list of one
+# proof (1089 launches of this library's kernels); entry points not listed
+# launch one kernel
+KERNELS_PER_CALL = {"zkp_msm_batch_table": 14, "zkp_ntt_batch_twisted": 2, "zkp_ntt_batch": 2, "ntt": 2,
+                    "calc_m": 2, "prepare_table_lookup": 1, "logup_sum_input_inv": 1, "eval_logup_z_compose": 6,
+                    "zkp_permutation_z": 6, "zkp_shuffle_z": 6, "zkp_powers": 2, "zkp_poly_divide_linear": 9,
+                    "zkp_poly_eval_batch": 2}
 NO_KERNEL = {"zkp_msm_batch_table_scratch_bytes", "zkp_scan_scratch_elems", "zkp_poly_divide_scratch_elems",
              "zkp_poly_eval_batch_scratch_elems", "zkp_msm_batch_table_default_window"}
 
