@@ -111,3 +111,36 @@ def test_commitments_match_known_dlogs(O, P):
         exp = O.msm_known_dlog(dl, a)
         ex = [O.fq_ints(exp[:, :4])[0], O.fq_ints(exp[:, 4:])[0]]
         assert tuple(ex) == adv[i]
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_sharded_schedule_same_proof(P, world):
+    """The batched schedule sharded over `world` ranks (commitments by column
+    ranges, quotient cosets round robin) gives the unsharded proof.  The ranks
+    are threads on one GPU exchanging through the host (shard.ThreadGroup):
+    their kernels never wait on one another."""
+    import threading
+
+    S = importlib.import_module("zkwasm-prover_b200.shard")
+    shape = _shapes(P)["shplonk_deg9"]
+    _, ref = _run(P, shape, "batched")
+    g = S.ThreadGroup(world)
+    proofs, errors = [None] * world, []
+
+    def rank(r):
+        try:
+            c = P.Circuit(shape, seed=3)
+            hp = P.HotPath(c, "batched", group=g.view(r))
+            proofs[r] = hp.prove()
+        except BaseException as e:  # noqa: BLE001
+            errors.append(e)
+            g.barrier.abort()
+
+    ts = [threading.Thread(target=rank, args=(r,)) for r in range(world)]
+    for t in ts:
+        t.start()
+    for t in ts:
+        t.join(timeout=600)
+    assert not errors, errors
+    for p in proofs:
+        assert p["commitments"] == ref["commitments"] and p["evals"] == ref["evals"]

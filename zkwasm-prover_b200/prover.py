@@ -293,6 +293,7 @@ def ntt_cols(buf, tables: Tables, ncols: int, inverse: bool, tmp=None, stream=No
 
 
 NTT_CHUNK = 32
+MSM_BATCH = 8
 
 
 def ntt_into(out, src, tables: Tables, ncols: int, inverse: bool, in_mul=None, tmp=None, stream=None, events=None):
@@ -525,7 +526,7 @@ class HotPath:
     (default: DeviceHostWork)."""
 
     def __init__(self, circuit: Circuit, schedule="batched", symbols=None, host_work=None, seed=7, srs_seed=11,
-                 pair_tables=False, pk_cache_gib=None):
+                 pair_tables=False, pk_cache_gib=None, group=None):
         if schedule not in ("plain", "batched"):
             raise ValueError(schedule)
         self.c = circuit
@@ -546,6 +547,18 @@ class HotPath:
         self.pair_tables = pair_tables
         self.pk_cache_gib = pk_cache_gib
         self.pk_cos = {}
+        # batched schedule on several GPUs: a torch.distributed process group
+        # whose ranks (one per GPU, each with the same circuit) share the
+        # proof: commitments by column ranges, the quotient by cosets (shard.py)
+        self.group = group
+        if group is not None:
+            from . import shard
+
+            self.rank, self.world = shard.rank_world(group)
+            if schedule != "batched":
+                raise ValueError("sharding needs the batched schedule")
+        else:
+            self.rank, self.world = 0, 1
         s = self.shape
         self.E = 1 << s.ext_bits
         self.ek = self.k + s.ext_bits
@@ -642,8 +655,14 @@ class HotPath:
         tmp = torch.empty((NTT_CHUNK * n, 4), dtype=torch.int64, device="cuda")
         order = [("fixed", self.fixed_coeff, s.fixed), ("l", self.l_coeff, 3), ("sigma", self.sigma_coeff, s.perm)]
         used = 0
+        if self.world > 1:
+            from . import shard
+
+            mine = shard.coset_ranks(E, self.world)[self.rank]
+        else:
+            mine = list(range(E))
         for name, src, cnt in order:
-            for j in range(E):
+            for j in mine:
                 size = cnt * n * 32
                 if used + size > budget:
                     break
@@ -671,8 +690,10 @@ class HotPath:
             return []
         table = self.table_gl if lagrange else self.table_g
         outs = []
-        for i in range(0, len(cols), 16):
-            part = cols[i:i + 16]
+        # pipelines of MSM_BATCH MSMs: at 2^22 over the c = 19 table, 8 a
+        # pipeline run at 13.05 ms an MSM against 13.64 for 16 and 14.21 for 32
+        for i in range(0, len(cols), MSM_BATCH):
+            part = cols[i:i + MSM_BATCH]
             out = H.msm_batch_table(table, self.n, self.tc, part, [self.n] * len(part))
             outs.append(out)
         torch.cuda.synchronize()
@@ -681,6 +702,11 @@ class HotPath:
     def commit(self, lagrange: bool, cols):
         if self.schedule == "plain":
             return self._msm_plain(self.g_lagrange if lagrange else self.g, cols)
+        if self.world > 1:
+            from . import shard
+
+            a, b = shard.column_ranges(len(cols), self.world)[self.rank]
+            return shard.gather_points(self._msm_batched(lagrange, cols[a:b]), self.group)
         return self._msm_batched(lagrange, cols)
 
     def intt_many(self, cols):
@@ -1049,9 +1075,14 @@ class HotPath:
         # one rotation (0) per column entry of the gate terms: 4 + 2 + 2 a gate
         gate_rots = torch.zeros(max(1, 8 * G), dtype=torch.int32, device="cuda")
         kinds = {"advice": "adv", "fixed": "fixed", "instance": "inst"}
-        hc = torch.empty((E, n, 4), dtype=torch.int64, device="cuda")
-        for j in range(E):
-            tw = self.coset_twist[j]
+        hc = torch.zeros((E, n, 4), dtype=torch.int64, device="cuda")
+        if self.world > 1:
+            from . import shard
+
+            mine = shard.coset_ranks(E, self.world)[self.rank]
+        else:
+            mine = list(range(E))
+        for j in mine:
             # this coset's values of every column not cached
             for name, src, cnt in work:
                 if (name, j) in self.pk_cos:
@@ -1105,6 +1136,8 @@ class HotPath:
             # keep this coset's pointer arrays referenced until the kernel has read them
             self._keep = (gate_terms, perm_cols, perm_sig, perm_z, lookup_cols, shuffle_cols)
         del ev, tmp
+        if self.world > 1:
+            shard.gather_cosets(hc, mine, E, self.group)
         # back to the 2^(k+e) coefficients of h
         g = torch.empty_like(hc)
         ntt_into(g, hc, self.tab_n, E, True)
