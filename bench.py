@@ -1264,18 +1264,22 @@ def _time_proofs(hp, steps, warmup, ws, clocks=None, profile=False):
 def _e2e_proofs(P, hp, circuit, steps, ws):
     """The same proof end to end from HOST buffers: every step copies the
     witness (advice and instance Lagrange columns) from pinned host memory
-    into the device columns, proves, and reads the proof (every commitment and
-    evaluation) back to the host."""
+    into the device columns (the advice in groups of columns, overlapped with
+    the commitments and transforms of the groups already copied), proves, and
+    reads the proof (every commitment and evaluation) back to the host."""
     host_adv = torch.empty(circuit.advice.shape, dtype=torch.int64, pin_memory=True)
     host_adv.copy_(circuit.advice)
     host_inst = torch.empty(circuit.instance.shape, dtype=torch.int64, pin_memory=True)
     host_inst.copy_(circuit.instance)
     h2d = (host_adv.numel() + host_inst.numel()) * 8
 
+    stage = P.HostStage(host_adv, circuit.advice)
+
     def one():
-        circuit.advice.copy_(host_adv, non_blocking=True)
+        # the instance column first, the advice columns in groups while phase
+        # 1 commits and transforms the groups already on the device
         circuit.instance.copy_(host_inst, non_blocking=True)
-        return hp.prove()
+        return hp.prove(stage=stage)
 
     proof = one()
     torch.cuda.synchronize()

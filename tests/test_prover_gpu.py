@@ -144,3 +144,17 @@ def test_sharded_schedule_same_proof(P, world):
     assert not errors, errors
     for p in proofs:
         assert p["commitments"] == ref["commitments"] and p["evals"] == ref["evals"]
+
+
+def test_witness_staged_from_host(P):
+    """The advice columns copied in from pinned host memory group by group,
+    overlapped with phase 1, give the same proof as resident columns."""
+    shape = _shapes(P)["shplonk_deg9"]
+    hp, ref = _run(P, shape, "batched")
+    host = torch.empty(hp.c.advice.shape, dtype=torch.int64, pin_memory=True)
+    host.copy_(hp.c.advice)
+    hp.c.advice.zero_()
+    stage = P.HostStage(host, hp.c.advice, group=3)
+    for _ in range(2):
+        proof = hp.prove(stage=stage)
+        assert proof["commitments"] == ref["commitments"] and proof["evals"] == ref["evals"]

@@ -460,6 +460,37 @@ class Circuit:
         del ident, mapping, vals
 
 
+# ---------------------------------------------------------------- witness from host memory
+
+
+class HostStage:
+    """Copies the advice columns from pinned host memory into the circuit's
+    device columns in groups of `group` columns on a copy stream, one event
+    per group; the prover waits on a group's event before its first use."""
+
+    def __init__(self, host_advice: torch.Tensor, dev_advice: torch.Tensor, group: int = MSM_BATCH):
+        self.host, self.dev, self.group = host_advice, dev_advice, group
+        self.stream = torch.cuda.Stream()
+        self.events = []
+
+    def start(self):
+        # the copies overwrite the columns: order them after the work already queued
+        self.stream.wait_stream(torch.cuda.current_stream())
+        self.events = []
+        with torch.cuda.stream(self.stream):
+            for g0 in range(0, self.host.shape[0], self.group):
+                g1 = min(self.host.shape[0], g0 + self.group)
+                self.dev[g0:g1].copy_(self.host[g0:g1], non_blocking=True)
+                ev = torch.cuda.Event()
+                ev.record(self.stream)
+                self.events.append((g0, g1, ev))
+
+    def wait(self, lo: int, hi: int):
+        for g0, g1, ev in self.events:
+            if g0 < hi and g1 > lo:
+                torch.cuda.current_stream().wait_event(ev)
+
+
 # ---------------------------------------------------------------- host-side steps
 
 
@@ -732,9 +763,11 @@ class HotPath:
 
     # ------------------------------------------------------------ the proof
 
-    def prove(self):
+    def prove(self, stage=None):
         """Runs phases 1-6; returns the proof stand-in: every commitment
-        (affine ints) and evaluation, in transcript order."""
+        (affine ints) and evaluation, in transcript order.  stage: a
+        HostStage bringing the advice columns in from host memory during
+        phase 1 (batched schedule)."""
         s, c, n, u = self.shape, self.c, self.n, self.u
         tr = Transcript(self.seed)
         proof = {"commitments": [], "evals": []}
@@ -760,6 +793,24 @@ class HotPath:
             self.adv_coeff = c.advice.clone()
             self.inst_coeff = c.instance.clone()
             self.intt_many([self.adv_coeff[i] for i in range(s.advice)] + [self.inst_coeff[0]])
+        elif stage is not None and self.world == 1:
+            # the witness arrives from host memory: commit and transform each
+            # group of columns as soon as its copy has landed, while later
+            # groups are still crossing PCIe (src/lib.rs overlaps the copies
+            # of its columns with the MSMs of earlier ones the same way)
+            self.adv_coeff = torch.empty_like(c.advice)
+            self.inst_coeff = torch.empty_like(c.instance)
+            stage.start()
+            outs = []
+            for a0 in range(0, s.advice, MSM_BATCH):
+                a1 = min(s.advice, a0 + MSM_BATCH)
+                stage.wait(a0, a1)
+                part = adv[a0:a1] + (inst if a1 == s.advice else [])
+                outs.append(H.msm_batch_table(self.table_gl, n, self.tc, part, [n] * len(part)))
+                ntt_into(self.adv_coeff[a0:a1], c.advice[a0:a1], self.tab_n, a1 - a0, True)
+            ntt_into(self.inst_coeff, c.instance, self.tab_n, 1, True)
+            torch.cuda.synchronize()
+            com = jac_to_affine(torch.cat(outs).cpu().numpy().view(np.uint64))
         else:
             com = self.commit(True, adv + inst)
             self.adv_coeff = torch.empty_like(c.advice)
