@@ -93,7 +93,7 @@ struct EvalHView {
 // max permutation columns whose beta delta^c factors are staged per block
 static constexpr int EVAL_H_MAX_PERM = 256;
 
-__global__ void __launch_bounds__(256) eval_h_fused_kernel(Fr* h, EvalHView a) {
+__global__ void __launch_bounds__(256, 2) eval_h_fused_kernel(Fr* h, EvalHView a) {
     __shared__ KnownFr s_dbeta[EVAL_H_MAX_PERM];
     for (int c = threadIdx.x; c < a.perm_cols_n; c += blockDim.x) s_dbeta[c] = known_fr(ld_elem<FrCfg>(a.perm_dbeta + c));
     const KnownFr ky = block_known(a.y);
