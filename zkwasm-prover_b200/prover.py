@@ -503,6 +503,7 @@ class DeviceHostWork:
         s, n, u = ctx.shape, ctx.n, ctx.u
         L = lib()
         scratch = H.empty_fr(n + L.zkp_scan_scratch_elems(n))
+        zall = ctx._ws("perm_z", (s.perm_chunks, n, 4))
         zs = []
         bt, gt = fr_tensor([beta]), fr_tensor([gamma])
         for j in range(s.perm_chunks):
@@ -510,7 +511,7 @@ class DeviceHostWork:
             pc = ptr_array([c.data_ptr() for c in cols[c0:c1]])
             ps = ptr_array([c.data_ptr() for c in sigmas[c0:c1]])
             db = fr_tensor([beta * pow(DELTA, c, R_MOD) for c in range(c0, c1)])
-            z = torch.empty((n, 4), dtype=torch.int64, device="cuda")
+            z = zall[j]
             init = zs[-1][u:u + 1] if zs else fr_tensor([1])
             abi.check(L.zkp_permutation_z(z.data_ptr(), pc.data_ptr(), ps.data_ptr(), c1 - c0, bt.data_ptr(),
                                           gt.data_ptr(), db.data_ptr(), ctx.own_n.natural.data_ptr(), init.data_ptr(), n,
@@ -524,8 +525,9 @@ class DeviceHostWork:
         scratch = H.empty_fr(n + L.zkp_scan_scratch_elems(n))
         zs = []
         betas = fr_tensor([beta])
-        for inp, tab in pairs:
-            z = torch.empty((n, 4), dtype=torch.int64, device="cuda")
+        zall = ctx._ws("shuffle_z", (len(pairs), n, 4))
+        for j, (inp, tab) in enumerate(pairs):
+            z = zall[j]
             # the pointer arrays stay referenced until the call returns: a
             # temporary freed inside the argument list can be handed out again
             # to the next one before the kernel reads it
@@ -578,6 +580,7 @@ class HotPath:
         self.pair_tables = pair_tables
         self.pk_cache_gib = pk_cache_gib
         self.pk_cos = {}
+        self._wsd = {}
         # batched schedule on several GPUs: a torch.distributed process group
         # whose ranks (one per GPU, each with the same circuit) share the
         # proof: commitments by column ranges, the quotient by cosets (shard.py)
@@ -661,7 +664,53 @@ class HotPath:
             for j in range(E):
                 abi.check(L.zkp_shoup_pairs(self.coset_twist_pairs[j].data_ptr(), self.coset_twist[j].data_ptr(), n,
                                             _st()), "zkp_shoup_pairs")
+        self._workspaces()
         self._cache_pk_cosets()
+        self._alloc_quotient_workspace()
+
+    def _ws(self, name, shape, dtype=torch.int64):
+        """A per-proof buffer: allocated once for the batched schedule (a
+        prover runs proof after proof, and at k = 22 the proof's buffers take
+        most of the 180 GB; allocating them per proof fragments HBM), fresh
+        for the plain schedule (the reference host's per-call allocations)."""
+        if self.schedule != "batched":
+            return torch.empty(shape, dtype=dtype, device="cuda")
+        t = self._wsd.get(name)
+        if t is None or tuple(t.shape) != tuple(shape):
+            t = torch.empty(shape, dtype=dtype, device="cuda")
+            self._wsd[name] = t
+        return t
+
+    def _workspaces(self):
+        """The batched schedule's per-proof buffers, allocated at setup."""
+        s, n, E = self.shape, self.n, self.E
+        A, L_ = s.advice, s.lookups
+        for name, shape in (("adv_coeff", (A, n, 4)), ("inst_coeff", (1, n, 4)), ("m", (L_, n, 4)),
+                            ("m_coeff", (L_, n, 4)), ("lookup_z", (L_, n, 4)),
+                            ("perm_z", (s.perm_chunks, n, 4)), ("shuffle_z", (s.shuffles, n, 4)),
+                            ("ntt_tmp", (NTT_CHUNK * n, 4)), ("hc", (E, n, 4)), ("hg", (E, n, 4)),
+                            ("h_coeff", (E * n, 4))):
+            self._ws(name, shape)
+        na = (ctypes.c_uint32 * (MSM_BATCH + 1))(*([n] * (MSM_BATCH + 1)))
+        nbytes = lib().zkp_msm_batch_table_scratch_bytes(ctypes.addressof(na), MSM_BATCH + 1, n, self.tc)
+        self._ws("msm_scratch", (max(1, nbytes),), torch.uint8)
+
+    def _quotient_rows(self):
+        """(name, source, columns) of every column group the quotient reads,
+        the witness's first."""
+        s = self.shape
+        dyn = [("adv", "adv_coeff", s.advice), ("inst", "inst_coeff", 1), ("pz", "perm_z", s.perm_chunks),
+               ("m", "m_coeff", s.lookups), ("lz", "lookup_z", s.lookups), ("sz", "shuffle_z", s.shuffles)]
+        pk = [("fixed", "fixed_coeff", s.fixed), ("sigma", "sigma_coeff", s.perm), ("l", "l_coeff", 3)]
+        return [g for g in dyn if g[2] > 0], [g for g in pk if g[2] > 0]
+
+    def _alloc_quotient_workspace(self):
+        """One coset of every column the quotient transforms per proof: the
+        witness's and the proving key's not cached for every coset."""
+        dyn, pk = self._quotient_rows()
+        work = dyn + [g for g in pk if not all((g[0], j) in self.pk_cos for j in range(self.E))]
+        rows = sum(g[2] for g in work)
+        self._ws("ev", (max(1, rows), self.n, 4))
 
     def _cache_pk_cosets(self):
         """Coset values of the proving key's columns (fixed, then l_0 / l_last /
@@ -674,16 +723,14 @@ class HotPath:
         if self.pk_cache_gib is not None:
             budget = self.pk_cache_gib * (1 << 30)
         else:
+            # what is left once the per-proof buffers (allocated already) and
+            # the quotient's workspace for the witness's columns are set aside,
+            # less a margin for the proof's small buffers
+            torch.cuda.empty_cache()
             free, _ = torch.cuda.mem_get_info()
-            col = n * 32
-            # the proof's own peak: coefficient forms of the witness's columns,
-            # the per-coset workspace of the uncached columns, MSM scratch and
-            # transforms, with a margin
-            per_proof = col * (2 * (s.advice + 1) + 3 * s.lookups + 2 * (s.perm_chunks + s.shuffles) +
-                               (s.advice + 1 + s.perm_chunks + 2 * s.lookups + s.shuffles) + NTT_CHUNK + 3 * E)
-            per_proof += 8 << 30
-            budget = free - per_proof - (24 << 30)
-        tmp = torch.empty((NTT_CHUNK * n, 4), dtype=torch.int64, device="cuda")
+            dyn, _ = self._quotient_rows()
+            budget = free - sum(g[2] for g in dyn) * n * 32 - (10 << 30)
+        tmp = self._ws("ntt_tmp", (NTT_CHUNK * n, 4))
         order = [("fixed", self.fixed_coeff, s.fixed), ("l", self.l_coeff, 3), ("sigma", self.sigma_coeff, s.perm)]
         used = 0
         if self.world > 1:
@@ -702,7 +749,6 @@ class HotPath:
                 self.pk_cos[(name, j)] = t
                 used += size
         self.pk_cache_bytes = used
-        del tmp
         torch.cuda.synchronize()
 
     # ------------------------------------------------------------ MSM helpers
@@ -725,7 +771,8 @@ class HotPath:
         # pipeline run at 13.05 ms an MSM against 13.64 for 16 and 14.21 for 32
         for i in range(0, len(cols), MSM_BATCH):
             part = cols[i:i + MSM_BATCH]
-            out = H.msm_batch_table(table, self.n, self.tc, part, [self.n] * len(part))
+            out = H.msm_batch_table(table, self.n, self.tc, part, [self.n] * len(part),
+                                    scratch=self._wsd.get("msm_scratch"))
             outs.append(out)
         torch.cuda.synchronize()
         return jac_to_affine(torch.cat(outs).cpu().numpy().view(np.uint64))
@@ -798,32 +845,35 @@ class HotPath:
             # group of columns as soon as its copy has landed, while later
             # groups are still crossing PCIe (src/lib.rs overlaps the copies
             # of its columns with the MSMs of earlier ones the same way)
-            self.adv_coeff = torch.empty_like(c.advice)
-            self.inst_coeff = torch.empty_like(c.instance)
+            self.adv_coeff = self._ws("adv_coeff", tuple(c.advice.shape))
+            self.inst_coeff = self._ws("inst_coeff", tuple(c.instance.shape))
             stage.start()
             outs = []
             for a0 in range(0, s.advice, MSM_BATCH):
                 a1 = min(s.advice, a0 + MSM_BATCH)
                 stage.wait(a0, a1)
                 part = adv[a0:a1] + (inst if a1 == s.advice else [])
-                outs.append(H.msm_batch_table(self.table_gl, n, self.tc, part, [n] * len(part)))
-                ntt_into(self.adv_coeff[a0:a1], c.advice[a0:a1], self.tab_n, a1 - a0, True)
+                outs.append(H.msm_batch_table(self.table_gl, n, self.tc, part, [n] * len(part),
+                                              scratch=self._wsd["msm_scratch"]))
+                ntt_into(self.adv_coeff[a0:a1], c.advice[a0:a1], self.tab_n, a1 - a0, True,
+                         tmp=self._wsd["ntt_tmp"])
             ntt_into(self.inst_coeff, c.instance, self.tab_n, 1, True)
             torch.cuda.synchronize()
             com = jac_to_affine(torch.cat(outs).cpu().numpy().view(np.uint64))
         else:
             com = self.commit(True, adv + inst)
-            self.adv_coeff = torch.empty_like(c.advice)
-            ntt_into(self.adv_coeff, c.advice, self.tab_n, s.advice, True)
-            self.inst_coeff = torch.empty_like(c.instance)
-            ntt_into(self.inst_coeff, c.instance, self.tab_n, 1, True)
+            self.adv_coeff = self._ws("adv_coeff", tuple(c.advice.shape))
+            ntt_into(self.adv_coeff, c.advice, self.tab_n, s.advice, True, tmp=self._wsd.get("ntt_tmp"))
+            self.inst_coeff = self._ws("inst_coeff", tuple(c.instance.shape))
+            ntt_into(self.inst_coeff, c.instance, self.tab_n, 1, True, tmp=self._wsd.get("ntt_tmp"))
         absorb("instance", com[s.advice:])
         absorb("advice", com[:s.advice])
         theta = tr.challenge()
         mark("1 advice commit + iNTT")
 
         # 2. lookup multiplicities
-        self.m = torch.zeros((s.lookups, n, 4), dtype=torch.int64, device="cuda")
+        self.m = self._ws("m", (s.lookups, n, 4))
+        self.m.zero_()
         self._lookup_m()
         absorb("lookup_m", self.commit(True, [self.m[i] for i in range(s.lookups)]))
         beta, gamma = tr.challenge(), tr.challenge()
@@ -914,7 +964,7 @@ class HotPath:
         s, n, u = self.shape, self.n, self.u
         c = self.c
         bt = fr_tensor([beta])
-        self.lookup_z = torch.empty((s.lookups, n, 4), dtype=torch.int64, device="cuda")
+        self.lookup_z = self._ws("lookup_z", (s.lookups, n, 4))
         last = torch.zeros((max(1, s.lookups), 4), dtype=torch.int64, device="cuda")
         ssum = H.empty_fr(n)
         tmp = H.empty_fr(n)
@@ -927,7 +977,8 @@ class HotPath:
                                                     self.m[i].data_ptr(), bt.data_ptr(), last[i].data_ptr(), u, n,
                                                     _st()), "eval_logup_z_compose")
         # m (committed in Lagrange form above) and z to coefficients
-        self.m_coeff = self.m.clone()
+        self.m_coeff = self._ws("m_coeff", (s.lookups, n, 4))
+        self.m_coeff.copy_(self.m)
         if self.schedule == "plain":
             self.intt_many([self.m_coeff[i] for i in range(s.lookups)] + [self.lookup_z[i] for i in range(s.lookups)])
         else:
@@ -1101,21 +1152,20 @@ class HotPath:
         # every coefficient column the constraints read: the witness's, and the
         # proving key's (fixed, sigma, l_0 / l_last / l_active) unless their
         # coset values are cached (setup)
-        dyn = [("adv", self.adv_coeff, s.advice), ("inst", self.inst_coeff, 1),
-               ("pz", torch.stack(self.perm_z), len(self.perm_z)), ("m", self.m_coeff, s.lookups),
-               ("lz", self.lookup_z, s.lookups), ("sz", torch.stack(self.shuffle_z) if self.shuffle_z else None,
-                                                   len(self.shuffle_z))]
-        pk = [("fixed", self.fixed_coeff, s.fixed), ("sigma", self.sigma_coeff, s.perm), ("l", self.l_coeff, 3)]
-        groups = [w for w in dyn + pk if w[2] > 0]
+        dyn, pk = self._quotient_rows()
+        src = {"adv_coeff": self.adv_coeff, "inst_coeff": self.inst_coeff, "m_coeff": self.m_coeff,
+               "lookup_z": self.lookup_z, "fixed_coeff": self.fixed_coeff, "sigma_coeff": self.sigma_coeff,
+               "l_coeff": self.l_coeff, "perm_z": _stacked(self.perm_z), "shuffle_z": _stacked(self.shuffle_z)}
+        groups = [(name, src[key], cnt) for name, key, cnt in dyn + pk]
         # rows of the per-coset workspace: every group that is not cached for all cosets
         work = [w for w in groups if not all((w[0], j) in self.pk_cos for j in range(E))]
         total = sum(w[2] for w in work)
-        ev = torch.empty((max(1, total), n, 4), dtype=torch.int64, device="cuda")
+        ev = self._ws("ev", (max(1, total), n, 4))
         off, base = {}, 0
         for name, _, cnt in work:
             off[name] = base
             base += cnt
-        tmp = torch.empty((min(NTT_CHUNK, max(w[2] for w in groups)) * n, 4), dtype=torch.int64, device="cuda")
+        tmp = self._ws("ntt_tmp", (NTT_CHUNK * n, 4))
         yt, bt, gt = fr_tensor([y]), fr_tensor([beta]), fr_tensor([gamma])
         G = s.gates
         coeffs = fr_tensor([pow(y, G - 1 - g, R_MOD) if t < 2 else (-pow(y, G - 1 - g, R_MOD)) % R_MOD
@@ -1126,7 +1176,8 @@ class HotPath:
         # one rotation (0) per column entry of the gate terms: 4 + 2 + 2 a gate
         gate_rots = torch.zeros(max(1, 8 * G), dtype=torch.int32, device="cuda")
         kinds = {"advice": "adv", "fixed": "fixed", "instance": "inst"}
-        hc = torch.zeros((E, n, 4), dtype=torch.int64, device="cuda")
+        hc = self._ws("hc", (E, n, 4))
+        hc.zero_()
         if self.world > 1:
             from . import shard
 
@@ -1186,13 +1237,12 @@ class HotPath:
             abi.check(L.zkp_eval_h_fused(hc[j].data_ptr(), ctypes.byref(args), st), "zkp_eval_h_fused")
             # keep this coset's pointer arrays referenced until the kernel has read them
             self._keep = (gate_terms, perm_cols, perm_sig, perm_z, lookup_cols, shuffle_cols)
-        del ev, tmp
         if self.world > 1:
             shard.gather_cosets(hc, mine, E, self.group)
         # back to the 2^(k+e) coefficients of h
-        g = torch.empty_like(hc)
-        ntt_into(g, hc, self.tab_n, E, True)
-        out = torch.empty((E * n, 4), dtype=torch.int64, device="cuda")
+        g = self._ws("hg", (E, n, 4))
+        ntt_into(g, hc, self.tab_n, E, True, tmp=tmp)
+        out = self._ws("h_coeff", (E * n, 4))
         abi.check(L.zkp_coset_combine(out.data_ptr(), g.data_ptr(), n, self.winv_N.data_ptr(),
                                       self.combine_consts.data_ptr(), self.k, s.ext_bits, st), "zkp_coset_combine")
         torch.cuda.synchronize()
@@ -1375,6 +1425,19 @@ class HotPath:
         field_op(fz, fz, None, 2, n, l_c=fr_tensor([z0inv]), sym=sym)
         lx = self.hw.divide_linear(self, fz, uu)
         return c1 + self.commit(False, [lx])
+
+
+def _stacked(ts):
+    """The columns of a list as one (count, n, 4) tensor: the list's own
+    storage when its entries are consecutive rows of one tensor (the batched
+    schedule's workspaces), else a copy."""
+    if not ts:
+        return None
+    base = ts[0]
+    row = base.numel() * base.element_size()
+    if all(t.data_ptr() == base.data_ptr() + i * row for i, t in enumerate(ts)):
+        return torch.as_strided(base, (len(ts),) + tuple(base.shape), (base.numel(),) + tuple(base.stride()))
+    return torch.stack(ts)
 
 
 def _lagrange_interpolate(points, evals):
