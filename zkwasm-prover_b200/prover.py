@@ -691,8 +691,13 @@ class HotPath:
                             ("ntt_tmp", (NTT_CHUNK * n, 4)), ("hc", (E, n, 4)), ("hg", (E, n, 4)),
                             ("h_coeff", (E * n, 4))):
             self._ws(name, shape)
-        na = (ctypes.c_uint32 * (MSM_BATCH + 1))(*([n] * (MSM_BATCH + 1)))
-        nbytes = lib().zkp_msm_batch_table_scratch_bytes(ctypes.addressof(na), MSM_BATCH + 1, n, self.tc)
+        # the pipeline's scratch is not monotonic in the MSM count (the
+        # reduction's threads are shared out over the batch): the largest over
+        # every count a pipeline of the proof can have
+        nbytes = 0
+        for cnt in range(1, MSM_BATCH + 2):
+            na = (ctypes.c_uint32 * cnt)(*([n] * cnt))
+            nbytes = max(nbytes, lib().zkp_msm_batch_table_scratch_bytes(ctypes.addressof(na), cnt, n, self.tc))
         self._ws("msm_scratch", (max(1, nbytes),), torch.uint8)
 
     def _quotient_rows(self):
