@@ -1360,6 +1360,9 @@ def run_pipeline(args):
     ntt_cols = sum(e[2] for e in timed)
     hp.ntt_events = None
     counts = hp.counts()
+    memory = {"pk_coset_cache_gib": round(hp.pk_cache_bytes / 2 ** 30, 1),
+              "peak_allocated_gib": round(torch.cuda.max_memory_allocated() / 2 ** 30, 1),
+              "device_gib": round(torch.cuda.get_device_properties(device).total_memory / 2 ** 30, 1)}
     e2e = _e2e_proofs(P, hp, circuit, max(1, min(args.steps, 3)), ws)
     launches = _launch_count(calls_per_proof, shape)
     del hp
@@ -1436,6 +1439,7 @@ def run_pipeline(args):
                 "frac": round(mults_per / (avg_ms / 1e3) / mont_rate, 4),
                 "peak_kind": "measured Fr Montgomery products/s (zkp_calib_mont_rate)"},
             "counts": counts,
+            "memory": memory,
             "cpu_baseline": cpu,
         }
         out.update(extra)
