@@ -1350,6 +1350,7 @@ def run_pipeline(args):
     sec, proof, clk = _time_proofs(hp, args.steps, args.warmup, ws, clocks, profile=args.profile_range)
     digest = proof_digest(proof)
     phases = dict(hp.phase_s)
+    learned_picks = dict(hp.learned_picks)
     # the dominant kernel: the coset transforms of the quotient (two NTT
     # passes per launch group), timed by the events recorded inside the
     # timed region (the last `steps` proofs' groups)
@@ -1396,7 +1397,7 @@ def run_pipeline(args):
             extra = pipeline_extras(args, P, zkp, device)
         cpu = cpu_baseline_pipeline(counts, shape.k) if ws == 1 and not args.no_cpu_baseline else None
         out = {
-            "metric": f"k={shape.k} proof hot-path wall time (s/proof), batched schedule",
+            "metric": f"k={shape.k} proof hot-path wall time (s/proof), batched+learned schedule",
             "value": round(sec, 4),
             "unit": "s",
             "n_gpus": ws,
@@ -1414,13 +1415,15 @@ def run_pipeline(args):
                                    f"{shape.lookups} logup lookups, {shape.shuffles} shuffles, {shape.perm} "
                                    f"permutation columns, degree {shape.degree} (extended domain "
                                    f"2^{shape.k + shape.ext_bits})",
-                       "schedule": "batched: MSM pipelines over SRS tables, batched NTTs, per-coset fused "
-                                   "quotient (zkp_eval_h_fused) and coset combine, batched evaluations",
+                       "schedule": "batched+learned: MSM pipelines of 8 over SRS tables or plain bases as the "
+                                   "learned table-or-plain model picks, batched NTTs, per-coset fused quotient "
+                                   "(zkp_eval_h_fused) and coset combine, batched evaluations",
                        "parallelism": f"replicas x{ws}", "proofs_per_s": round(ws / sec, 4),
                        "l2": "every step streams > 100 GB of columns through HBM; no flush needed",
                        "transcript": "seeded BLAKE2b stand-in over every commitment and evaluation"},
             "proof_digest": digest,
             "phases_s": {k_: round(v, 4) for k_, v in phases.items()},
+            "learned_msm_picks_per_proof": learned_picks,
             "plain": plain,
             "speedup_vs_plain": round(plain["s_per_proof"] / sec, 3) if plain else None,
             "e2e": e2e,
@@ -1542,7 +1545,7 @@ def run_pipeline_reference(args):
     cb["value"] = v
     out = {
         "impl": "reference",
-        "metric": f"k={shape.k} proof hot-path wall time (s/proof), batched schedule",
+        "metric": f"k={shape.k} proof hot-path wall time (s/proof), batched+learned schedule",
         "value": v, "unit": "s", "n_gpus": ws, "steps": len(vals), "warmup": min(args.warmup, 1),
         "ms_per_step": round(v * 1e3, 1), "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
         "dtype": "bn254-fr", "data": "synthetic, seeded",

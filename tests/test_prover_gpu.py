@@ -40,8 +40,8 @@ def _run(P, shape, schedule, symbols=None, host_work=None, seed=3, **kw):
 # the batched schedule with (w, w') pair tables and every proving-key coset
 # cached, with Montgomery tables and nothing cached, and with the cache holding
 # only part of the cosets (the rest transformed per proof)
-BATCHED = {"pairs_cached": {}, "montgomery_uncached": {"pair_tables": False, "pk_cache_gib": 0},
-           "partly_cached": {"pk_cache_gib": 0.0003}}
+BATCHED = {"pairs_cached": {"pair_tables": True}, "montgomery_uncached": {"pair_tables": False, "pk_cache_gib": 0},
+           "partly_cached": {"pk_cache_gib": 0.0003}, "tables_only": {"learned": False}}
 
 
 @pytest.mark.parametrize("variant", sorted(BATCHED))

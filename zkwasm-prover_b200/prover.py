@@ -559,7 +559,7 @@ class HotPath:
     (default: DeviceHostWork)."""
 
     def __init__(self, circuit: Circuit, schedule="batched", symbols=None, host_work=None, seed=7, srs_seed=11,
-                 pair_tables=False, pk_cache_gib=None, group=None):
+                 pair_tables=False, pk_cache_gib=None, group=None, learned=True):
         if schedule not in ("plain", "batched"):
             raise ValueError(schedule)
         self.c = circuit
@@ -581,6 +581,16 @@ class HotPath:
         self.pk_cache_gib = pk_cache_gib
         self.pk_cos = {}
         self._wsd = {}
+        # batched schedule: MSM pipelines over the table or the plain bases as
+        # the learned table-or-plain model picks (with learned windows for the
+        # plain ones); learned=False keeps every pipeline on the table
+        self.learned = learned and schedule == "batched"
+        self.learned_picks = {}
+        if self.learned:
+            from . import choices, schedule as S
+
+            self._choice_msm = choices.ChoiceModel.load("msm_table")
+            self._window_model = S.Model.load()
         # batched schedule on several GPUs: a torch.distributed process group
         # whose ranks (one per GPU, each with the same circuit) share the
         # proof: commitments by column ranges, the quotient by cosets (shard.py)
@@ -771,16 +781,42 @@ class HotPath:
         if not cols:
             return []
         table = self.table_gl if lagrange else self.table_g
+        bases = self.g_lagrange if lagrange else self.g
         outs = []
         # pipelines of MSM_BATCH MSMs: at 2^22 over the c = 19 table, 8 a
         # pipeline run at 13.05 ms an MSM against 13.64 for 16 and 14.21 for 32
         for i in range(0, len(cols), MSM_BATCH):
             part = cols[i:i + MSM_BATCH]
-            out = H.msm_batch_table(table, self.n, self.tc, part, [self.n] * len(part),
-                                    scratch=self._wsd.get("msm_scratch"))
-            outs.append(out)
+            outs.append(self._msm_part(table, bases, part))
         torch.cuda.synchronize()
         return jac_to_affine(torch.cat(outs).cpu().numpy().view(np.uint64))
+
+    def _msm_part(self, table, bases, part):
+        """One MSM pipeline: over the SRS table, or over the plain bases with
+        learned windows when the learned table-or-plain choice says that runs
+        faster for this batch's size, count and scalar distribution."""
+        n = self.n
+        ns = [n] * len(part)
+        if self.learned:
+            from . import schedule as S
+
+            hist = S.histogram(part[0])
+            shape = {"n": n, "batch": len(part), "hist": hist}
+            if self._choice_msm.pick(shape, [0, 1]) == 0:
+                feats = S.shape_features(n, len(part), hist)
+                c = self._window_model.pick(feats)
+                ws = [c] * len(part)
+                na = (ctypes.c_uint32 * len(part))(*ns)
+                ca = (ctypes.c_int * len(part))(*ws)
+                nbytes = lib().zkp_msm_batch_scratch_bytes(ctypes.addressof(na), ctypes.addressof(ca), len(part))
+                scratch = self._wsd.get("msm_plain_scratch")
+                if scratch is None or scratch.numel() < nbytes:
+                    scratch = torch.empty(max(1, nbytes), dtype=torch.uint8, device="cuda")
+                    self._wsd["msm_plain_scratch"] = scratch
+                self.learned_picks["plain"] = self.learned_picks.get("plain", 0) + 1
+                return H.msm_batch(bases, part, ns, ws, scratch=scratch)
+            self.learned_picks["table"] = self.learned_picks.get("table", 0) + 1
+        return H.msm_batch_table(table, n, self.tc, part, ns, scratch=self._wsd.get("msm_scratch"))
 
     def commit(self, lagrange: bool, cols):
         if self.schedule == "plain":
@@ -824,6 +860,7 @@ class HotPath:
         tr = Transcript(self.seed)
         proof = {"commitments": [], "evals": []}
         self.phase_s = {}
+        self.learned_picks = {}
         t0 = [time.perf_counter()]
 
         def absorb(name, pts):
@@ -858,8 +895,7 @@ class HotPath:
                 a1 = min(s.advice, a0 + MSM_BATCH)
                 stage.wait(a0, a1)
                 part = adv[a0:a1] + (inst if a1 == s.advice else [])
-                outs.append(H.msm_batch_table(self.table_gl, n, self.tc, part, [n] * len(part),
-                                              scratch=self._wsd["msm_scratch"]))
+                outs.append(self._msm_part(self.table_gl, self.g_lagrange, part))
                 ntt_into(self.adv_coeff[a0:a1], c.advice[a0:a1], self.tab_n, a1 - a0, True,
                          tmp=self._wsd["ntt_tmp"])
             ntt_into(self.inst_coeff, c.instance, self.tab_n, 1, True)
