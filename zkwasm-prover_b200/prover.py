@@ -744,7 +744,7 @@ class HotPath:
             torch.cuda.empty_cache()
             free, _ = torch.cuda.mem_get_info()
             dyn, _ = self._quotient_rows()
-            budget = free - sum(g[2] for g in dyn) * n * 32 - (10 << 30)
+            budget = free - sum(g[2] for g in dyn) * n * 32 - (14 << 30)
         tmp = self._ws("ntt_tmp", (NTT_CHUNK * n, 4))
         order = [("fixed", self.fixed_coeff, s.fixed), ("l", self.l_coeff, 3), ("sigma", self.sigma_coeff, s.perm)]
         used = 0
