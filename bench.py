@@ -22,6 +22,7 @@ from __future__ import annotations
 import argparse
 import ctypes
 import datetime
+import gc
 import importlib
 import json
 import math
@@ -611,7 +612,8 @@ def run_msm_columns(zkp, device, count=16, log_n=18, reps=3):
     return res
 
 
-def run_msm_batch(zkp, device, count=32, lo=14, hi=20, seed=2024, reps=3, reference_windows=False):
+def run_msm_batch(zkp, device, count=32, lo=14, hi=20, seed=2024, reps=3, reference_windows=False,
+                  one_window_sweep=True):
     """Batched uneven MSMs over one SRS (sizes 2^U, U uniform in [lo, hi];
     per MSM the scalars are uniform (50%), small < 2^20 (35%) or 90%-sparse
     (15%)): plain per-MSM zkp_msm launches against one zkp_msm_batch pipeline,
@@ -672,7 +674,7 @@ def run_msm_batch(zkp, device, count=32, lo=14, hi=20, seed=2024, reps=3, refere
         res[f"batched_{name}_ms"] = round(timed(lambda: H.msm_batch(bases, cols, ns, ws, scratch=bscr, out=bout)), 3)
         # the result keeps its scratch alive (tens of GB for a 256-MSM pipeline)
         del bscr, bout
-    if reference_windows:
+    if reference_windows and one_window_sweep:
         # the exhaustive autotuner over one window for the whole pipeline
         tuned = {}
         n_arr = (ctypes.c_uint32 * count)(*ns)
@@ -728,20 +730,63 @@ def run_msm_batch(zkp, device, count=32, lo=14, hi=20, seed=2024, reps=3, refere
     return res
 
 
-def run_msm_config_c(args):
+def msm_uneven(zkp, device, one_window_sweep=True):
     """256 uneven MSMs over one SRS, sizes 2^U with U uniform in [14, 22], the
     mixed scalar distribution of run_msm_batch: plain per-MSM launches and
     one batched pipeline, with the library's windows, the learned schedule
-    and the reference host's window formula (src/cuda/msm.rs:105)."""
-    torch.cuda.set_device(0)
-    zkp = importlib.import_module("zkwasm-prover_b200")
-    zkp.load_library()
-    r = run_msm_batch(zkp, torch.device("cuda", 0), count=256, lo=14, hi=22, reps=1, reference_windows=True)
+    and the reference host's window formula (src/cuda/msm.rs:105), and one
+    pipeline over an SRS table."""
+    r = run_msm_batch(zkp, device, count=256, lo=14, hi=22, reps=1, reference_windows=True,
+                      one_window_sweep=one_window_sweep)
     r.pop("mixes", None)
     r.pop("sizes_log2", None)
     for k in ("learned_windows", "default_windows", "reference_windows"):
         r.pop(k, None)
-    print(json.dumps({"metric": "256 uneven MSMs 2^14..2^22 (ms)", "msm_config_c": r}))
+    torch.cuda.empty_cache()
+    return r
+
+
+def run_coset_ntt(args):
+    """The quotient's coset transform alone: NTT_n of --cols coefficient
+    columns of 2^k twisted by (zeta w_N)^i (coset 1 of the 8n domain), one
+    zkp_ntt_batch_twisted launch group, Montgomery tables as the proof uses at
+    k >= 22.  Prints the device time per launch group and the algorithmic
+    GB/s (one read and one write of every column); a bounded case for a
+    profiler (8 columns of 2^22: 3 GiB on the device)."""
+    torch.cuda.set_device(0)
+    P = _prover()
+    n = 1 << args.k
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(7)
+    src = P.rand_fr(args.cols * n, gen).reshape(args.cols, n, 4)
+    out = torch.empty_like(src)
+    tmp = torch.empty((args.cols * n, 4), dtype=torch.int64, device="cuda")
+    tab = P.Tables(args.k)
+    sj = P.ZETA * P.omega(args.k + 3) % P.R_MOD
+    twist = P.powers(1, sj, n)
+    for _ in range(max(3, args.warmup)):
+        P.ntt_into(out, src, tab, args.cols, False, in_mul=twist, tmp=tmp)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(args.steps):
+        P.ntt_into(out, src, tab, args.cols, False, in_mul=twist, tmp=tmp)
+    b.record()
+    b.synchronize()
+    ms = a.elapsed_time(b) / args.steps
+    peak, kind = load_peaks()
+    gbs = 2 * args.cols * n * 32 / (ms / 1e3) / 1e9
+    print(json.dumps({"metric": f"coset NTT of {args.cols} columns of 2^{args.k}", "ms_per_launch_group": round(ms, 3),
+                      "algorithmic_gb_per_s": round(gbs, 1), "frac_of_hbm": round(gbs / peak, 4),
+                      "peak_kind": kind, "steps": args.steps}))
+
+
+def run_msm_uneven(args):
+    torch.cuda.set_device(0)
+    zkp = importlib.import_module("zkwasm-prover_b200")
+    zkp.load_library()
+    r = msm_uneven(zkp, torch.device("cuda", 0))
+    print(json.dumps({"metric": "256 uneven MSMs 2^14..2^22 (ms)", "msm_256_uneven": r}))
 
 
 def run_graph(ph, steps):
@@ -1215,7 +1260,7 @@ def _prover():
 
 
 def _shape(P, args):
-    return P.config_e(args.k) if args.config == "e" else P.config_d(args.k)
+    return P.shplonk_shape(args.k) if args.config == "e" else P.gwc_shape(args.k)
 
 
 def proof_digest(proof) -> str:
@@ -1360,6 +1405,9 @@ def run_pipeline(args):
     ntt_ms = sum(e[0].elapsed_time(e[1]) for e in timed)
     ntt_cols = sum(e[2] for e in timed)
     hp.ntt_events = None
+    # the fused constraint pass against the reference's kernels one family at
+    # a time on the same coset (and both against the proof's h)
+    fused_vs_separate = hp.coset_fused_vs_separate()
     counts = hp.counts()
     memory = {"pk_coset_cache_gib": round(hp.pk_cache_bytes / 2 ** 30, 1),
               "peak_allocated_gib": round(torch.cuda.max_memory_allocated() / 2 ** 30, 1),
@@ -1367,6 +1415,7 @@ def run_pipeline(args):
     e2e = _e2e_proofs(P, hp, circuit, max(1, min(args.steps, 3)), ws)
     launches = _launch_count(calls_per_proof, shape)
     del hp
+    gc.collect()
     torch.cuda.empty_cache()
     # the plain schedule (the reference host's one-kernel-per-column calls
     # through this library) on the same circuit, for the batched/plain ratio
@@ -1377,6 +1426,7 @@ def run_pipeline(args):
         plain = {"s_per_proof": round(psec, 4), "phases_s": {k_: round(v, 4) for k_, v in hpp.phase_s.items()},
                  "steps": max(1, min(args.steps, 3)), "same_proof_as_batched": proof_digest(pproof) == digest}
         del hpp
+        gc.collect()
         torch.cuda.empty_cache()
     out = None
     if rank == 0:
@@ -1409,8 +1459,7 @@ def run_pipeline(args):
             "vs_baseline": None,
             "dtype": "bn254-fr / bn254-fq (8x u32 Montgomery)",
             "data": "synthetic seeded circuit generated on the device; witness satisfies every constraint",
-            "config": {"workload": ("configs[4]: SHPLONK proof hot path, " if args.config == "e" else
-                                    "configs[3]: GWC proof hot path, ") +
+            "config": {"workload": ("SHPLONK proof hot path, " if args.config == "e" else "GWC proof hot path, ") +
                                    f"k={shape.k}, {shape.advice} advice, {shape.fixed} fixed, 1 instance, "
                                    f"{shape.lookups} logup lookups, {shape.shuffles} shuffles, {shape.perm} "
                                    f"permutation columns, degree {shape.degree} (extended domain "
@@ -1424,6 +1473,7 @@ def run_pipeline(args):
             "proof_digest": digest,
             "phases_s": {k_: round(v, 4) for k_, v in phases.items()},
             "learned_msm_picks_per_proof": learned_picks,
+            "quotient_coset_fused_vs_separate": fused_vs_separate,
             "plain": plain,
             "speedup_vs_plain": round(plain["s_per_proof"] / sec, 3) if plain else None,
             "e2e": e2e,
@@ -1476,11 +1526,12 @@ def _launch_count(calls, shape):
 
 def pipeline_extras(args, P, zkp, device):
     """Smaller companions of the headline on one GPU: the GWC proof of
-    configs[3] (k = 20) in both schedules, and the batched NTT phase of
-    configs[1] (64 columns of 2^20 -> 2^23)."""
+    k = 20 (40 advice columns, degree 4) in both schedules, and the batched
+    NTT phase of 64 columns of 2^20 extended to 2^23, and 256 uneven MSMs
+    (2^14..2^22) plain and batched."""
     out = {}
     if args.config == "e":
-        shape = P.config_d(20)
+        shape = P.gwc_shape(20)
         c = P.Circuit(shape, seed=PIPE_SEED)
         res = {}
         for sched in ("batched", "plain"):
@@ -1488,9 +1539,10 @@ def pipeline_extras(args, P, zkp, device):
             sec, proof, _ = _time_proofs(hp, 3, 1, 1)
             res[sched] = {"s_per_proof": round(sec, 4), "digest": proof_digest(proof)}
             del hp
+            gc.collect()
         res["speedup_vs_plain"] = round(res["plain"]["s_per_proof"] / res["batched"]["s_per_proof"], 3)
         res["same_proof"] = res["plain"]["digest"] == res["batched"]["digest"]
-        out["config_d_gwc_k20"] = res
+        out["gwc_proof_k20"] = res
         del c
         torch.cuda.empty_cache()
     ph = ExtendPhase(zkp, device, columns=64, log_n=20, ext_bits=3, chunk=8, seed=1)
@@ -1504,11 +1556,12 @@ def pipeline_extras(args, P, zkp, device):
     b.record()
     torch.cuda.synchronize()
     ms = a.elapsed_time(b) / 3
-    out["ntt_phase_config_b"] = {"ms_per_step": round(ms, 3), "unit": "GB/s",
+    out["ntt_phase_64x2^20_to_2^23"] = {"ms_per_step": round(ms, 3), "unit": "GB/s",
                                  "value": round(64 * ph.bytes_per_column() / (ms / 1e3) / 1e9, 2),
                                  "workload": "64 columns x 2^20 Lagrange -> iNTT -> coset NTT on 2^23 (shift 7)"}
     del ph
     torch.cuda.empty_cache()
+    out["msm_256_uneven_2^14..2^22"] = msm_uneven(zkp, device, one_window_sweep=False)
     return out
 
 
@@ -1549,7 +1602,7 @@ def run_pipeline_reference(args):
         "value": v, "unit": "s", "n_gpus": ws, "steps": len(vals), "warmup": min(args.warmup, 1),
         "ms_per_step": round(v * 1e3, 1), "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
         "dtype": "bn254-fr", "data": "synthetic, seeded",
-        "config": {"workload": f"k={shape.k} proof hot path ({'configs[4]' if args.config == 'e' else 'configs[3]'})",
+        "config": {"workload": f"k={shape.k} {'SHPLONK' if args.config == 'e' else 'GWC'} proof hot path",
                    "sample": cb["sample"]},
         "cpu_baseline": cb,
         "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -1600,16 +1653,19 @@ def main():
     ap.add_argument("--no-rows", action="store_true", help="skip the per-row kernel timings")
     ap.add_argument("--msm-only", action="store_true", help="time only single MSMs (sizes from --msm-log-sizes)")
     ap.add_argument("--msm-log-sizes", default="18,22")
-    ap.add_argument("--msm-config-c", action="store_true", help="256 uneven MSMs 2^14..2^22 (about a minute)")
+    ap.add_argument("--msm-uneven", action="store_true", help="256 uneven MSMs 2^14..2^22 (about a minute)")
     ap.add_argument("--rows-only", action="store_true",
                     help="time only the per-row kernels (with --impl reference: the reference's kernels)")
     ap.add_argument("--ntt-phase", action="store_true",
-                    help="the batched NTT phase of configs[1] as the headline (64 x 2^20 -> 2^23)")
+                    help="the batched NTT phase as the headline (64 columns of 2^20 -> 2^23)")
+    ap.add_argument("--coset-ntt", action="store_true",
+                    help="time only the quotient's coset transform (--cols columns of 2^--k)")
+    ap.add_argument("--cols", type=int, default=8)
     ap.add_argument("--config", default="e", choices=["d", "e"],
-                    help="proof hot path of configs[4] (e, k = 22) or configs[3] (d, k = 20)")
+                    help="proof hot path: e = SHPLONK k = 22, 120 advice, degree 9; d = GWC k = 20, 40 advice, degree 4")
     ap.add_argument("--k", type=int, default=None)
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-schedule comparison")
-    ap.add_argument("--no-extras", action="store_true", help="skip config D and the NTT phase companions")
+    ap.add_argument("--no-extras", action="store_true", help="skip the k = 20 GWC proof and the NTT phase companions")
     ap.add_argument("--ntt-traffic", type=float, default=None, help=argparse.SUPPRESS)
     ap.add_argument("--profile-range", action="store_true",
                     help="bracket the timed proofs with cudaProfilerStart/Stop (for ncu --profile-from-start off)")
@@ -1624,8 +1680,10 @@ def main():
         run_pipeline_reference(args)
     elif args.msm_only:
         run_msm_only(args)
-    elif args.msm_config_c:
-        run_msm_config_c(args)
+    elif args.msm_uneven:
+        run_msm_uneven(args)
+    elif args.coset_ntt:
+        run_coset_ntt(args)
     elif args.ntt_phase:
         run_ours(args)
     else:

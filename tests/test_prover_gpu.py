@@ -158,3 +158,12 @@ def test_witness_staged_from_host(P):
     for _ in range(2):
         proof = hp.prove(stage=stage)
         assert proof["commitments"] == ref["commitments"] and proof["evals"] == ref["evals"]
+
+
+@pytest.mark.parametrize("name", ["gwc_deg4", "shplonk_deg9"])
+def test_fused_coset_equals_separate_kernels(P, name):
+    """The fused constraint pass of one coset equals the reference symbols run
+    one constraint family at a time on the same coset rows."""
+    hp, _ = _run(P, _shapes(P)[name], "batched")
+    r = hp.coset_fused_vs_separate(reps=1)
+    assert r["equal"], r

@@ -143,7 +143,7 @@ class Transcript:
 
 @dataclass
 class Shape:
-    """Column counts of the synthetic circuit (BASELINE configs D and E): one
+    """Column counts of the synthetic circuit (gwc_shape, shplonk_shape): one
     degree-4 gate q (a b c + d) - e = 0 per group of five advice columns with its
     own selector, logup lookups of single advice columns (values < 2^16) into a
     2^16 range table, shuffles of advice column pairs, copy-constraint cycles
@@ -184,13 +184,13 @@ class Shape:
         return (self.perm + self.chunk_len - 1) // self.chunk_len
 
 
-def config_d(k=20):
+def gwc_shape(k=20):
     """GWC proof, k = 20: 40 advice, 10 fixed, 1 instance column, 6 lookups,
     2 shuffles, 20 permutation columns, degree 4 (extended domain 4n)."""
     return Shape(k=k, advice=40, fixed=10, lookups=6, shuffles=2, perm=20, degree=4, multiopen="gwc")
 
 
-def config_e(k=22):
+def shplonk_shape(k=22):
     """SHPLONK proof, k = 22: 120 advice, 30 fixed, 24 lookups, 4 shuffles, 60
     permutation columns, quotient degree 8 (extended domain 8n = 2^25)."""
     return Shape(k=k, advice=120, fixed=30, lookups=24, shuffles=4, perm=60, degree=9, multiopen="shplonk")
@@ -1232,8 +1232,10 @@ class HotPath:
                     continue
                 self._coset_ntt(ev[off[name]:off[name] + cnt], src, cnt, j, tmp)
 
-            def col(name, i, j=j):
-                cached = self.pk_cos.get((name, j))
+            def col(name, i, j=j, pk_cos=self.pk_cos):
+                # no reference to self: the last coset's resolver is kept on
+                # the prover, and a cycle would hold its HBM past `del`
+                cached = pk_cos.get((name, j))
                 return cached[i] if cached is not None else ev[off[name] + i]
 
             # the argument block of zkp_eval_h_fused for this coset
@@ -1276,8 +1278,12 @@ class HotPath:
             args.x = self.coset_x[j].data_ptr()
             args.scale = self.t_inv_dev[j].data_ptr()
             abi.check(L.zkp_eval_h_fused(hc[j].data_ptr(), ctypes.byref(args), st), "zkp_eval_h_fused")
-            # keep this coset's pointer arrays referenced until the kernel has read them
+            # keep this coset's pointer arrays referenced until the kernel has
+            # read them, and the last coset's inputs for coset_fused_vs_separate
             self._keep = (gate_terms, perm_cols, perm_sig, perm_z, lookup_cols, shuffle_cols)
+            self._last_coset = {"j": j, "col": col, "args": args, "h": hc[j],
+                                "keep": (gate_terms, gate_rots, perm_cols, perm_sig, perm_z, lookup_cols, shuffle_cols,
+                                         coeffs, yt, bt, gt, dbeta, betas, shuffle_len)}
         if self.world > 1:
             shard.gather_cosets(hc, mine, E, self.group)
         # back to the 2^(k+e) coefficients of h
@@ -1289,6 +1295,105 @@ class HotPath:
         torch.cuda.synchronize()
         self._keep = None
         return out
+
+    def coset_fused_vs_separate(self, reps=3):
+        """The last proof's last coset evaluated again two ways: one
+        zkp_eval_h_fused launch, and the reference symbols one constraint
+        family at a time on the same coset rows (field_op_batch_mul_sum,
+        permutation_eval_h_p1 / p2, field_op for the chunk products,
+        logup_eval_h, shuffle_eval_h_v2, field_op for 1/Z_H), as the
+        reference's quotient runs them on its extended buffers.  Returns the
+        device milliseconds of each and whether both equal the proof's h on
+        that coset."""
+        ctx = self._last_coset
+        n = self.n
+        L = lib()
+        st = _st()
+        h_f = torch.empty((n, 4), dtype=torch.int64, device="cuda")
+        h_s = torch.empty((n, 4), dtype=torch.int64, device="cuda")
+
+        def timed(fn):
+            fn()
+            torch.cuda.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            for _ in range(reps):
+                fn()
+            b.record()
+            b.synchronize()
+            return a.elapsed_time(b) / reps
+
+        fused_ms = timed(lambda: abi.check(L.zkp_eval_h_fused(h_f.data_ptr(), ctypes.byref(ctx["args"]), st),
+                                           "zkp_eval_h_fused"))
+        launches = [0]
+        sep_ms = timed(lambda: self._coset_separate(h_s, ctx, launches))
+        return {"rows": n, "coset": ctx["j"], "fused_ms": round(fused_ms, 3), "separate_ms": round(sep_ms, 3),
+                "separate_launches": launches[0] // (reps + 1),
+                "equal": bool(torch.equal(h_f, ctx["h"]) and torch.equal(h_s, ctx["h"]))}
+
+    def _coset_separate(self, h, ctx, launches):
+        s, c, n = self.shape, self.c, self.n
+        col, j = ctx["col"], ctx["j"]
+        (gate_terms, gate_rots, _, _, _, _, _, _, yt, bt, gt, dbeta, betas, _) = ctx["keep"]
+        L = lib()
+        st = _st()
+        cnt = [0]
+
+        def fo(res, l, r, op, l_c=None, r_c=None, l_rot=0):
+            field_op(res, l, r, op, n, l_c=l_c, r_c=r_c, l_rot=l_rot)
+            cnt[0] += 1
+
+        h.zero_()
+        args = ctx["args"]
+        abi.check(L.field_op_batch_mul_sum(h.data_ptr(), args.gate_terms, args.gate_rots, args.gate_terms_n, n, st),
+                  "field_op_batch_mul_sum")
+        l0, ll, la = col("l", 0), col("l", 1), col("l", 2)
+        zs = [col("pz", i) for i in range(s.perm_chunks)]
+        abi.check(L.permutation_eval_h_p1(h.data_ptr(), zs[0].data_ptr(), zs[-1].data_ptr(), l0.data_ptr(),
+                                          ll.data_ptr(), yt.data_ptr(), n), "permutation_eval_h_p1")
+        sets = ptr_array([z.data_ptr() for z in zs])
+        abi.check(L.permutation_eval_h_p2(h.data_ptr(), sets.data_ptr(), l0.data_ptr(), ll.data_ptr(), yt.data_ptr(),
+                                          len(zs), -(s.blinding + 1), n), "permutation_eval_h_p2")
+        cnt[0] += 3
+        kinds = {"advice": "adv", "fixed": "fixed", "instance": "inst"}
+        X = self.coset_x[j]
+        Lb, Rb, t = (torch.empty((n, 4), dtype=torch.int64, device="cuda") for _ in range(3))
+        ci = 0
+        for zj in zs:
+            fo(Lb, zj, None, 2, l_rot=1)
+            Rb.copy_(zj)
+            for _ in range(s.chunk_len):
+                if ci == s.perm:
+                    break
+                kd, idx = c.perm_cols[ci]
+                v, sg = col(kinds[kd], idx), col("sigma", ci)
+                fo(t, sg, v, 0, l_c=bt)
+                fo(t, t, None, 0, r_c=gt)
+                fo(Lb, Lb, t, 1)
+                fo(t, X, v, 0, l_c=dbeta[ci:ci + 1])
+                fo(t, t, None, 0, r_c=gt)
+                fo(Rb, Rb, t, 1)
+                ci += 1
+            fo(Lb, Lb, Rb, 3)
+            fo(Lb, Lb, la, 1)
+            fo(h, h, Lb, 0, l_c=yt)
+        ones = fr_tensor([1] * 1).expand(n, 4).contiguous()
+        for i, cl in enumerate(c.lookup_cols):
+            fo(Lb, col("adv", cl), None, 0, r_c=bt)
+            fo(Rb, col("fixed", c.table_col), None, 0, r_c=bt)
+            abi.check(L.logup_eval_h(h.data_ptr(), Lb.data_ptr(), ones.data_ptr(), Rb.data_ptr(),
+                                     col("m", i).data_ptr(), col("lz", i).data_ptr(), col("lz", i).data_ptr(),
+                                     l0.data_ptr(), ll.data_ptr(), la.data_ptr(), yt.data_ptr(), 1, n, st),
+                      "logup_eval_h")
+            cnt[0] += 1
+        for i, (a_, b_) in enumerate(c.shuffle_pairs):
+            pa, pb = ptr_array([col("adv", a_).data_ptr()]), ptr_array([col("adv", b_).data_ptr()])
+            abi.check(L.shuffle_eval_h_v2(h.data_ptr(), pa.data_ptr(), pb.data_ptr(), betas.data_ptr(), 1,
+                                          col("sz", i).data_ptr(), l0.data_ptr(), ll.data_ptr(), la.data_ptr(),
+                                          yt.data_ptr(), 1, n), "shuffle_eval_h_v2")
+            cnt[0] += 1
+        fo(h, h, None, 2, l_c=self.t_inv_dev[j:j + 1])
+        launches[0] += cnt[0]
 
     def _coset_ntt(self, out, src, cnt, j, tmp):
         """Coset j of cnt coefficient columns: NTT_n of c_k (zeta w_N^j)^k, over
