@@ -1512,7 +1512,7 @@ def run_pipeline(args):
 # launch one kernel
 KERNELS_PER_CALL = {"zkp_msm_batch_table": 14, "zkp_ntt_batch_twisted": 2, "zkp_ntt_batch": 2, "ntt": 2,
                     "calc_m": 2, "prepare_table_lookup": 1, "logup_sum_input_inv": 1, "eval_logup_z_compose": 6,
-                    "zkp_permutation_z": 6, "zkp_shuffle_z": 6, "zkp_powers": 2, "zkp_poly_divide_linear": 9,
+                    "zkp_permutation_z": 4, "zkp_shuffle_z": 4, "zkp_powers": 2, "zkp_poly_divide_linear": 9,
                     "zkp_poly_eval_batch": 2}
 NO_KERNEL = {"zkp_msm_batch_table_scratch_bytes", "zkp_scan_scratch_elems", "zkp_poly_divide_scratch_elems",
              "zkp_poly_eval_batch_scratch_elems", "zkp_msm_batch_table_default_window"}

@@ -347,11 +347,20 @@ cudaError_t zkp_fr_to_mont(void *out, const void *in, uint32_t n, cudaStream_t s
 size_t zkp_scan_scratch_elems(uint32_t n);
 
 /* Exclusive prefix product / sum with carried-in value (init may be NULL):
- * out[i] = init (op) in[0] (op) ... (op) in[i-1]; out may alias in. */
+ * out[i] = init (op) in[0] (op) ... (op) in[i-1]; out may alias in.  Above
+ * 2048 elements the product runs in one launch (decoupled look-back over
+ * tiles of 2048 elements) and the sum as tile sums, their scan and a scan of
+ * each tile from its prefix (launches that never wait on one another). */
 cudaError_t zkp_grand_product(void *out, const void *in, uint32_t n, const void *init, void *scratch,
                               cudaStream_t stream);
 cudaError_t zkp_grand_sum(void *out, const void *in, uint32_t n, const void *init, void *scratch,
                           cudaStream_t stream);
+
+/* Waits of the single-pass scans (zkp_grand_product / zkp_grand_sum and the
+ * grand products built on them) that ran out of polls since the library was
+ * loaded: each took the missing tile as the identity, so a non-zero count
+ * means a wrong result.  Synchronous; 0xffffffff if the read failed. */
+uint32_t zkp_scan_timeouts(void);
 
 /* Permutation argument, one chunk of ncols columns (src/permutation.rs:16-150):
  * z[0] = *init, z[i+1] = z[i] * prod_c (v_c[i] + dbeta[c]*w^i + gamma) /

@@ -35,7 +35,9 @@ def test_batch_inverse(O, gpu, n, with_scratch):
     assert (H.to_host(d) == O.batch_inv(a)).all()
 
 
-@pytest.mark.parametrize("n", [1, 7, 2048, 2049, 300000, 1 << 22])
+# 2049 and 4097: a last tile of one element; (1 << 22) + 3: 2049 tiles, so the
+# look-back windows of 32 tiles wrap many times
+@pytest.mark.parametrize("n", [1, 7, 2048, 2049, 4097, 300000, 1 << 22, (1 << 22) + 3])
 def test_grand_product_and_sum(O, gpu, n):
     H = gpu.host
     a = O.rand_fr(n, 200 + n)
@@ -47,6 +49,12 @@ def test_grand_product_and_sum(O, gpu, n):
     H.grand_sum(out, H.to_device(a), None)
     torch.cuda.synchronize()
     assert (H.to_host(out) == O.prefix_sum_excl(a)).all()
+    # in place, with an initial value, and no look-back wait ran out
+    d = H.to_device(a)
+    H.grand_sum(d, d, H.to_device(init))
+    torch.cuda.synchronize()
+    assert (H.to_host(d) == O.prefix_sum_excl(a, init)).all()
+    assert gpu.load_library().zkp_scan_timeouts() == 0
 
 
 def test_logup_reference_abi(O, gpu):

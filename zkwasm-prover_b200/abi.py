@@ -74,6 +74,7 @@ SIGNATURES = {
     "zkp_extend_batch_tables": [P, P, P, U, I, I, P, P, P, S],
     "zkp_batch_inverse": [P, P, P, U, I, P, S],
     "zkp_scan_scratch_elems": ([U], SZ),
+    "zkp_scan_timeouts": ([], U),
     "zkp_g1_multiples": [P, P, U, S],
     "zkp_fr_to_mont": [P, P, U, S],
     "zkp_grand_product": [P, P, U, P, P, S],

@@ -754,6 +754,8 @@ cudaError_t zkp_batch_inverse(void* out, const void* in, const void* c, uint32_t
 
 size_t zkp_scan_scratch_elems(uint32_t n) { return fr_scan_tmp_elems(n); }
 
+uint32_t zkp_scan_timeouts(void) { return fr_scan_timeouts(); }
+
 cudaError_t zkp_fr_to_mont(void* out, const void* in, uint32_t n, cudaStream_t stream) {
     if (n && (!out || !in)) return cudaErrorInvalidValue;
     if (n == 0) return cudaSuccess;

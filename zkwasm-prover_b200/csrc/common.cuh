@@ -38,6 +38,28 @@ __device__ __forceinline__ void st_elem(Fe<C>* p, const Fe<C>& v) {
     q[1] = make_uint4(v.v[4], v.v[5], v.v[6], v.v[7]);
 }
 
+// Shared-memory tiles hold 32-byte elements as two 16-byte halves.  Element
+// p, half h lives at 16-byte slot 2 * (p ^ ((p >> 3) & 3)) + (h ^ (((p >> 2) ^
+// (p >> 5)) & 1)): a bijection on each tile that gives the eight threads of a
+// quarter-warp eight distinct bank groups both for runs of consecutive elements
+// and for the stride-8 writes of the first radix-8 sub-stage.
+__device__ __forceinline__ uint4* sm_slot(Fr* x, uint32_t p, uint32_t h) {
+    const uint32_t pp = p ^ ((p >> 3) & 3u);
+    const uint32_t hh = h ^ (((p >> 2) ^ (p >> 5)) & 1u);
+    return reinterpret_cast<uint4*>(x) + 2 * pp + hh;
+}
+__device__ __forceinline__ Fr sm_ld(Fr* x, uint32_t p) {
+    const uint4 a = *sm_slot(x, p, 0), b = *sm_slot(x, p, 1);
+    Fr r;
+    r.v[0] = a.x; r.v[1] = a.y; r.v[2] = a.z; r.v[3] = a.w;
+    r.v[4] = b.x; r.v[5] = b.y; r.v[6] = b.z; r.v[7] = b.w;
+    return r;
+}
+__device__ __forceinline__ void sm_st(Fr* x, uint32_t p, const Fr& v) {
+    *sm_slot(x, p, 0) = make_uint4(v.v[0], v.v[1], v.v[2], v.v[3]);
+    *sm_slot(x, p, 1) = make_uint4(v.v[4], v.v[5], v.v[6], v.v[7]);
+}
+
 // entry i of a multiplier table from the Montgomery form wm of its factor:
 // wm itself, or the pair (w, w' = floor(w 2^256 / r)) of fe_mul_shoup at
 // elements 2i and 2i + 1

@@ -650,7 +650,7 @@ ZK_HD Fe<C> fe_inv(const Fe<C>& a) {
         x1[j] = j == 0 ? 1u : 0u;
         x2[j] = 0u;
     }
-    const uint32_t* res = x1;
+    bool first = true;
     for (;;) {
         while (!(u[0] & 1u)) {
             limbs_shr1(u);
@@ -660,12 +660,9 @@ ZK_HD Fe<C> fe_inv(const Fe<C>& a) {
             limbs_shr1(v);
             limbs_half_mod<C>(x2);
         }
-        if (limbs_is_one(u)) {
-            res = x1;
-            break;
-        }
+        if (limbs_is_one(u)) break;
         if (limbs_is_one(v)) {
-            res = x2;
+            first = false;
             break;
         }
         if (limbs_geq(u, v)) {
@@ -679,7 +676,7 @@ ZK_HD Fe<C> fe_inv(const Fe<C>& a) {
     Fe<C> x, r3;
 #pragma unroll
     for (int j = 0; j < 8; j++) {
-        x.v[j] = res[j];
+        x.v[j] = first ? x1[j] : x2[j];
         r3.v[j] = C::R3(j);
     }
     return fe_mul<C>(x, r3);

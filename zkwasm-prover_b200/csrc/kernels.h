@@ -186,6 +186,7 @@ cudaError_t batch_inverse(Fr* out, const Fr* in, const Fr* c, uint32_t n, int ac
 cudaError_t div_by_point_diffs(Fr* values, const Fr* omegas, const Fr* points, int np, uint32_t n, Fr* scratch,
                                size_t scratch_elems, cudaStream_t s);
 size_t fr_scan_tmp_elems(uint32_t n);
+uint32_t fr_scan_timeouts();
 cudaError_t fr_scan_excl(Fr* out, const Fr* in, uint32_t n, const Fr* init, int op, Fr* tmp, cudaStream_t s);
 cudaError_t logup_z_scan(Fr* z, Fr* last_z, int last_index, uint32_t n, Fr* tmp, cudaStream_t s);
 cudaError_t logup_z_compose(Fr* z, const Fr* sum, const Fr* table, const Fr* m, const Fr* beta, Fr* last_z,

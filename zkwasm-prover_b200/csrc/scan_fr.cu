@@ -239,37 +239,6 @@ cudaError_t div_by_point_diffs(Fr* values, const Fr* omegas, const Fr* points, i
 }
 
 // ------------------------------------------------------------ exclusive scan
-// Phase 1: block-local exclusive scan written to out, block totals to tmp.
-// Phase 2: exclusive scan of block totals (recursive) with the initial value.
-// Phase 3: out[i] = prefix(block) op out[i].
-
-__global__ void __launch_bounds__(ST) scan_local_kernel(Fr* out, const Fr* in, uint32_t n, int op, Fr* btot) {
-    __shared__ Fr wsm[32];
-    const size_t base = (size_t)blockIdx.x * SBLK + (size_t)threadIdx.x * SK;
-    Fr v[SK];
-    Fr run = op_ident(op);
-#pragma unroll
-    for (int k = 0; k < SK; k++) {
-        Fr a = (base + k < n) ? ld_elem<FrCfg>(in + base + k) : op_ident(op);
-        v[k] = run;  // exclusive within the thread
-        run = op_apply(op, run, a);
-    }
-    Fr tot;
-    Fr e = block_excl_scan_fr(op, run, wsm, tot);
-#pragma unroll
-    for (int k = 0; k < SK; k++)
-        if (base + k < n) st_elem<FrCfg>(out + base + k, op_apply(op, e, v[k]));
-    if (threadIdx.x == 0) st_elem<FrCfg>(btot + blockIdx.x, tot);
-}
-
-__global__ void __launch_bounds__(ST) scan_apply_kernel(Fr* out, uint32_t n, int op, const Fr* bpre) {
-    const Fr p = ld_elem<FrCfg>(bpre + blockIdx.x);
-    const size_t base = (size_t)blockIdx.x * SBLK;
-    for (int k = threadIdx.x; k < SBLK; k += ST) {
-        const size_t i = base + k;
-        if (i < n) st_elem<FrCfg>(out + i, op_apply(op, p, ld_elem<FrCfg>(out + i)));
-    }
-}
 
 // single block: exclusive scan of m <= SBLK values with init, in place; optional total
 __global__ void __launch_bounds__(ST) scan_small_kernel(Fr* x, uint32_t m, int op, const Fr* init) {
@@ -292,20 +261,205 @@ __global__ void __launch_bounds__(ST) scan_small_kernel(Fr* x, uint32_t m, int o
         if (base + k < m) st_elem<FrCfg>(x + base + k, op_apply(op, e, v[k]));
 }
 
+// ------------------------------------------------------------ single-pass scan
+// One launch over tiles of SBLK elements (decoupled look-back).  A block takes
+// the next tile number from an atomic ticket, so every tile it waits on
+// belongs to a block that started before it and is running; it scans its tile
+// locally, publishes the tile's aggregate (state 1), then one warp looks back
+// over the preceding tiles 32 at a time, combining aggregates until it meets a
+// published inclusive prefix (state 2), and publishes its own inclusive
+// prefix.  The elements are read once and written once.  The prefix product
+// uses it: there the two products per element hide the waits.  The prefix
+// sum, bound by HBM, runs as reduce-then-scan (further below).
+//
+// Every wait polls at most SCAN_POLL_LIMIT times.  A wait that runs out adds
+// one to the device counter g_scan_timeouts (zkp_scan_timeouts reads it), takes
+// the missing tile as the identity and carries on, so a launch always ends.
+
+static constexpr uint32_t SCAN_POLL_LIMIT = 1u << 22;
+__device__ uint32_t g_scan_timeouts;
+
+struct ScanTiles {
+    uint32_t* words;  // [0] the ticket, [1 .. 1 + nb) tile states
+    Fr* agg;          // nb tile aggregates
+    Fr* incl;         // nb inclusive prefixes
+};
+
+__device__ __forceinline__ uint32_t ld_acquire_u32(const uint32_t* p) {
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_u32(uint32_t* p, uint32_t v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+// a value another block published: read past L1
+__device__ __forceinline__ Fr ldcg_fr(const Fr* p) {
+    const uint4* q = reinterpret_cast<const uint4*>(p);
+    const uint4 a = __ldcg(q), b = __ldcg(q + 1);
+    Fr r;
+    r.v[0] = a.x; r.v[1] = a.y; r.v[2] = a.z; r.v[3] = a.w;
+    r.v[4] = b.x; r.v[5] = b.y; r.v[6] = b.z; r.v[7] = b.w;
+    return r;
+}
+__device__ __forceinline__ Fr shfl_xor_fr(const Fr& v, int m) {
+    Fr r;
+#pragma unroll
+    for (int j = 0; j < 8; j++) r.v[j] = __shfl_xor_sync(0xffffffffu, v.v[j], m);
+    return r;
+}
+
+// The tile passes through shared memory (swizzled 32-byte slots, sm_slot) so
+// that global loads and stores are coalesced 16-byte accesses while each
+// thread scans SK consecutive elements.
+static constexpr size_t SCAN_TILE_SMEM = (size_t)SBLK * sizeof(Fr);
+
+// LOOKBACK false: the tiles' exclusive prefixes are given in tiles.agg (the
+// reduce-then-scan form below) and no block waits on another.
+// OPK: OP_ADD or OP_MUL, fixed at compile time (the sum's kernel carries no
+// product code).
+template <bool LOOKBACK, int OPK>
+__global__ void __launch_bounds__(ST, LOOKBACK ? 2 : 3) scan_onepass_kernel(Fr* out, const Fr* in, uint32_t n, const Fr* init,
+                                                          ScanTiles tiles) {
+    constexpr int op = OPK;
+    __shared__ Fr wsm[32];
+    __shared__ uint32_t s_tile;
+    __shared__ Fr s_prefix;
+    extern __shared__ uint4 smem_u4[];
+    Fr* sm = reinterpret_cast<Fr*>(smem_u4);
+    if (threadIdx.x == 0) s_tile = LOOKBACK ? atomicAdd(tiles.words, 1u) : blockIdx.x;
+    __syncthreads();
+    const uint32_t tile = s_tile;
+    const size_t t0 = (size_t)tile * SBLK;
+    const uint32_t cnt = n - t0 < (size_t)SBLK ? (uint32_t)(n - t0) : (uint32_t)SBLK;
+    {
+        const Fr id = op_ident(op);
+        const uint4* src = reinterpret_cast<const uint4*>(in + t0);
+        for (uint32_t c = threadIdx.x; c < 2u * SBLK; c += ST) {
+            const uint32_t e = c >> 1, h = c & 1;
+            *sm_slot(sm, e, h) = e < cnt ? src[c]
+                                         : (h ? make_uint4(id.v[4], id.v[5], id.v[6], id.v[7])
+                                              : make_uint4(id.v[0], id.v[1], id.v[2], id.v[3]));
+        }
+    }
+    __syncthreads();
+    const uint32_t lbase = threadIdx.x * SK;
+    Fr v[SK];
+    Fr run = op_ident(op);
+#pragma unroll
+    for (int k = 0; k < SK; k++) {
+        const Fr a = sm_ld(sm, lbase + k);
+        v[k] = run;
+        run = op_apply(op, run, a);
+    }
+    Fr tot;
+    const Fr e = block_excl_scan_fr(op, run, wsm, tot);
+    uint32_t* state = tiles.words + 1;
+    if (!LOOKBACK) {
+        if (threadIdx.x == 0) s_prefix = ld_elem<FrCfg>(tiles.agg + tile);
+    } else if (threadIdx.x < 32) {
+        const int lane = threadIdx.x;
+        Fr prefix = op_ident(op);
+        if (tile == 0) {
+            if (init) prefix = ld_elem<FrCfg>(init);
+        } else {
+            if (lane == 0) {
+                st_elem<FrCfg>(tiles.agg + tile, tot);
+                st_release_u32(state + tile, 1u);
+            }
+            // window of the 32 tiles p, p - 1, ..., p - 31 (lane order)
+            int64_t p = (int64_t)tile - 1;
+            for (;;) {
+                const int64_t idx = p - lane;
+                uint32_t f = 2;  // before tile 0: never reached, tile 0 is inclusive
+                Fr val = op_ident(op);
+                if (idx >= 0) {
+                    f = ld_acquire_u32(state + idx);
+                    uint32_t polls = 0;
+                    while (f == 0 && ++polls < SCAN_POLL_LIMIT) {
+                        __nanosleep(64);
+                        f = ld_acquire_u32(state + idx);
+                    }
+                    if (f == 0) {
+                        atomicAdd(&g_scan_timeouts, 1u);
+                        f = 1;
+                    } else {
+                        val = ldcg_fr(f == 2 ? tiles.incl + idx : tiles.agg + idx);
+                    }
+                }
+                // the nearest inclusive prefix ends the walk: lanes up to it count
+                const unsigned incl_mask = __ballot_sync(0xffffffffu, f == 2);
+                const int last = incl_mask ? __ffs(incl_mask) - 1 : 31;
+                Fr c = lane <= last ? val : op_ident(op);
+#pragma unroll
+                for (int m = 16; m > 0; m >>= 1) c = op_apply(op, c, shfl_xor_fr(c, m));
+                prefix = op_apply(op, c, prefix);
+                if (incl_mask) break;
+                p -= 32;
+            }
+        }
+        if (lane == 0) {
+            st_elem<FrCfg>(tiles.incl + tile, op_apply(op, prefix, tot));
+            st_release_u32(state + tile, 2u);
+            s_prefix = prefix;
+        }
+    }
+    __syncthreads();
+    const Fr pre = op_apply(op, s_prefix, e);
+#pragma unroll
+    for (int k = 0; k < SK; k++) sm_st(sm, lbase + k, op_apply(op, pre, v[k]));
+    __syncthreads();
+    uint4* dst = reinterpret_cast<uint4*>(out + t0);
+    for (uint32_t c = threadIdx.x; c < 2u * cnt; c += ST) dst[c] = *sm_slot(sm, c >> 1, c & 1);
+}
+
+// Reduce-then-scan, for the sum (bound by HBM, where the look-back's waits
+// cost more than they save): (1) every tile's sum, read with coalesced loads
+// and no shared tile; (2) their exclusive scan with the initial value, one
+// block (or this routine again above 2048 tiles); (3) every tile scanned from
+// its prefix.  Three reads and one write of the elements' bytes against the
+// one-pass form's read and write, but no block ever waits on another.
+__global__ void __launch_bounds__(ST) tile_sum_kernel(const Fr* in, uint32_t n, Fr* agg) {
+    __shared__ Fr wsm[32];
+    const size_t t0 = (size_t)blockIdx.x * SBLK;
+    Fr acc = fe_zero<FrCfg>();
+#pragma unroll
+    for (int k = 0; k < SK; k++) {
+        const size_t i = t0 + threadIdx.x + (size_t)ST * k;
+        if (i < n) acc = fe_add<FrCfg>(acc, ld_elem<FrCfg>(in + i));
+    }
+#pragma unroll
+    for (int m = 16; m > 0; m >>= 1) acc = fe_add<FrCfg>(acc, shfl_xor_fr(acc, m));
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) wsm[wid] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        Fr tot = wsm[0];
+        for (int w = 1; w < ST / 32; w++) tot = fe_add<FrCfg>(tot, wsm[w]);
+        st_elem<FrCfg>(agg + blockIdx.x, tot);
+    }
+}
+
+// tile states after the aggregates and prefixes, in Fr elements
+static size_t onepass_elems(uint32_t nb) { return 2 * (size_t)nb + ((size_t)nb + 1 + 7) / 8; }
+
 // scratch of the scans, also enough for the three-phase batch inversion
 // (the callers below use it for both, one after the other)
 size_t fr_scan_tmp_elems(uint32_t n) {
-    size_t t = 0;
-    uint32_t m = n;
-    while (m > (uint32_t)SBLK) {
-        m = (m + SBLK - 1) / SBLK;
-        t += m;
-    }
+    const uint32_t nb = (n + SBLK - 1) / SBLK;
+    const size_t one = n > (uint32_t)SBLK ? onepass_elems(nb) : 1;
     const size_t inv = batch_inv_scratch_elems(n);
-    return (t + 1 > inv ? t + 1 : inv);
+    return one > inv ? one : inv;
 }
 
-// out[i] = init op x_0 op ... op x_{i-1}; out may alias in
+uint32_t fr_scan_timeouts() {
+    uint32_t v = 0;
+    if (cudaMemcpyFromSymbol(&v, g_scan_timeouts, sizeof(v)) != cudaSuccess) return 0xffffffffu;
+    return v;
+}
+
+// out[i] = init op x_0 op ... op x_{i-1}; out may alias in (each tile is read
+// whole before it is written, and no block reads another's elements)
 cudaError_t fr_scan_excl(Fr* out, const Fr* in, uint32_t n, const Fr* init, int op, Fr* tmp, cudaStream_t s) {
     if (n == 0) return cudaSuccess;
     if (n <= (uint32_t)SBLK) {
@@ -313,12 +467,26 @@ cudaError_t fr_scan_excl(Fr* out, const Fr* in, uint32_t n, const Fr* init, int 
         scan_small_kernel<<<1, ST, 0, s>>>(out, n, op, init);
         return cudaGetLastError();
     }
+    if (!tmp) return cudaErrorInvalidValue;
     const uint32_t nb = (n + SBLK - 1) / SBLK;
-    Fr* btot = tmp;
-    scan_local_kernel<<<nb, ST, 0, s>>>(out, in, n, op, btot);
-    ZK_CHECK(cudaGetLastError());
-    ZK_CHECK(fr_scan_excl(btot, btot, nb, init, op, tmp + nb, s));
-    scan_apply_kernel<<<nb, ST, 0, s>>>(out, n, op, btot);
+    ScanTiles tiles;
+    tiles.agg = tmp;
+    tiles.incl = tmp + nb;
+    tiles.words = reinterpret_cast<uint32_t*>(tmp + 2 * (size_t)nb);
+    if (op == OP_ADD) {
+        static SmemOptIn opt_p;
+        ZK_CHECK(opt_p.ensure(scan_onepass_kernel<false, OP_ADD>, (int)SCAN_TILE_SMEM));
+        tile_sum_kernel<<<nb, ST, 0, s>>>(in, n, tiles.agg);
+        ZK_CHECK(cudaGetLastError());
+        ZK_CHECK(fr_scan_excl(tiles.agg, tiles.agg, nb, init, op, tmp + nb, s));
+        scan_onepass_kernel<false, OP_ADD><<<nb, ST, SCAN_TILE_SMEM, s>>>(out, in, n, nullptr, tiles);
+        return cudaGetLastError();
+    }
+    if (op != OP_MUL) return cudaErrorInvalidValue;
+    static SmemOptIn opt;
+    ZK_CHECK(opt.ensure(scan_onepass_kernel<true, OP_MUL>, (int)SCAN_TILE_SMEM));
+    ZK_CHECK(cudaMemsetAsync(tiles.words, 0, ((size_t)nb + 1) * sizeof(uint32_t), s));
+    scan_onepass_kernel<true, OP_MUL><<<nb, ST, SCAN_TILE_SMEM, s>>>(out, in, n, init, tiles);
     return cudaGetLastError();
 }
 
