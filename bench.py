@@ -986,11 +986,9 @@ def run_ours(args):
         prod_rate = mont_rate if args.montgomery_tables else shoup_rate
         sb, sm = ph.stage_bytes()[dom], ph.stage_mults()[dom]
         achieved = sb / (stage_ms[dom] / 1e3) / 1e9
+        # no capture of the extend kernels' DRAM bytes matches their current
+        # block order (column-fastest), so none is reported
         traffic = None
-        prof = os.path.join(ROOT, "profiles", "ntt_pass_traffic.json")
-        if os.path.exists(prof):
-            with open(prof) as f:
-                traffic = json.load(f).get("stage_traffic_bytes", [None] * 4)[dom]
         cpu = cpu_baseline_port(args.log_n, args.ext_bits) if extras and not args.no_cpu_baseline else None
         do_msm = extras and not args.no_msm
         do_rows = extras and not args.no_rows
@@ -1481,7 +1479,7 @@ def run_pipeline(args):
             "library_calls_per_proof": calls_per_proof,
             "roofline": {
                 "bound": "hbm", "achieved": round(achieved, 2), "peak": peak_hbm, "unit": "GB/s",
-                "frac": round(achieved / peak_hbm, 4), "traffic": args.ntt_traffic,
+                "frac": round(achieved / peak_hbm, 4), "traffic": coset_traffic(cols_per, shape.k),
                 "kernel": "ntt_pass_kernel via zkp_ntt_batch_twisted (coset transforms of the quotient)",
                 "launch_groups": groups, "avg_group_ms": round(avg_ms, 4), "columns_per_group": cols_per,
                 "peak_kind": peak_kind, "note": "integer-pipe bound: see roofline_int"},
@@ -1516,6 +1514,27 @@ KERNELS_PER_CALL = {"zkp_msm_batch_table": 14, "zkp_ntt_batch_twisted": 2, "zkp_
                     "zkp_poly_eval_batch": 2}
 NO_KERNEL = {"zkp_msm_batch_table_scratch_bytes", "zkp_scan_scratch_elems", "zkp_poly_divide_scratch_elems",
              "zkp_poly_eval_batch_scratch_elems", "zkp_msm_batch_table_default_window"}
+
+
+def coset_traffic(columns, log_n):
+    """DRAM bytes of one coset-transform launch group of `columns` columns of
+    2^log_n, from the committed ncu capture (profiles/coset_ntt_traffic.json,
+    per column), or None for another size or when ntt.cu no longer hashes to
+    the captured source (a stale figure is not reported)."""
+    import hashlib
+
+    prof = os.path.join(ROOT, "profiles", "coset_ntt_traffic.json")
+    src = os.path.join(ROOT, "zkwasm-prover_b200", "csrc", "ntt.cu")
+    if not (os.path.exists(prof) and os.path.exists(src)):
+        return None
+    with open(prof) as f:
+        d = json.load(f)
+    if d.get("log_n") != log_n:
+        return None
+    with open(src, "rb") as f:
+        if hashlib.sha256(f.read()).hexdigest() != d.get("source_sha256"):
+            return None
+    return round(d["bytes_per_column"] * columns)
 
 
 def _launch_count(calls, shape):
@@ -1666,7 +1685,6 @@ def main():
     ap.add_argument("--k", type=int, default=None)
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-schedule comparison")
     ap.add_argument("--no-extras", action="store_true", help="skip the k = 20 GWC proof and the NTT phase companions")
-    ap.add_argument("--ntt-traffic", type=float, default=None, help=argparse.SUPPRESS)
     ap.add_argument("--profile-range", action="store_true",
                     help="bracket the timed proofs with cudaProfilerStart/Stop (for ncu --profile-from-start off)")
     args = ap.parse_args()
