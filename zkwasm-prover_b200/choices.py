@@ -196,6 +196,15 @@ class ChoiceModel:
         X = np.array([encode(self.name, record, c) for c in cands], np.float32)
         return cands[int(np.argmin(self.m.predict(X)))]
 
+    def pick_many(self, records, cands):
+        """pick() for many records over the same candidates, in one forward
+        pass of the model."""
+        if not records:
+            return []
+        X = np.array([encode(self.name, r, c) for r in records for c in cands], np.float32)
+        y = self.m.predict(X).reshape(len(records), len(cands))
+        return [cands[int(i)] for i in np.argmin(y, axis=1)]
+
 
 def default_pick(name: str, record):
     """The library's fixed rule for the choice."""

@@ -82,10 +82,19 @@ def limbs(x: int, mont=True) -> list:
     return [(v >> (64 * i)) & 0xFFFFFFFFFFFFFFFF for i in range(4)]
 
 
+def _to_device(h: torch.Tensor, device) -> torch.Tensor:
+    """Host tensor -> device through pinned memory, without waiting for the
+    work queued on the stream (a pageable copy would; the caching host
+    allocator keeps the pinned block until the copy has run)."""
+    if torch.device(device).type != "cuda":
+        return h.to(device)
+    return h.pin_memory().to(device, non_blocking=True)
+
+
 def fr_tensor(xs, device="cuda") -> torch.Tensor:
     """Python ints -> (len, 4) int64 Montgomery-form tensor."""
     a = np.array([limbs(int(x)) for x in xs], dtype=np.uint64).reshape(-1, 4)
-    return torch.from_numpy(a.view(np.int64)).to(device)
+    return _to_device(torch.from_numpy(a.view(np.int64)), device)
 
 
 def fr_ints(t: torch.Tensor) -> list:
@@ -233,7 +242,7 @@ def field_op(res, l, r, op, n, l_c=None, r_c=None, l_rot=0, r_rot=0, sym=None, s
 
 
 def ptr_array(ptrs, device="cuda") -> torch.Tensor:
-    return torch.tensor([int(p) for p in ptrs], dtype=torch.int64, device=device)
+    return _to_device(torch.tensor([int(p) for p in ptrs], dtype=torch.int64), device)
 
 
 def omega_table(sym, w: int, log_n: int, may_bit_reversed: int) -> torch.Tensor:
@@ -472,15 +481,27 @@ class HostStage:
         self.host, self.dev, self.group = host_advice, dev_advice, group
         self.stream = torch.cuda.Stream()
         self.events = []
+        ngroups = -(-host_advice.shape[0] // group)
+        self.h_dev = torch.zeros((ngroups, 8), dtype=torch.int32, device="cuda")
+        self.h_host = torch.zeros((ngroups, 8), dtype=torch.int32, pin_memory=True)
 
-    def start(self):
+    def start(self, histograms: bool = False):
+        """Queues every group's copy; with histograms, also the scalar
+        histogram of each group's first column right behind its copy (the
+        learned MSM choice reads it without waiting for the compute stream)."""
         # the copies overwrite the columns: order them after the work already queued
         self.stream.wait_stream(torch.cuda.current_stream())
         self.events = []
         with torch.cuda.stream(self.stream):
-            for g0 in range(0, self.host.shape[0], self.group):
+            for gi, g0 in enumerate(range(0, self.host.shape[0], self.group)):
                 g1 = min(self.host.shape[0], g0 + self.group)
                 self.dev[g0:g1].copy_(self.host[g0:g1], non_blocking=True)
+                if histograms:
+                    self.h_dev[gi].zero_()
+                    abi.check(lib().zkp_scalar_histogram(self.dev[g0].data_ptr(), self.dev.shape[1],
+                                                         self.h_dev[gi].data_ptr(), _st(self.stream)),
+                              "zkp_scalar_histogram")
+                    self.h_host[gi].copy_(self.h_dev[gi], non_blocking=True)
                 ev = torch.cuda.Event()
                 ev.record(self.stream)
                 self.events.append((g0, g1, ev))
@@ -489,6 +510,13 @@ class HostStage:
         for g0, g1, ev in self.events:
             if g0 < hi and g1 > lo:
                 torch.cuda.current_stream().wait_event(ev)
+
+    def histogram(self, gi: int) -> list:
+        """The histogram features of group gi's first column: waits for that
+        group's copy only."""
+        self.events[gi][2].synchronize()
+        v = self.h_host[gi].numpy()[:7].astype(np.float64)
+        return list(v / max(1.0, v.sum()))
 
 
 # ---------------------------------------------------------------- host-side steps
@@ -782,28 +810,49 @@ class HotPath:
             return []
         table = self.table_gl if lagrange else self.table_g
         bases = self.g_lagrange if lagrange else self.g
-        outs = []
         # pipelines of MSM_BATCH MSMs: at 2^22 over the c = 19 table, 8 a
         # pipeline run at 13.05 ms an MSM against 13.64 for 16 and 14.21 for 32
-        for i in range(0, len(cols), MSM_BATCH):
-            part = cols[i:i + MSM_BATCH]
-            outs.append(self._msm_part(table, bases, part))
+        parts = [cols[i:i + MSM_BATCH] for i in range(0, len(cols), MSM_BATCH)]
+        # every pipeline's schedule choice before the first launch: the
+        # histograms and the model run once for the whole call, so the
+        # pipelines queue back to back with no host round trip between them
+        picks = self._msm_picks(parts)
+        outs = [self._msm_part(table, bases, part, pick) for part, pick in zip(parts, picks)]
         torch.cuda.synchronize()
         return jac_to_affine(torch.cat(outs).cpu().numpy().view(np.uint64))
 
-    def _msm_part(self, table, bases, part):
-        """One MSM pipeline: over the SRS table, or over the plain bases with
-        learned windows when the learned table-or-plain choice says that runs
-        faster for this batch's size, count and scalar distribution."""
+    def _msm_picks(self, parts, hists=None):
+        """For each pipeline: None (over the SRS table) or the scalar
+        histogram features (over the plain bases, with a learned window), as
+        the learned table-or-plain choice predicts faster for the pipeline's
+        size, count and scalar distribution.  hists: the features when the
+        caller has them (then the model runs on a side stream, so reading its
+        answer does not wait for the work queued on the compute stream)."""
+        if not self.learned:
+            return [None] * len(parts)
+        from . import schedule as S
+
+        recs = lambda hs: [{"n": self.n, "batch": len(p), "hist": h} for p, h in zip(parts, hs)]
+        if hists is None:
+            hists = S.histograms([p[0] for p in parts])
+            table = self._choice_msm.pick_many(recs(hists), [0, 1])
+        else:
+            if getattr(self, "_pick_stream", None) is None:
+                self._pick_stream = torch.cuda.Stream()
+            with torch.cuda.stream(self._pick_stream):
+                table = self._choice_msm.pick_many(recs(hists), [0, 1])
+        return [None if t == 1 else h for t, h in zip(table, hists)]
+
+    def _msm_part(self, table, bases, part, pick=None):
+        """One MSM pipeline: over the SRS table (pick None), or over the plain
+        bases with the learned window for the histogram features `pick`."""
         n = self.n
         ns = [n] * len(part)
         if self.learned:
             from . import schedule as S
 
-            hist = S.histogram(part[0])
-            shape = {"n": n, "batch": len(part), "hist": hist}
-            if self._choice_msm.pick(shape, [0, 1]) == 0:
-                feats = S.shape_features(n, len(part), hist)
+            if pick is not None:
+                feats = S.shape_features(n, len(part), pick)
                 c = self._window_model.pick(feats)
                 ws = [c] * len(part)
                 na = (ctypes.c_uint32 * len(part))(*ns)
@@ -889,13 +938,14 @@ class HotPath:
             # of its columns with the MSMs of earlier ones the same way)
             self.adv_coeff = self._ws("adv_coeff", tuple(c.advice.shape))
             self.inst_coeff = self._ws("inst_coeff", tuple(c.instance.shape))
-            stage.start()
+            stage.start(histograms=self.learned)
             outs = []
-            for a0 in range(0, s.advice, MSM_BATCH):
+            for gi, a0 in enumerate(range(0, s.advice, MSM_BATCH)):
                 a1 = min(s.advice, a0 + MSM_BATCH)
                 stage.wait(a0, a1)
                 part = adv[a0:a1] + (inst if a1 == s.advice else [])
-                outs.append(self._msm_part(self.table_gl, self.g_lagrange, part))
+                pick = self._msm_picks([part], [stage.histogram(gi)])[0] if self.learned else None
+                outs.append(self._msm_part(self.table_gl, self.g_lagrange, part, pick))
                 ntt_into(self.adv_coeff[a0:a1], c.advice[a0:a1], self.tab_n, a1 - a0, True,
                          tmp=self._wsd["ntt_tmp"])
             ntt_into(self.inst_coeff, c.instance, self.tab_n, 1, True)

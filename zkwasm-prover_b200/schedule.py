@@ -77,12 +77,18 @@ def scalars(n: int, mix: str, seed: int, device="cuda") -> torch.Tensor:
 
 
 def histogram(s: torch.Tensor) -> list:
-    h = torch.zeros(8, dtype=torch.int32, device=s.device)
-    abi.check(lib().zkp_scalar_histogram(s.data_ptr(), s.shape[0], h.data_ptr(), H.stream_handle()),
-              "zkp_scalar_histogram")
-    torch.cuda.synchronize()
-    v = h.cpu().numpy()[:7].astype(np.float64)
-    return list(v / max(1.0, v.sum()))
+    return histograms([s])[0]
+
+
+def histograms(cols) -> list:
+    """The scalar-distribution features of each column: every histogram is
+    launched first and all are read back with one synchronisation."""
+    h = torch.zeros((len(cols), 8), dtype=torch.int32, device="cuda")
+    for i, s in enumerate(cols):
+        abi.check(lib().zkp_scalar_histogram(s.data_ptr(), s.shape[0], h[i].data_ptr(), H.stream_handle()),
+                  "zkp_scalar_histogram")
+    v = h.cpu().numpy()[:, :7].astype(np.float64)
+    return [list(r / max(1.0, r.sum())) for r in v]
 
 
 # largest batch the model is trained on; larger batches are presented as this
