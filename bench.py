@@ -781,6 +781,52 @@ def run_coset_ntt(args):
                       "peak_kind": kind, "steps": args.steps}))
 
 
+def run_timeline(args):
+    """One proof of the headline workload under CUPTI activity tracing
+    (torch.profiler): the device's busy and idle time over the proof, the
+    longest idle gaps and every kernel's launches and device time, warm and
+    unserialised (ncu's launch list replays each kernel cold)."""
+    from torch.profiler import ProfilerActivity, profile
+
+    torch.cuda.set_device(0)
+    zkp = importlib.import_module("zkwasm-prover_b200")
+    zkp.load_library()
+    P = _prover()
+    hp = P.HotPath(P.Circuit(_shape(P, args), seed=PIPE_SEED), "batched")
+    hp.prove()
+    torch.cuda.synchronize()
+    with profile(activities=[ProfilerActivity.CUDA]) as prof:
+        t0 = time.perf_counter()
+        hp.prove()
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+    iv = sorted((e.time_range.start, e.time_range.end, e.name) for e in prof.events()
+                if e.device_type == torch.autograd.DeviceType.CUDA)
+    busy, gaps, cur = 0.0, [], None
+    for s_, e_, name in iv:
+        if cur is None:
+            cur = [s_, e_]
+        elif s_ > cur[1]:
+            busy += cur[1] - cur[0]
+            gaps.append((s_ - cur[1], name))
+            cur = [s_, e_]
+        else:
+            cur[1] = max(cur[1], e_)
+    busy += cur[1] - cur[0]
+    tot = {}
+    for s_, e_, name in iv:
+        a = tot.setdefault(name.split("(")[0], [0, 0.0])
+        a[0] += 1
+        a[1] += e_ - s_
+    gaps.sort(reverse=True)
+    print(json.dumps({"metric": f"k={args.k} proof device timeline (CUPTI)", "wall_s": round(wall, 4),
+                      "span_ms": round((iv[-1][1] - iv[0][0]) / 1e3, 2), "busy_ms": round(busy / 1e3, 2),
+                      "phases_s": {k_: round(v, 4) for k_, v in hp.phase_s.items()},
+                      "longest_gaps_us": [(round(g), nm.split("(")[0]) for g, nm in gaps[:10]],
+                      "kernels": [(k_, n_, round(t_ / 1e3, 2), round(100 * t_ / busy, 1))
+                                  for k_, (n_, t_) in sorted(tot.items(), key=lambda x: -x[1][1])]}))
+
+
 def run_msm_uneven(args):
     torch.cuda.set_device(0)
     zkp = importlib.import_module("zkwasm-prover_b200")
@@ -1677,6 +1723,8 @@ def main():
                     help="time only the per-row kernels (with --impl reference: the reference's kernels)")
     ap.add_argument("--ntt-phase", action="store_true",
                     help="the batched NTT phase as the headline (64 columns of 2^20 -> 2^23)")
+    ap.add_argument("--timeline", action="store_true",
+                    help="one proof under CUPTI tracing: device busy time and per-kernel device time")
     ap.add_argument("--coset-ntt", action="store_true",
                     help="time only the quotient's coset transform (--cols columns of 2^--k)")
     ap.add_argument("--cols", type=int, default=8)
@@ -1702,6 +1750,8 @@ def main():
         run_msm_uneven(args)
     elif args.coset_ntt:
         run_coset_ntt(args)
+    elif args.timeline:
+        run_timeline(args)
     elif args.ntt_phase:
         run_ours(args)
     else:
