@@ -795,11 +795,22 @@ def run_timeline(args):
     hp = P.HotPath(P.Circuit(_shape(P, args), seed=PIPE_SEED), "batched")
     hp.prove()
     torch.cuda.synchronize()
+    # the host's garbage-collection pauses during the traced proof
+    gc_pauses, gc_t0 = [], [0.0]
+
+    def on_gc(phase, info):
+        if phase == "start":
+            gc_t0[0] = time.perf_counter()
+        else:
+            gc_pauses.append((time.perf_counter() - gc_t0[0], info.get("generation")))
+
+    gc.callbacks.append(on_gc)
     with profile(activities=[ProfilerActivity.CUDA]) as prof:
         t0 = time.perf_counter()
         hp.prove()
         torch.cuda.synchronize()
         wall = time.perf_counter() - t0
+    gc.callbacks.remove(on_gc)
     iv = sorted((e.time_range.start, e.time_range.end, e.name) for e in prof.events()
                 if e.device_type == torch.autograd.DeviceType.CUDA)
     busy, gaps, cur = 0.0, [], None
@@ -823,6 +834,9 @@ def run_timeline(args):
                       "span_ms": round((iv[-1][1] - iv[0][0]) / 1e3, 2), "busy_ms": round(busy / 1e3, 2),
                       "phases_s": {k_: round(v, 4) for k_, v in hp.phase_s.items()},
                       "longest_gaps_us": [(round(g), nm.split("(")[0]) for g, nm in gaps[:10]],
+                      "host_gc_pauses": {"count": len(gc_pauses),
+                                         "total_ms": round(1e3 * sum(p for p, _ in gc_pauses), 2),
+                                         "longest_ms": round(1e3 * max([p for p, _ in gc_pauses] or [0]), 2)},
                       "kernels": [(k_, n_, round(t_ / 1e3, 2), round(100 * t_ / busy, 1))
                                   for k_, (n_, t_) in sorted(tot.items(), key=lambda x: -x[1][1])]}))
 

@@ -883,9 +883,15 @@ class HotPath:
             tmp = H.empty_fr(self.n)
             for c in cols:
                 ntt_raw(self.sym, c, tmp, self.tab_n, True, self.tab_n.n_inv)
-        else:
-            for c in cols:
-                ntt_cols(c, self.tab_n, 1, True)
+        elif cols:
+            st = _stacked(cols)
+            if st.data_ptr() == cols[0].data_ptr() and len(cols) <= NTT_CHUNK and "ntt_tmp" in self._wsd:
+                # consecutive rows of one workspace: one batched launch group
+                tmp = self._wsd["ntt_tmp"][:len(cols) * self.n].view(st.shape)
+                ntt_cols(st, self.tab_n, len(cols), True, tmp=tmp)
+            else:
+                for c in cols:
+                    ntt_cols(c, self.tab_n, 1, True)
 
     def counts(self):
         """Work units of one proof in this schedule: MSMs of n points, NTTs of
@@ -904,7 +910,24 @@ class HotPath:
         """Runs phases 1-6; returns the proof stand-in: every commitment
         (affine ints) and evaluation, in transcript order.  stage: a
         HostStage bringing the advice columns in from host memory during
-        phase 1 (batched schedule)."""
+        phase 1 (batched schedule).
+
+        Python's automatic garbage collection is paused while the proof runs
+        (reference counting still frees its objects; any left in cycles wait
+        for the first collection after it): a full collection, tens of ms
+        with the proving key's objects alive, landing at a phase boundary,
+        where the device waits for the host, stalled the device."""
+        import gc
+
+        enabled = gc.isenabled()
+        gc.disable()
+        try:
+            return self._prove(stage)
+        finally:
+            if enabled:
+                gc.enable()
+
+    def _prove(self, stage):
         s, c, n, u = self.shape, self.c, self.n, self.u
         tr = Transcript(self.seed)
         proof = {"commitments": [], "evals": []}
