@@ -349,8 +349,9 @@ size_t zkp_scan_scratch_elems(uint32_t n);
 /* Exclusive prefix product / sum with carried-in value (init may be NULL):
  * out[i] = init (op) in[0] (op) ... (op) in[i-1]; out may alias in.  Above
  * 2048 elements the product runs in one launch (decoupled look-back over
- * tiles of 2048 elements) and the sum as tile sums, their scan and a scan of
- * each tile from its prefix (launches that never wait on one another). */
+ * tiles of 2048 elements) and the sum as the sums of 256-element segments,
+ * their scan and a scan of each segment from its prefix, one warp a segment
+ * (launches that never wait on one another). */
 cudaError_t zkp_grand_product(void *out, const void *in, uint32_t n, const void *init, void *scratch,
                               cudaStream_t stream);
 cudaError_t zkp_grand_sum(void *out, const void *in, uint32_t n, const void *init, void *scratch,

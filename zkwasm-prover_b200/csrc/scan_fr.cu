@@ -314,20 +314,18 @@ __device__ __forceinline__ Fr shfl_xor_fr(const Fr& v, int m) {
 // thread scans SK consecutive elements.
 static constexpr size_t SCAN_TILE_SMEM = (size_t)SBLK * sizeof(Fr);
 
-// LOOKBACK false: the tiles' exclusive prefixes are given in tiles.agg (the
-// reduce-then-scan form below) and no block waits on another.
-// OPK: OP_ADD or OP_MUL, fixed at compile time (the sum's kernel carries no
-// product code).
-template <bool LOOKBACK, int OPK>
-__global__ void __launch_bounds__(ST, LOOKBACK ? 2 : 3) scan_onepass_kernel(Fr* out, const Fr* in, uint32_t n, const Fr* init,
-                                                          ScanTiles tiles) {
+// OPK: the operation, fixed at compile time (OP_MUL: the sum uses the
+// reduce-then-scan form below).
+template <int OPK>
+__global__ void __launch_bounds__(ST, 2) scan_onepass_kernel(Fr* out, const Fr* in, uint32_t n, const Fr* init,
+                                                              ScanTiles tiles) {
     constexpr int op = OPK;
     __shared__ Fr wsm[32];
     __shared__ uint32_t s_tile;
     __shared__ Fr s_prefix;
     extern __shared__ uint4 smem_u4[];
     Fr* sm = reinterpret_cast<Fr*>(smem_u4);
-    if (threadIdx.x == 0) s_tile = LOOKBACK ? atomicAdd(tiles.words, 1u) : blockIdx.x;
+    if (threadIdx.x == 0) s_tile = atomicAdd(tiles.words, 1u);
     __syncthreads();
     const uint32_t tile = s_tile;
     const size_t t0 = (size_t)tile * SBLK;
@@ -355,9 +353,7 @@ __global__ void __launch_bounds__(ST, LOOKBACK ? 2 : 3) scan_onepass_kernel(Fr* 
     Fr tot;
     const Fr e = block_excl_scan_fr(op, run, wsm, tot);
     uint32_t* state = tiles.words + 1;
-    if (!LOOKBACK) {
-        if (threadIdx.x == 0) s_prefix = ld_elem<FrCfg>(tiles.agg + tile);
-    } else if (threadIdx.x < 32) {
+    if (threadIdx.x < 32) {
         const int lane = threadIdx.x;
         Fr prefix = op_ident(op);
         if (tile == 0) {
@@ -414,30 +410,63 @@ __global__ void __launch_bounds__(ST, LOOKBACK ? 2 : 3) scan_onepass_kernel(Fr* 
 }
 
 // Reduce-then-scan, for the sum (bound by HBM, where the look-back's waits
-// cost more than they save): (1) every tile's sum, read with coalesced loads
-// and no shared tile; (2) their exclusive scan with the initial value, one
-// block (or this routine again above 2048 tiles); (3) every tile scanned from
-// its prefix.  Three reads and one write of the elements' bytes against the
-// one-pass form's read and write, but no block ever waits on another.
-__global__ void __launch_bounds__(ST) tile_sum_kernel(const Fr* in, uint32_t n, Fr* agg) {
-    __shared__ Fr wsm[32];
-    const size_t t0 = (size_t)blockIdx.x * SBLK;
+// cost more than they save), over segments of 256 elements, one warp each,
+// read row by row (32 consecutive elements an instruction): (1) every
+// segment's sum, (2) their exclusive scan with the initial value (this routine
+// again above 2048 segments), (3) every segment scanned from its prefix, each
+// row by shuffles with the carry of the rows before it.  No shared tile and no
+// block barrier, so few registers and many warps per SM hide the loads; the
+// elements are read twice and written once.
+static constexpr uint32_t WSEG = 256;
+
+__global__ void __launch_bounds__(256) seg_sum_kernel(const Fr* in, uint32_t n, Fr* agg) {
+    const uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    const size_t base = (size_t)w * WSEG;
+    if (base >= n) return;  // the whole warp: w is uniform across it
     Fr acc = fe_zero<FrCfg>();
 #pragma unroll
-    for (int k = 0; k < SK; k++) {
-        const size_t i = t0 + threadIdx.x + (size_t)ST * k;
+    for (uint32_t k = 0; k < WSEG / 32; k++) {
+        const size_t i = base + k * 32 + lane;
         if (i < n) acc = fe_add<FrCfg>(acc, ld_elem<FrCfg>(in + i));
     }
 #pragma unroll
     for (int m = 16; m > 0; m >>= 1) acc = fe_add<FrCfg>(acc, shfl_xor_fr(acc, m));
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    if (lane == 0) wsm[wid] = acc;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        Fr tot = wsm[0];
-        for (int w = 1; w < ST / 32; w++) tot = fe_add<FrCfg>(tot, wsm[w]);
-        st_elem<FrCfg>(agg + blockIdx.x, tot);
+    if (lane == 0) st_elem<FrCfg>(agg + w, acc);
+}
+
+// out may alias in: a warp reads each row before it writes it, and segments
+// belong to one warp each
+__global__ void __launch_bounds__(256) seg_scan_kernel(Fr* out, const Fr* in, uint32_t n, const Fr* pre) {
+    const uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    const size_t base = (size_t)w * WSEG;
+    if (base >= n) return;
+    Fr carry = ld_elem<FrCfg>(pre + w);
+#pragma unroll 1
+    for (uint32_t k = 0; k < WSEG / 32; k++) {
+        const size_t i = base + k * 32 + lane;
+        const Fr x = i < n ? ld_elem<FrCfg>(in + i) : fe_zero<FrCfg>();
+        Fr v = x;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const Fr y = shfl_up_fr(v, o);
+            if ((int)lane >= o) v = fe_add<FrCfg>(y, v);
+        }
+        Fr e = shfl_up_fr(v, 1);
+        if (lane == 0) e = fe_zero<FrCfg>();
+        if (i < n) st_elem<FrCfg>(out + i, fe_add<FrCfg>(carry, e));
+        Fr tot;
+#pragma unroll
+        for (int j = 0; j < 8; j++) tot.v[j] = __shfl_sync(0xffffffffu, v.v[j], 31);
+        carry = fe_add<FrCfg>(carry, tot);
     }
+}
+
+// scratch of the sum's reduce-then-scan: the segment sums, then the same for
+// the segment sums' own scan
+static size_t seg_scan_elems(uint32_t n) {
+    if (n <= (uint32_t)SBLK) return 0;
+    const uint32_t ns = (n + WSEG - 1) / WSEG;
+    return ns + seg_scan_elems(ns);
 }
 
 // tile states after the aggregates and prefixes, in Fr elements
@@ -447,7 +476,8 @@ static size_t onepass_elems(uint32_t nb) { return 2 * (size_t)nb + ((size_t)nb +
 // (the callers below use it for both, one after the other)
 size_t fr_scan_tmp_elems(uint32_t n) {
     const uint32_t nb = (n + SBLK - 1) / SBLK;
-    const size_t one = n > (uint32_t)SBLK ? onepass_elems(nb) : 1;
+    size_t one = n > (uint32_t)SBLK ? onepass_elems(nb) : 1;
+    if (seg_scan_elems(n) > one) one = seg_scan_elems(n);
     const size_t inv = batch_inv_scratch_elems(n);
     return one > inv ? one : inv;
 }
@@ -468,25 +498,25 @@ cudaError_t fr_scan_excl(Fr* out, const Fr* in, uint32_t n, const Fr* init, int 
         return cudaGetLastError();
     }
     if (!tmp) return cudaErrorInvalidValue;
+    if (op == OP_ADD) {
+        const uint32_t ns = (n + WSEG - 1) / WSEG;
+        const unsigned blocks = (unsigned)(((uint64_t)ns * 32 + 255) / 256);
+        seg_sum_kernel<<<blocks, 256, 0, s>>>(in, n, tmp);
+        ZK_CHECK(cudaGetLastError());
+        ZK_CHECK(fr_scan_excl(tmp, tmp, ns, init, op, tmp + ns, s));
+        seg_scan_kernel<<<blocks, 256, 0, s>>>(out, in, n, tmp);
+        return cudaGetLastError();
+    }
+    if (op != OP_MUL) return cudaErrorInvalidValue;
     const uint32_t nb = (n + SBLK - 1) / SBLK;
     ScanTiles tiles;
     tiles.agg = tmp;
     tiles.incl = tmp + nb;
     tiles.words = reinterpret_cast<uint32_t*>(tmp + 2 * (size_t)nb);
-    if (op == OP_ADD) {
-        static SmemOptIn opt_p;
-        ZK_CHECK(opt_p.ensure(scan_onepass_kernel<false, OP_ADD>, (int)SCAN_TILE_SMEM));
-        tile_sum_kernel<<<nb, ST, 0, s>>>(in, n, tiles.agg);
-        ZK_CHECK(cudaGetLastError());
-        ZK_CHECK(fr_scan_excl(tiles.agg, tiles.agg, nb, init, op, tmp + nb, s));
-        scan_onepass_kernel<false, OP_ADD><<<nb, ST, SCAN_TILE_SMEM, s>>>(out, in, n, nullptr, tiles);
-        return cudaGetLastError();
-    }
-    if (op != OP_MUL) return cudaErrorInvalidValue;
     static SmemOptIn opt;
-    ZK_CHECK(opt.ensure(scan_onepass_kernel<true, OP_MUL>, (int)SCAN_TILE_SMEM));
+    ZK_CHECK(opt.ensure(scan_onepass_kernel<OP_MUL>, (int)SCAN_TILE_SMEM));
     ZK_CHECK(cudaMemsetAsync(tiles.words, 0, ((size_t)nb + 1) * sizeof(uint32_t), s));
-    scan_onepass_kernel<true, OP_MUL><<<nb, ST, SCAN_TILE_SMEM, s>>>(out, in, n, init, tiles);
+    scan_onepass_kernel<OP_MUL><<<nb, ST, SCAN_TILE_SMEM, s>>>(out, in, n, init, tiles);
     return cudaGetLastError();
 }
 
